@@ -1,0 +1,252 @@
+/*
+ * sph3.h -- C ABI of the B200 (sm_100a) SPH + Barnes-Hut particle step.
+ *
+ * One shared library (sph_3_b200/lib/libsph3.so).  Plain pointers and sizes,
+ * int status returns, no C++ or torch types.  A context (sph3_ctx) owns the
+ * device copy of one particle set -- or of a batch of independent particle
+ * systems ("clouds") -- in Morton order, its octree and all scratch buffers,
+ * so a step allocates nothing.
+ *
+ * Which reference interface each entry point replaces (paths are within the
+ * reference project hassanfv/SPH_3):
+ *
+ *   sph3_set_particles / sph3_set_field   the NumPy arrays handed to every
+ *        libsx function (sph_code/sph_serial.py:37-97 builds them)
+ *   sph3_compute(SPH3_DO_BOOT_H)          smoothing_length_mpi / do_smoothingX
+ *        (sph_code/libsx.py:752-800)
+ *   sph3_compute(SPH3_DO_H)               h_smooth_fast(_mpi) (libsx.py:804-902);
+ *        GPU: smoothing_h_ngb + ngbDB_new_v3
+ *        (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:485-579,
+ *         .../ngb_v5.1.h:125-264)
+ *   sph3_compute(SPH3_DO_DENSITY)         getDensity(_mpi) (libsx.py:10-86),
+ *        getPressure (libsx.py:91-96) and c = sqrt(gamma (gamma-1) u)
+ *        (sph_serial.py:116); with SPH3_DO_DIVCURL also div_curlVel(_mpi)
+ *        (sph_code/shear.py:7-142)
+ *   sph3_compute(SPH3_DO_ACC_SPH | SPH3_DO_DUDT)  getAcc_sph(_mpi), get_dU(_mpi)
+ *        (libsx.py:100-177, 268-347, 353-421, 496-564), their Monaghan-Gingold
+ *        forms (libsx.py:183-262, 427-491) and the Balsara forms
+ *        getAcc_sph_shear(_mpi), get_dU_shear(_mpi) (shear.py:149-485)
+ *   sph3_compute(SPH3_DO_GRAVITY)         getAcc_g_smth* (libsx.py:623-747, 908-947)
+ *        as a Barnes-Hut walk; GPU: bh_tree_iteration_v2.h:29-588
+ *   sph3_gravity_direct_rows              getAcc_g_smth_mpi (libsx.py:667-705), FP64
+ *   sph3_first_step                       sph_serial.py:85-134
+ *   sph3_step                             one loop body of sph_serial.py:142-196
+ *        (or sph_mpi4_v4.py:278-430 with step_order = SPH3_ORDER_MPI4);
+ *        GPU: hfvGpuSphBHtree_newCool_v8_KH.cu:985-1582
+ *   sph3_energy                           getKE / getPE (libsx.py:569-620)
+ *
+ * Buffers: every pointer argument names memory of the kind its `on_device`
+ * flag says (0: host memory, pageable or pinned; 1: device memory of the
+ * context's GPU).  Host pointers are copied with cudaMemcpyAsync on `stream`
+ * and the call synchronises that stream before it returns; device pointers
+ * are used in stream order without synchronisation.  `stream` is a
+ * cudaStream_t (NULL: the context's own stream).
+ *
+ * Threads: a context is not thread-safe; use one context per host thread or
+ * lock around it.  Errors: every call returns SPH3_OK (0) or an SPH3_ERR_*
+ * code; sph3_error_string() names it.  Device-side conditions (an h search
+ * that did not converge, non-finite input, ...) set bits in a status word that
+ * sph3_status() returns; kernels never trap and every loop in them is bounded.
+ */
+#ifndef SPH3_H
+#define SPH3_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------- return codes */
+#define SPH3_OK 0
+#define SPH3_ERR_INVALID_ARG 1
+#define SPH3_ERR_CUDA 2
+#define SPH3_ERR_NO_DEVICE 3
+#define SPH3_ERR_STATE 4
+#define SPH3_ERR_UNSUPPORTED 5
+#define SPH3_ERR_OUT_OF_MEMORY 6
+#define SPH3_ERR_DEVICE_STATUS 7 /* a device status bit is set, see sph3_status */
+
+/* ----------------------------------------------- device status word bits */
+#define SPH3_STATUS_H_NOT_CONVERGED 0x1u  /* h search hit its iteration cap */
+#define SPH3_STATUS_STACK_OVERFLOW 0x2u   /* walk stack full (cannot happen with stack_cap >= 7*(max_level+2)+32) */
+#define SPH3_STATUS_NAN_INPUT 0x4u        /* non-finite position, velocity, mass or h */
+#define SPH3_STATUS_TREE_CAPACITY 0x8u    /* node array too small */
+#define SPH3_STATUS_ZERO_DENSITY 0x10u    /* rho <= 0 where a division by rho follows */
+#define SPH3_STATUS_LIST_OVERFLOW 0x20u   /* neighbour export capacity exceeded */
+#define SPH3_STATUS_SORT 0x40u            /* radix-sort bookkeeping mismatch */
+
+/* ----------------------------------------------------------------- enums */
+#define SPH3_PREC_MIXED 0 /* FP32 cell-relative pair arithmetic, FP64 state/accumulators/sums */
+#define SPH3_PREC_FP64 1  /* FP64 everywhere */
+
+#define SPH3_H_NEWTON 0  /* Newton iteration on ln N(h) to the window, bounded */
+#define SPH3_H_REFSTEP 1 /* the reference rule: h -/+= 0.003 h until N in the window */
+
+#define SPH3_VISC_SIGNAL 0  /* getAcc_sph / get_dU (libsx.py:151-160) */
+#define SPH3_VISC_MG83 1    /* getAcc_sph_mpiXXX / get_dU_mpiXXXX (libsx.py:236-246) */
+#define SPH3_VISC_BALSARA 2 /* getAcc_sph_shear / get_dU_shear (shear.py:193-215) */
+
+#define SPH3_ORDER_SERIAL 0 /* du/dt with the half-step v, before the 2nd kick (sph_serial.py) */
+#define SPH3_ORDER_MPI4 1   /* du/dt with the full-step v, after the 2nd kick (sph_mpi4_v4.py) */
+
+/* compute flags for sph3_compute */
+#define SPH3_DO_TREE 0x1u      /* Morton sort + octree (implied by every walk) */
+#define SPH3_DO_BOOT_H 0x2u    /* h = 0.5 * distance to the n_boot-th nearest particle */
+#define SPH3_DO_H 0x4u         /* h search to n_ngb +- n_ngb_tol */
+#define SPH3_DO_DENSITY 0x8u   /* rho, P, c (EOS from u) */
+#define SPH3_DO_DIVCURL 0x10u  /* div v, |curl v|, Balsara factor (needs rho: fused with DENSITY) */
+#define SPH3_DO_ACC_SPH 0x20u  /* hydro acceleration from the stored rho, P, c */
+#define SPH3_DO_DUDT 0x40u     /* du/dt from the stored rho, P, c */
+#define SPH3_DO_GRAVITY 0x80u  /* Barnes-Hut acceleration and potential (theta = 0: exact) */
+#define SPH3_DO_EOS 0x100u     /* P, c from the stored rho and u only */
+
+/* field ids for sph3_set_field / sph3_get_field (components per particle) */
+#define SPH3_FIELD_POS 0       /* 3 */
+#define SPH3_FIELD_VEL 1       /* 3 */
+#define SPH3_FIELD_MASS 2      /* 1 */
+#define SPH3_FIELD_U 3         /* 1 */
+#define SPH3_FIELD_H 4         /* 1 */
+#define SPH3_FIELD_EPS 5       /* 1 */
+#define SPH3_FIELD_RHO 6       /* 1 */
+#define SPH3_FIELD_P 7         /* 1 */
+#define SPH3_FIELD_C 8         /* 1 */
+#define SPH3_FIELD_DIVV 9      /* 1 */
+#define SPH3_FIELD_CURLV 10    /* 1 */
+#define SPH3_FIELD_ACC 11      /* 3, total acceleration of the last step */
+#define SPH3_FIELD_ACC_G 12    /* 3 */
+#define SPH3_FIELD_ACC_SPH 13  /* 3 */
+#define SPH3_FIELD_DUDT 14     /* 1 */
+#define SPH3_FIELD_DUDT_PREV 15 /* 1 */
+#define SPH3_FIELD_PHI 16      /* 1, gravitational potential (G included) */
+#define SPH3_FIELD_NNGB 17     /* 1, neighbour count N(r < 2h) of the last h search */
+#define SPH3_FIELD_BALSARA 18  /* 1 */
+#define SPH3_FIELD_U_PREV 19   /* 1 */
+#define SPH3_NUM_FIELDS 20
+
+/* ---------------------------------------------------------------- config */
+typedef struct sph3_config {
+    int32_t precision;   /* SPH3_PREC_* */
+    int32_t h_mode;      /* SPH3_H_* */
+    int32_t visc;        /* SPH3_VISC_* */
+    int32_t step_order;  /* SPH3_ORDER_* */
+    int32_t n_ngb;       /* target neighbour count N(r < 2h) (reference CPU: 50, GPU: 64) */
+    int32_t n_ngb_tol;   /* accepted window n_ngb +- tol (reference: 5) */
+    int32_t h_max_iter;  /* cap on h iterations (SPH3_STATUS_H_NOT_CONVERGED past it) */
+    int32_t n_boot;      /* k of the bootstrap h (reference: 50, 0-based sorted index) */
+    int32_t leaf_size;   /* octree leaf capacity (1..64) */
+    int32_t stack_cap;   /* walk-stack entries per warp: 256 or 512 */
+    int32_t max_level;   /* octree levels (3 key bits each), 4..21 */
+    int32_t gravity;     /* 0: hydro only */
+    int32_t quadrupole;  /* 1: monopole + quadrupole nodes, 0: monopole only */
+    int32_t use_graph;   /* 1: sph3_step replays a captured CUDA graph */
+    int32_t timing;      /* 1: record per-phase CUDA events (no graph) */
+    int32_t reserved_i[5];
+    double gamma;        /* adiabatic index (5/3) */
+    double alpha;        /* artificial viscosity alpha (1) */
+    double beta;         /* beta of the MG83 form (2) */
+    double eta;          /* eta of the MG83 form (0.1) */
+    double G;            /* gravitational constant (1) */
+    double theta;        /* opening angle; 0 = exact direct sum through the tree */
+    double eps;          /* softening length used when no eps field is set (0.01) */
+    double box[3];       /* periodic box lengths, 0 = open boundary in that axis */
+    double reserved_d[4];
+} sph3_config;
+
+typedef struct sph3_ctx sph3_ctx;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int sph3_version(void);
+
+/* Fills cfg with the defaults listed in the struct comments. */
+void sph3_default_config(sph3_config *cfg);
+
+/* Names an SPH3_ERR_* code; a static string. */
+const char *sph3_error_string(int code);
+
+/* Creates a context on CUDA device `device` (-1: the current device). */
+int sph3_ctx_create(const sph3_config *cfg, int device, sph3_ctx **out);
+int sph3_ctx_destroy(sph3_ctx *ctx);
+
+/* Replaces the physics / numerics parameters (sizes of existing buffers stay). */
+int sph3_set_config(sph3_ctx *ctx, const sph3_config *cfg);
+int sph3_get_config(const sph3_ctx *ctx, sph3_config *cfg);
+
+/* Splits the next particle set into `ncloud` independent systems of
+ * counts[0..ncloud) consecutive particles (a batched ensemble).  Default: one
+ * system.  Call before sph3_set_particles. */
+int sph3_set_clouds(sph3_ctx *ctx, const int64_t *counts, int32_t ncloud);
+
+/* Loads n particles (arrays in the caller's order, pos/vel as (n,3) row-major
+ * FP64).  pos and mass are required; vel, u, h, eps may be NULL (0, 0, 0 and
+ * cfg.eps).  Sorts them into Morton order and builds the octree. */
+int sph3_set_particles(sph3_ctx *ctx, int64_t n, const double *pos, const double *vel,
+                       const double *mass, const double *u, const double *h,
+                       const double *eps, int on_device, void *stream);
+
+/* Number of particles currently loaded. */
+int64_t sph3_num_particles(const sph3_ctx *ctx);
+
+/* Overwrites one field from an array in the caller's particle order.
+ * Writing SPH3_FIELD_POS re-sorts and rebuilds the tree. */
+int sph3_set_field(sph3_ctx *ctx, int field, const double *src, int on_device, void *stream);
+
+/* Copies rows [row_begin, row_end) of a field, in the caller's particle order,
+ * to dst ((row_end-row_begin) x components, FP64). */
+int sph3_get_field(sph3_ctx *ctx, int field, double *dst, int64_t row_begin, int64_t row_end,
+                   int on_device, void *stream);
+
+/* Runs the passes named by `what` (SPH3_DO_* bits) on the loaded state. */
+int sph3_compute(sph3_ctx *ctx, uint32_t what, void *stream);
+
+/* The reference's start-up: h (bootstrap if h is all zero, then the h search),
+ * rho, gravity, P, c, hydro acceleration, du/dt, then u += du/dt * dt,
+ * u_prev = u, dudt_prev = du/dt (sph_serial.py:85-134). */
+int sph3_first_step(sph3_ctx *ctx, double dt, void *stream);
+
+/* nsteps leapfrog kick-drift-kick steps of length dt. */
+int sph3_step(sph3_ctx *ctx, double dt, int32_t nsteps, void *stream);
+
+/* Global sums in FP64 of the current state: out[0] KE, out[1] thermal energy
+ * sum m u, out[2] PE = 1/2 sum m phi, out[3] total, out[4..6] momentum,
+ * out[7] mass.  Synchronises `stream`. */
+int sph3_energy(sph3_ctx *ctx, double out[8], void *stream);
+
+/* Device status word (SPH3_STATUS_* bits) accumulated since the last clear.
+ * Synchronises the context's streams. */
+int sph3_status(sph3_ctx *ctx, uint32_t *status, int clear);
+
+/* FP64 spline-softened direct sum for the listed rows (caller's order) against
+ * every particle of the same system: acc (nrows x 3) and, if phi != NULL,
+ * the potential.  Host output buffers. */
+int sph3_gravity_direct_rows(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, double *acc,
+                             double *phi);
+
+/* Neighbour sets {j : |r_ij| <= h_i + h_j} (the q <= 2 support of the
+ * reference kernels) of the listed rows, as caller's indices in ascending
+ * order: row k's set is idx[offsets[k] .. offsets[k+1]).  offsets has nrows+1
+ * entries; at most cap indices are written (SPH3_STATUS_LIST_OVERFLOW past
+ * it).  Host buffers. */
+int sph3_neighbours(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *offsets,
+                    int64_t *idx, int64_t cap);
+
+/* Current Morton order: order[k] = caller's index of the k-th sorted particle,
+ * keys[k] its 64-bit key (either pointer may be NULL).  Host buffers. */
+int sph3_morton_order(sph3_ctx *ctx, int64_t *order, uint64_t *keys);
+
+/* Interaction counters of the last passes: [0] gravity node interactions,
+ * [1] gravity particle interactions, [2] SPH candidate pairs of the density
+ * pass, [3] of the hydro pass, [4] h-search candidate pairs, [5] h passes,
+ * [6] tree nodes, [7] tree leaves.  Clears them if `clear`. */
+int sph3_counters(sph3_ctx *ctx, int64_t out[8], int clear);
+
+/* Per-phase device times in ms accumulated while cfg.timing = 1:
+ * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,
+ * [5] density, [6] gravity, [7] hydro, [8] kick+u+energy.  Clears if `clear`. */
+int sph3_phase_times(sph3_ctx *ctx, double out[9], int clear);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPH3_H */

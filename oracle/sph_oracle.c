@@ -1,0 +1,491 @@
+/*
+ * CPU oracle for the SPH_3 per-step particle path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * This file restates, in plain C with FP64 arithmetic, the all-pairs numba
+ * functions of the reference's CPU library (sph_code/libsx.py and
+ * sph_code/shear.py).  It exists so that the tests, the smoke check and the
+ * CPU-baseline leg of the benchmark have a checker; nothing in the product
+ * (sph_3_b200/) links to it.
+ *
+ * Faithfulness rules (so that results agree bit-for-bit with the numba
+ * originals on the committed golden vectors):
+ *   - every row keeps the reference's j = 0..N-1 summation order;
+ *   - expressions keep the reference's operation order, and the file is
+ *     compiled with -ffp-contract=off (numba/LLVM do not fuse a*b+c);
+ *   - integer powers x**n use the same left-to-right binary exponentiation
+ *     that numba unrolls for a constant integer exponent (ipow below);
+ *   - x**0.5 is the correctly rounded square root.
+ * Rows are processed in parallel with OpenMP; each row is independent, so the
+ * result does not depend on the thread count.
+ *
+ * Additions that the reference does not have (each one reduces to the
+ * reference when left at its default):
+ *   - a `rows` index list instead of the contiguous [nbeg, nend) of the
+ *     *_mpi functions (a contiguous list reproduces them);
+ *   - a periodic minimum-image displacement when box[k] > 0 (box = 0: none);
+ *   - an iteration cap on the h search (the reference loops without bound).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define SIG_M4 (1.0 / 3.141592653589793)
+
+/* numba's unrolled integer power: r = 1; while e: if e&1: r *= v; e >>= 1; v *= v */
+static inline double ipow(double x, int e) {
+    double r = 1.0, v = x;
+    while (e) {
+        if (e & 1) r = r * v;
+        e >>= 1;
+        if (e) v = v * v;
+    }
+    return r;
+}
+
+/* periodic minimum image of one displacement component; no-op for L <= 0 */
+static inline double min_image(double d, double L) {
+    if (L > 0.0) {
+        if (d > 0.5 * L) d -= L;
+        else if (d < -0.5 * L) d += L;
+    }
+    return d;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* M4 gradient factor nW (gradW = nW * (x_i - x_j)); follows
+ * sph_code/libsx.py:127-141 (identical in every hydro function). */
+static inline double m4_grad_factor(double q, double hij) {
+    double nW = 0.0;
+    if (q <= 1.0) {
+        nW = SIG_M4 / ipow(hij, 5) * (-3.0 + 9.0 / 4.0 * q);
+    }
+    if ((q > 1.0) && (q <= 2.0)) {
+        nW = -3.0 * SIG_M4 / 4.0 / ipow(hij, 5) * ipow(2.0 - q, 2) / (q + 1e-20);
+    }
+    return nW;
+}
+
+/* ---------------------------------------------------------------- density
+ * getDensity / getDensity_mpi, sph_code/libsx.py:10-44, 50-86. */
+void orc_density(int64_t n, const double *pos, const double *m, const double *h,
+                 const int64_t *rows, int64_t nrows, const double *box, double *rho) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        double s = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
+            double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
+            double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
+            double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            double hij = 0.5 * (h[i] + h[j]);
+            double q = rr / hij;
+            double W = 0.0;
+            if (q <= 1.0) W = SIG_M4 / ipow(hij, 3) * (1.0 - (3.0 / 2.0) * ipow(q, 2) + (3.0 / 4.0) * ipow(q, 3));
+            if ((q > 1.0) && (q <= 2.0)) W = SIG_M4 / ipow(hij, 3) * (1.0 / 4.0) * ipow(2.0 - q, 3);
+            s += m[j] * W;
+        }
+        rho[r] = s;
+    }
+}
+
+/* Neighbour set of one row: every j with q = |r_ij| / hbar_ij <= 2, the
+ * support of all reference hydro kernels (sph_code/libsx.py:34-38).  Writes at
+ * most cap indices (ascending j) and returns the full count. */
+int64_t orc_neighbours(int64_t n, const double *pos, const double *h, int64_t i,
+                       const double *box, int64_t *out, int64_t cap) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+    int64_t k = 0;
+    for (int64_t j = 0; j < n; ++j) {
+        double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
+        double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
+        double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
+        double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+        double hij = 0.5 * (h[i] + h[j]);
+        double q = rr / hij;
+        if (q <= 2.0) {
+            if (k < cap) out[k] = j;
+            ++k;
+        }
+    }
+    return k;
+}
+
+/* ------------------------------------------------------------- h search
+ * h_smooth_fast / h_smooth_fast_mpi, sph_code/libsx.py:804-845, 852-902:
+ * count N(dist < 2h) including the particle itself, step h by -/+0.3% until
+ * N is in [n_ngb - tol, n_ngb + tol].  The reference fixes n_ngb=50, tol=5 and
+ * has no cap; status[r] = number of steps taken, or -1 if max_iter was hit
+ * (h is then the value after max_iter steps).
+ * The count over all N uses the sorted distance list (same predicate, same
+ * result as np.sum(dist < 2h)). */
+static int cmp_double(const void *a, const void *b) {
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+static int64_t count_below(const double *sorted, int64_t n, double t) {
+    /* number of elements strictly below t */
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (sorted[mid] < t) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static void select_kth(double *a, int64_t n, int64_t k) {
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        double pivot = a[(lo + hi) >> 1];
+        int64_t i = lo, j = hi;
+        while (i <= j) {
+            while (a[i] < pivot) ++i;
+            while (a[j] > pivot) --j;
+            if (i <= j) { double t = a[i]; a[i] = a[j]; a[j] = t; ++i; --j; }
+        }
+        if (k <= j) hi = j;
+        else if (k >= i) lo = i;
+        else break;
+    }
+}
+
+/* count of dist[] < t where dist[0..K) holds the K smallest values sorted */
+static int64_t count_prefix(const double *dist, int64_t n, int64_t K, double t) {
+    if (K == n || (K > 0 && t <= dist[K - 1])) return count_below(dist, K, t);
+    int64_t k = 0;
+    for (int64_t j = 0; j < n; ++j) k += dist[j] < t;
+    return k;
+}
+
+void orc_h_smooth(int64_t n, const double *pos, const double *h_in, const int64_t *rows,
+                  int64_t nrows, int n_ngb, int tol, int64_t max_iter, const double *box,
+                  double *h_out, int64_t *status) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+    const int64_t up = n_ngb + tol, low = n_ngb - tol;
+#pragma omp parallel
+    {
+        double *dist = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t r = 0; r < nrows; ++r) {
+            int64_t i = rows[r];
+            double hi = h_in[i];
+            for (int64_t j = 0; j < n; ++j) {
+                double dx = min_image(pos[3 * j + 0] - pos[3 * i + 0], bx);
+                double dy = min_image(pos[3 * j + 1] - pos[3 * i + 1], by);
+                double dz = min_image(pos[3 * j + 2] - pos[3 * i + 2], bz);
+                dist[j] = sqrt(dx * dx + dy * dy + dz * dz);
+            }
+            /* sort only the K smallest distances: a count below t <= dist[K-1]
+             * is exact on that prefix; larger t falls back to a full scan. */
+            int64_t K = n < 2048 ? n : 2048;
+            if (K < n) select_kth(dist, n, K - 1);
+            qsort(dist, (size_t)K, sizeof(double), cmp_double);
+            int64_t nn = count_prefix(dist, n, K, 2.0 * hi);
+            int64_t it = 0;
+            while ((nn > up) || (nn < low)) {
+                if (it >= max_iter) { it = -1; break; }
+                if (nn > up) hi -= 0.003 * hi;
+                if (nn < low) hi += 0.003 * hi;
+                nn = count_prefix(dist, n, K, 2.0 * hi);
+                ++it;
+            }
+            h_out[r] = hi;
+            if (status) status[r] = it;
+        }
+        free(dist);
+    }
+}
+
+/* Neighbour count N(dist < 2h) of each row with the row's own h. */
+void orc_count_within(int64_t n, const double *pos, const double *h, const int64_t *rows,
+                      int64_t nrows, const double *box, int64_t *count) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        double t = 2.0 * h[i];
+        int64_t k = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = min_image(pos[3 * j + 0] - pos[3 * i + 0], bx);
+            double dy = min_image(pos[3 * j + 1] - pos[3 * i + 1], by);
+            double dz = min_image(pos[3 * j + 2] - pos[3 * i + 2], bz);
+            if (sqrt(dx * dx + dy * dy + dz * dz) < t) ++k;
+        }
+        count[r] = k;
+    }
+}
+
+/* smoothing_length_mpi / do_smoothingX, sph_code/libsx.py:752-800:
+ * h = 0.5 * (k-th smallest distance, self included; the reference uses k=50). */
+void orc_smoothing_length(int64_t n, const double *pos, const int64_t *rows, int64_t nrows,
+                          int k, const double *box, double *h_out) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+#pragma omp parallel
+    {
+        double *dist = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t r = 0; r < nrows; ++r) {
+            int64_t i = rows[r];
+            for (int64_t j = 0; j < n; ++j) {
+                double dx = min_image(pos[3 * j + 0] - pos[3 * i + 0], bx);
+                double dy = min_image(pos[3 * j + 1] - pos[3 * i + 1], by);
+                double dz = min_image(pos[3 * j + 2] - pos[3 * i + 2], bz);
+                dist[j] = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            }
+            int64_t kk = k < n ? k : n - 1;
+            select_kth(dist, n, kk);
+            h_out[r] = dist[kk] * 0.5;
+        }
+        free(dist);
+    }
+}
+
+/* -------------------------------------------------------- div / curl v
+ * div_curlVel / div_curlVel_mpi, sph_code/shear.py:7-69, 76-142. */
+void orc_div_curl(int64_t n, const double *pos, const double *v, const double *rho,
+                  const double *m, const double *h, const int64_t *rows, int64_t nrows,
+                  const double *box, double *divV, double *curlV) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        double s = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
+            double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
+            double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
+            double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            double hij = 0.5 * (h[i] + h[j]);
+            double q = rr / hij;
+            double nW = m4_grad_factor(q, hij);
+            double gWx = 0.0, gWy = 0.0, gWz = 0.0;
+            if (q <= 2.0) { gWx = nW * dx; gWy = nW * dy; gWz = nW * dz; }
+            double vxji = v[3 * j + 0] - v[3 * i + 0];
+            double vyji = v[3 * j + 1] - v[3 * i + 1];
+            double vzji = v[3 * j + 2] - v[3 * i + 2];
+            s += m[j] / rho[i] * (vxji * gWx + vyji * gWy + vzji * gWz);
+            double vxij = v[3 * i + 0] - v[3 * j + 0];
+            double vyij = v[3 * i + 1] - v[3 * j + 1];
+            double vzij = v[3 * i + 2] - v[3 * j + 2];
+            cx += m[j] / rho[i] * (vyij * gWz - vzij * gWy);
+            cy += m[j] / rho[i] * (vzij * gWx - vxij * gWz);
+            cz += m[j] / rho[i] * (vxij * gWy - vyij * gWx);
+        }
+        divV[r] = fabs(s);
+        curlV[r] = sqrt(cx * cx + cy * cy + cz * cz);
+    }
+}
+
+/* ------------------------------------------------ hydro accel and du/dt
+ * visc = 0: signal-velocity viscosity of getAcc_sph / get_dU
+ *           (sph_code/libsx.py:100-177, 268-347, 353-421, 496-564);
+ * visc = 1: Monaghan & Gingold (1983) form of getAcc_sph_mpiXXX /
+ *           get_dU_mpiXXXX (sph_code/libsx.py:183-262, 427-491);
+ * visc = 2: signal form times the Balsara factor of getAcc_sph_shear /
+ *           get_dU_shear (sph_code/shear.py:149-235, 332-406).
+ * acc (3 per row) and/or dudt may be NULL. */
+void orc_hydro(int64_t n, const double *pos, const double *v, const double *rho,
+               const double *P, const double *c, const double *h, const double *m,
+               const double *divV, const double *curlV, int visc, double alpha, double beta,
+               double eta, const int64_t *rows, int64_t nrows, const double *box,
+               double *acc, double *dudt) {
+    const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        double axt = 0.0, ayt = 0.0, azt = 0.0, du_t = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
+            double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
+            double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
+            double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            double hij = 0.5 * (h[i] + h[j]);
+            double q = rr / hij;
+            double nW = m4_grad_factor(q, hij);
+            double gWx = 0.0, gWy = 0.0, gWz = 0.0;
+            if (q <= 2.0) { gWx = nW * dx; gWy = nW * dy; gWz = nW * dz; }
+            double vxij = v[3 * i + 0] - v[3 * j + 0];
+            double vyij = v[3 * i + 1] - v[3 * j + 1];
+            double vzij = v[3 * i + 2] - v[3 * j + 2];
+            double vij_gWij = vxij * gWx + vyij * gWy + vzij * gWz;
+            double vij_rij = vxij * dx + vyij * dy + vzij * dz;
+            double cij = 0.5 * (c[i] + c[j]);
+            double rhoij = 0.5 * (rho[i] + rho[j]);
+            double PIij = 0.0;
+            if (visc == 1) {
+                double muij = hij * vij_rij / (rr * rr + hij * hij * eta * eta);
+                if (vij_rij <= 0) PIij = (-alpha * cij * muij + beta * muij * muij) / rhoij;
+            } else {
+                double wij = vij_rij / (rr + 1e-5);
+                double vij_sig = c[i] + c[j] - 3.0 * wij;
+                if (vij_rij <= 0) PIij = -0.5 * alpha * vij_sig * wij / rhoij;
+                if (visc == 2) {
+                    double fi = divV[i] / (divV[i] + curlV[i] + 0.0001 * c[i] / h[i]);
+                    double fj = divV[j] / (divV[j] + curlV[j] + 0.0001 * c[j] / h[j]);
+                    double fij = 0.5 * (fi + fj);
+                    PIij = fij * PIij;
+                }
+            }
+            double pterm = P[i] / ipow(rho[i], 2) + P[j] / ipow(rho[j], 2) + PIij;
+            axt -= m[j] * pterm * gWx;
+            ayt -= m[j] * pterm * gWy;
+            azt -= m[j] * pterm * gWz;
+            du_t += m[j] * (P[i] / ipow(rho[i], 2) + PIij / 2.) * vij_gWij;
+        }
+        if (acc) { acc[3 * r + 0] = axt; acc[3 * r + 1] = ayt; acc[3 * r + 2] = azt; }
+        if (dudt) dudt[r] = du_t;
+    }
+}
+
+/* --------------------------------------------------------------- gravity
+ * Spline-softened direct sum, row form of getAcc_g_smth_mpi / getAcc_g_smthx
+ * (sph_code/libsx.py:667-705, 710-747): a_i = -sum_{j != i} G fk (x_i - x_j) m_j
+ * with eps_ij = (eps_i + eps_j) / 2.  phi (may be NULL) is the matching
+ * potential with getPE's kernel (sph_code/libsx.py:583-620), without G*m_i
+ * (a coincident pair adds 0 to phi, as its q = 0 case does in getPE).
+ * A coincident pair (r = 0, j != i) contributes nothing, where the reference
+ * raises ZeroDivisionError. */
+static inline double grav_fk(double rr, double epsij) {
+    double q = rr / epsij;
+    double fk;
+    if (q <= 1.0) {
+        fk = (1.0 / ipow(epsij, 3)) * ((4.0 / 3.0) - (6.0 / 5.0) * ipow(q, 2) + (1.0 / 2.0) * ipow(q, 3));
+    } else {
+        double inv_r3 = 1.0 / ipow(rr, 3);
+        if (q <= 2.0)
+            fk = inv_r3 * ((-1.0 / 15.0) + (8.0 / 3.0) * ipow(q, 3) - 3.0 * ipow(q, 4) + (6.0 / 5.0) * ipow(q, 5) - (1.0 / 6.0) * ipow(q, 6));
+        else
+            fk = inv_r3;
+    }
+    return fk;
+}
+
+static inline double grav_pk(double rr, double epsij) {
+    /* potential kernel of getPE (positive; phi = -G * sum m_j pk) */
+    double q = rr / epsij;
+    double inv_r = rr != 0.0 ? 1.0 / rr : 0.0;
+    double fk = 0.0;
+    if ((q <= 1.0) && (q != 0.0))
+        fk = ((-2.0 / epsij) * ((1.0 / 3.0) * ipow(q, 2) - (3.0 / 20.0) * ipow(q, 4) + (1.0 / 20.0) * ipow(q, 5)) + 7.0 / 5.0 / epsij);
+    if ((q > 1.) && (q <= 2.))
+        fk = ((-1.0 / 15.0) * inv_r - (1.0 / epsij) * ((4.0 / 3.0) * ipow(q, 2) - ipow(q, 3) + (3.0 / 10.0) * ipow(q, 4) - (1.0 / 30.0) * ipow(q, 5)) + 8.0 / 5.0 / epsij);
+    if (q > 2.) fk = inv_r;
+    return fk;
+}
+
+void orc_grav_direct(int64_t n, const double *pos, const double *mass, double G,
+                     const double *eps, const int64_t *rows, int64_t nrows, double *acc,
+                     double *phi) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        double fx = 0.0, fy = 0.0, fz = 0.0, ph = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (i == j) continue;
+            double dx = pos[3 * i + 0] - pos[3 * j + 0];
+            double dy = pos[3 * i + 1] - pos[3 * j + 1];
+            double dz = pos[3 * i + 2] - pos[3 * j + 2];
+            double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            double epsij = 0.5 * (eps[i] + eps[j]);
+            if (rr > 0.0) {
+                double fk = grav_fk(rr, epsij);
+                fx -= G * fk * dx * mass[j];
+                fy -= G * fk * dy * mass[j];
+                fz -= G * fk * dz * mass[j];
+            }
+            if (phi) {
+                ph -= G * mass[j] * grav_pk(rr, epsij);
+            }
+        }
+        acc[3 * r + 0] = fx; acc[3 * r + 1] = fy; acc[3 * r + 2] = fz;
+        if (phi) phi[r] = ph;
+    }
+}
+
+/* Pairwise-symmetric form of getAcc_g_smth (sph_code/libsx.py:623-662): the
+ * j > i loop with both updates, serial (its sums depend on the order). */
+void orc_grav_sym(int64_t n, const double *pos, const double *mass, double G,
+                  const double *eps, double *field) {
+    memset(field, 0, sizeof(double) * 3 * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        for (int64_t j = i + 1; j < n; ++j) {
+            double dx = pos[3 * j + 0] - pos[3 * i + 0];
+            double dy = pos[3 * j + 1] - pos[3 * i + 1];
+            double dz = pos[3 * j + 2] - pos[3 * i + 2];
+            double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            double epsij = 0.5 * (eps[i] + eps[j]);
+            double q = rr / epsij;
+            double fk;
+            if (q <= 1.0) {
+                fk = (1.0 / ipow(epsij, 3)) * ((4.0 / 3.0) - (6.0 / 5.0) * ipow(q, 2) + (1.0 / 2.0) * ipow(q, 3));
+            } else {
+                double inv_r3 = 1.0 / ipow(rr, 3);
+                if (q <= 2.)
+                    fk = inv_r3 * ((-1.0 / 15.0) + (8.0 / 3.0) * ipow(q, 3) - 3.0 * ipow(q, 4) + (6.0 / 5.0) * ipow(q, 5) - (1.0 / 6.0) * ipow(q, 6));
+                else
+                    fk = inv_r3;
+            }
+            field[3 * i + 0] += G * fk * dx * mass[j];
+            field[3 * j + 0] -= G * fk * dx * mass[i];
+            field[3 * i + 1] += G * fk * dy * mass[j];
+            field[3 * j + 1] -= G * fk * dy * mass[i];
+            field[3 * i + 2] += G * fk * dz * mass[j];
+            field[3 * j + 2] -= G * fk * dz * mass[i];
+        }
+    }
+}
+
+/* getPE, sph_code/libsx.py:583-620 (serial j > i double loop). */
+double orc_pe(int64_t n, const double *pos, const double *m, double G, const double *eps) {
+    double PE = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        for (int64_t j = i + 1; j < n; ++j) {
+            double dx = pos[3 * i + 0] - pos[3 * j + 0];
+            double dy = pos[3 * i + 1] - pos[3 * j + 1];
+            double dz = pos[3 * i + 2] - pos[3 * j + 2];
+            double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            double epsij = 0.5 * (eps[i] + eps[j]);
+            double fk = 0.0;
+            double q = rr / epsij;
+            double inv_r = rr != 0.0 ? 1.0 / rr : 0.0;
+            if ((q <= 1.0) && (q != 0.0))
+                fk = m[j] * ((-2.0 / epsij) * ((1.0 / 3.0) * ipow(q, 2) - (3.0 / 20.0) * ipow(q, 4) + (1.0 / 20.0) * ipow(q, 5)) + 7.0 / 5.0 / epsij);
+            if ((q > 1.) && (q <= 2.))
+                fk = m[j] * ((-1.0 / 15.0) * inv_r - (1.0 / epsij) * ((4.0 / 3.0) * ipow(q, 2) - ipow(q, 3) + (3.0 / 10.0) * ipow(q, 4) - (1.0 / 30.0) * ipow(q, 5)) + 8.0 / 5.0 / epsij);
+            if (q > 2.) fk = m[j] * inv_r;
+            PE -= G * m[i] * fk;
+        }
+    }
+    return PE;
+}
+
+/* getKE, sph_code/libsx.py:569-579. */
+double orc_ke(int64_t n, const double *v, const double *m) {
+    double KE = 0.0;
+    for (int64_t i = 0; i < n; ++i)
+        KE += 0.5 * m[i] * (ipow(v[3 * i + 0], 2) + ipow(v[3 * i + 1], 2) + ipow(v[3 * i + 2], 2));
+    return KE;
+}

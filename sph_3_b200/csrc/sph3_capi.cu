@@ -1,0 +1,1049 @@
+// C ABI of libsph3: context lifetime, host/device transfers in the caller's
+// particle order, the compute passes and the captured timestep.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "sph3_internal.cuh"
+
+using namespace sph3;
+
+namespace sph3 {
+void launch_balsara(State &S, cudaStream_t st);
+}
+
+// ------------------------------------------------------------ context
+struct sph3_ctx {
+    sph3_config cfg{};
+    Params P{};
+    State S{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    // carried fields (permuted with the particles every step), two blocks
+    double *carried[2] = {nullptr, nullptr};
+    int64_t *orig_blk[2] = {nullptr, nullptr};
+    int cur = 0;
+    // fields recomputed every step (permuted only on an explicit re-sort)
+    double *fixed = nullptr;
+    double *tmp = nullptr;       // 9 n scratch for permuting fixed fields
+    double *staging = nullptr;   // 3 n, transfers in the caller's order
+    int64_t *inv = nullptr;      // caller index -> sorted index
+    bool inv_valid = false;
+    int64_t cap_n = -1;
+    int cap_nodes = 0;
+    int cap_groups = 0;
+    int cap_clouds = 0;
+    int cap_sortblk = 0;
+    std::vector<int64_t> cloud_counts;  // layout for the next set_particles
+    std::vector<int64_t> cur_counts;
+    bool have = false;
+    unsigned pack_dirty = 0;
+    bool bal_dirty = false;
+    bool tree_dirty = true;
+    bool h_dirty_tree = false;  // node hmax stale
+    // graphs (one per carried-block parity)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double graph_dt[2] = {0, 0};
+    int warm_steps = 0;
+    // timing
+    cudaEvent_t ev[12] = {};
+    double phase_ms[9] = {};
+};
+
+namespace {
+
+int cuda_err(cudaError_t e) { return e == cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA; }
+
+#define CK(x)                                            \
+    do {                                                 \
+        cudaError_t _e = (x);                            \
+        if (_e != cudaSuccess) return SPH3_ERR_CUDA;     \
+    } while (0)
+
+int check_launch() { return cuda_err(cudaGetLastError()); }
+
+constexpr int kCarried = 12;  // pos(3) vel(3) u u_prev dudt_prev m h eps
+constexpr int kFixed = 17;    // acc(3) acc_g(3) acc_sph(3) dudt rho P c divV curlV bal phi
+
+void point_carried(sph3_ctx *c) {
+    State &S = c->S;
+    const int64_t n = std::max<int64_t>(c->cap_n, 1);
+    double *b = c->carried[c->cur];
+    S.pos = b;
+    S.vel = b + 3 * n;
+    S.u = b + 6 * n;
+    S.u_prev = b + 7 * n;
+    S.dudt_prev = b + 8 * n;
+    S.m = b + 9 * n;
+    S.h = b + 10 * n;
+    S.eps = b + 11 * n;
+    S.orig = c->orig_blk[c->cur];
+}
+
+void point_fixed(sph3_ctx *c) {
+    State &S = c->S;
+    const int64_t n = std::max<int64_t>(c->cap_n, 1);
+    double *b = c->fixed;
+    S.acc = b;
+    S.acc_g = b + 3 * n;
+    S.acc_sph = b + 6 * n;
+    S.dudt = b + 9 * n;
+    S.rho = b + 10 * n;
+    S.P = b + 11 * n;
+    S.c = b + 12 * n;
+    S.divV = b + 13 * n;
+    S.curlV = b + 14 * n;
+    S.bal = b + 15 * n;
+    S.phi = b + 16 * n;
+}
+
+void params_from(const sph3_config &cfg, Params &P) {
+    P.precision = cfg.precision;
+    P.h_mode = cfg.h_mode;
+    P.visc = cfg.visc;
+    P.step_order = cfg.step_order;
+    P.n_ngb = cfg.n_ngb;
+    P.n_ngb_tol = cfg.n_ngb_tol;
+    P.h_max_iter = cfg.h_max_iter;
+    P.n_boot = cfg.n_boot;
+    P.leaf_size = cfg.leaf_size;
+    P.stack_cap = cfg.stack_cap;
+    P.max_level = cfg.max_level;
+    P.gravity = cfg.gravity;
+    P.quadrupole = cfg.quadrupole;
+    P.gamma = cfg.gamma;
+    P.alpha = cfg.alpha;
+    P.beta = cfg.beta;
+    P.eta = cfg.eta;
+    P.G = cfg.G;
+    P.theta = cfg.theta;
+    P.eps = cfg.eps;
+    P.periodic = 0;
+    for (int d = 0; d < 3; ++d) {
+        P.box[d] = cfg.box[d];
+        if (cfg.box[d] > 0) P.periodic = 1;
+    }
+}
+
+int validate(const sph3_config *c) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (c->precision != SPH3_PREC_MIXED && c->precision != SPH3_PREC_FP64) return SPH3_ERR_INVALID_ARG;
+    if (c->h_mode != SPH3_H_NEWTON && c->h_mode != SPH3_H_REFSTEP) return SPH3_ERR_INVALID_ARG;
+    if (c->visc < 0 || c->visc > 2) return SPH3_ERR_INVALID_ARG;
+    if (c->step_order != SPH3_ORDER_SERIAL && c->step_order != SPH3_ORDER_MPI4) return SPH3_ERR_INVALID_ARG;
+    if (c->n_ngb < 1 || c->n_ngb_tol < 0 || c->n_ngb_tol >= c->n_ngb) return SPH3_ERR_INVALID_ARG;
+    if (c->h_max_iter < 1 || c->n_boot < 0) return SPH3_ERR_INVALID_ARG;
+    if (c->leaf_size < 1 || c->leaf_size > 64) return SPH3_ERR_INVALID_ARG;
+    if (c->max_level < 4 || c->max_level > 21) return SPH3_ERR_INVALID_ARG;
+    if (c->stack_cap < 7 * (c->max_level + 2) + 32 || c->stack_cap > 4096) return SPH3_ERR_INVALID_ARG;
+    if (!(c->theta >= 0.0) || !(c->eps > 0.0) || !(c->gamma >= 1.0)) return SPH3_ERR_INVALID_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!(c->box[d] >= 0.0) || !std::isfinite(c->box[d])) return SPH3_ERR_INVALID_ARG;
+    if ((c->box[0] > 0 || c->box[1] > 0 || c->box[2] > 0) && c->gravity) return SPH3_ERR_UNSUPPORTED;
+    return SPH3_OK;
+}
+
+void free_buffers(sph3_ctx *c) {
+    State &S = c->S;
+    void *ptrs[] = {c->carried[0], c->carried[1], c->orig_blk[0], c->orig_blk[1], c->fixed, c->tmp,
+                    c->staging, c->inv, S.nngb, S.key, S.key_alt, S.perm, S.perm_alt, S.pk_pos, S.pk_hme,
+                    S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
+                    S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
+                    S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
+                    S.tree.scan_tmp, S.groups, S.group_cloud, S.clouds};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    c->carried[0] = c->carried[1] = nullptr;
+    c->orig_blk[0] = c->orig_blk[1] = nullptr;
+    c->fixed = c->tmp = c->staging = nullptr;
+    c->inv = nullptr;
+    S.nngb = nullptr;
+    S.key = S.key_alt = nullptr;
+    S.perm = S.perm_alt = nullptr;
+    S.pk_pos = S.pk_hme = S.pk_vel = S.pk_thm = nullptr;
+    S.sort_hist = nullptr;
+    S.tree = Tree{};
+    S.groups = nullptr;
+    S.group_cloud = nullptr;
+    S.clouds = nullptr;
+    c->cap_n = -1;
+    c->cap_nodes = c->cap_groups = c->cap_clouds = c->cap_sortblk = 0;
+}
+
+void drop_graphs(sph3_ctx *c) {
+    for (int k = 0; k < 2; ++k) {
+        if (c->graph[k]) cudaGraphExecDestroy(c->graph[k]);
+        c->graph[k] = nullptr;
+    }
+    c->warm_steps = 0;
+}
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+    return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+}
+
+int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
+    if (n == c->cap_n && ncloud <= c->cap_clouds && ngroups <= c->cap_groups) return SPH3_OK;
+    drop_graphs(c);
+    free_buffers(c);
+    State &S = c->S;
+    const int64_t nn = std::max<int64_t>(n, 1);
+    c->cap_n = n;
+    CK(dalloc(&c->carried[0], kCarried * nn));
+    CK(dalloc(&c->carried[1], kCarried * nn));
+    CK(dalloc(&c->orig_blk[0], nn));
+    CK(dalloc(&c->orig_blk[1], nn));
+    CK(dalloc(&c->fixed, kFixed * nn));
+    CK(dalloc(&c->tmp, 9 * nn));
+    CK(dalloc(&c->staging, 3 * nn));
+    CK(dalloc(&c->inv, nn));
+    CK(cudaMemset(c->carried[0], 0, sizeof(double) * kCarried * nn));
+    CK(cudaMemset(c->carried[1], 0, sizeof(double) * kCarried * nn));
+    CK(cudaMemset(c->fixed, 0, sizeof(double) * kFixed * nn));
+    CK(dalloc(&S.nngb, nn));
+    CK(cudaMemset(S.nngb, 0, sizeof(int) * nn));
+    CK(dalloc(&S.key, nn));
+    CK(dalloc(&S.key_alt, nn));
+    CK(dalloc(&S.perm, nn));
+    CK(dalloc(&S.perm_alt, nn));
+    CK(dalloc(&S.pk_pos, nn));
+    CK(dalloc(&S.pk_hme, nn));
+    CK(dalloc(&S.pk_vel, nn));
+    CK(dalloc(&S.pk_thm, nn));
+    CK(cudaMemset(S.pk_thm, 0, sizeof(float4) * nn));
+    c->cap_sortblk = (int)((nn + 2047) / 2048);
+    CK(dalloc(&S.sort_hist, (size_t)256 * c->cap_sortblk));
+    const int cap = (int)std::min<int64_t>(2 * nn + ncloud + 64, (int64_t)INT32_MAX - 1);
+    c->cap_nodes = cap;
+    Tree &T = S.tree;
+    T.cap = cap;
+    CK(dalloc(&T.range, cap));
+    CK(dalloc(&T.child, cap));
+    CK(dalloc(&T.mass, cap));
+    CK(dalloc(&T.com, 3 * (size_t)cap));
+    CK(dalloc(&T.bmin, 3 * (size_t)cap));
+    CK(dalloc(&T.bmax, 3 * (size_t)cap));
+    CK(dalloc(&T.hmax, cap));
+    CK(dalloc(&T.epsmax, cap));
+    CK(dalloc(&T.quad, 6 * (size_t)cap));
+    CK(dalloc(&T.box_c, cap));
+    CK(dalloc(&T.box_h, cap));
+    CK(dalloc(&T.com_c, cap));
+    CK(dalloc(&T.mono, cap));
+    CK(dalloc(&T.quad4, cap));
+    CK(dalloc(&T.quad1, cap));
+    CK(dalloc(&T.nchild_tmp, cap));
+    // scan_tmp doubles as depth_begin (+64) and scratch counters
+    CK(dalloc(&T.scan_tmp, (size_t)cap + 128));
+    T.depth_begin = T.scan_tmp + cap;
+    T.total = T.scan_tmp + cap + 96;
+    c->cap_groups = std::max(ngroups, 1);
+    CK(dalloc(&S.groups, c->cap_groups));
+    CK(dalloc(&S.group_cloud, c->cap_groups));
+    c->cap_clouds = std::max(ncloud, 1);
+    CK(dalloc(&S.clouds, c->cap_clouds));
+    c->cur = 0;
+    point_carried(c);
+    point_fixed(c);
+    return SPH3_OK;
+}
+
+cudaStream_t pick(sph3_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
+
+// ------------------------------------------------------------ small kernels
+// row-major (n, ncomp) caller-order array -> component-major sorted field
+__global__ void k_scatter_in(const double *src, double *dst, const int64_t *orig, int64_t n, int ncomp) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = orig[k];
+        for (int c = 0; c < ncomp; ++c) dst[c * n + k] = src[o * ncomp + c];
+    }
+}
+
+// rows [b, e) of a component-major sorted field -> row-major caller order
+__global__ void k_gather_out(const double *src, double *dst, const int64_t *inv, int64_t n, int ncomp,
+                             int64_t b, int64_t e) {
+    for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = inv[r];
+        for (int c = 0; c < ncomp; ++c) dst[(r - b) * ncomp + c] = src[c * n + k];
+    }
+}
+
+__global__ void k_gather_out_int(const int *src, double *dst, const int64_t *inv, int64_t b, int64_t e) {
+    for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x)
+        dst[r - b] = (double)src[inv[r]];
+}
+
+__global__ void k_invert(const int64_t *orig, int64_t *inv, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        inv[orig[k]] = k;
+}
+
+__global__ void k_iota64(int64_t *a, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        a[k] = k;
+}
+
+__global__ void k_fill(double *a, int64_t n, double v) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        a[k] = v;
+}
+
+__global__ void k_copy(const double *s, double *d, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        d[k] = s[k];
+}
+
+int blocks_for(const sph3_ctx *c, int64_t n) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)c->S.num_sms * 8));
+}
+
+// field id -> (pointer, components)
+double *field_ptr(sph3_ctx *c, int f, int *ncomp) {
+    State &S = c->S;
+    *ncomp = 1;
+    switch (f) {
+        case SPH3_FIELD_POS: *ncomp = 3; return S.pos;
+        case SPH3_FIELD_VEL: *ncomp = 3; return S.vel;
+        case SPH3_FIELD_MASS: return S.m;
+        case SPH3_FIELD_U: return S.u;
+        case SPH3_FIELD_H: return S.h;
+        case SPH3_FIELD_EPS: return S.eps;
+        case SPH3_FIELD_RHO: return S.rho;
+        case SPH3_FIELD_P: return S.P;
+        case SPH3_FIELD_C: return S.c;
+        case SPH3_FIELD_DIVV: return S.divV;
+        case SPH3_FIELD_CURLV: return S.curlV;
+        case SPH3_FIELD_ACC: *ncomp = 3; return S.acc;
+        case SPH3_FIELD_ACC_G: *ncomp = 3; return S.acc_g;
+        case SPH3_FIELD_ACC_SPH: *ncomp = 3; return S.acc_sph;
+        case SPH3_FIELD_DUDT: return S.dudt;
+        case SPH3_FIELD_DUDT_PREV: return S.dudt_prev;
+        case SPH3_FIELD_PHI: return S.phi;
+        case SPH3_FIELD_BALSARA: return S.bal;
+        case SPH3_FIELD_U_PREV: return S.u_prev;
+        default: return nullptr;
+    }
+}
+
+// sort the current particles (positions changed) and permute every field
+int resort_all(sph3_ctx *c, cudaStream_t st) {
+    State &S = c->S;
+    if (S.n == 0) return SPH3_OK;
+    launch_cloud_boxes(S, c->P, st);
+    launch_keys(S, c->P, st);
+    launch_radix_sort(S, st);
+    // carried block -> other block
+    const int other = c->cur ^ 1;
+    double *src = c->carried[c->cur], *dst = c->carried[other];
+    const int64_t n = c->cap_n;
+    const double *srcs[kCarried];
+    double *dsts[kCarried];
+    int nc[kCarried];
+    for (int k = 0; k < kCarried; ++k) {
+        srcs[k] = src + k * n;
+        dsts[k] = dst + k * n;
+        nc[k] = 1;
+    }
+    launch_gather(S, srcs, dsts, kCarried, nc, st);
+    launch_gather_orig(S, c->orig_blk[c->cur], c->orig_blk[other], st);
+    // fixed fields: through tmp, 9 at a time
+    for (int k0 = 0; k0 < kFixed; k0 += 9) {
+        const int cnt = std::min(9, kFixed - k0);
+        const double *s2[9];
+        double *d2[9];
+        int n2[9];
+        for (int k = 0; k < cnt; ++k) {
+            s2[k] = c->fixed + (k0 + k) * n;
+            d2[k] = c->tmp + k * n;
+            n2[k] = 1;
+        }
+        launch_gather(S, s2, d2, cnt, n2, st);
+        k_copy<<<blocks_for(c, cnt * n), 256, 0, st>>>(c->tmp, c->fixed + k0 * n, cnt * n);
+    }
+    // nngb is not permuted (an h-search output); clear it
+    cudaMemsetAsync(S.nngb, 0, sizeof(int) * n, st);
+    c->cur = other;
+    point_carried(c);
+    c->inv_valid = false;
+    launch_pack(S, c->P, kPackPos | kPackHme | kPackVel | kPackThm, st);
+    c->pack_dirty = 0;
+    launch_tree_build(S, c->P, st);
+    c->tree_dirty = false;
+    c->h_dirty_tree = false;
+    return check_launch();
+}
+
+int ensure_inv(sph3_ctx *c, cudaStream_t st) {
+    if (c->inv_valid || c->S.n == 0) return SPH3_OK;
+    k_invert<<<blocks_for(c, c->S.n), 256, 0, st>>>(c->S.orig, c->inv, c->S.n);
+    c->inv_valid = true;
+    return check_launch();
+}
+
+int sync_packs(sph3_ctx *c, cudaStream_t st) {
+    if (c->pack_dirty) {
+        launch_pack(c->S, c->P, c->pack_dirty, st);
+        c->pack_dirty = 0;
+    }
+    if (c->bal_dirty) {
+        launch_balsara(c->S, st);
+        c->bal_dirty = false;
+    }
+    if (c->tree_dirty) {
+        launch_tree_build(c->S, c->P, st);
+        c->tree_dirty = false;
+        c->h_dirty_tree = false;
+    }
+    if (c->h_dirty_tree) {
+        launch_tree_refit_h(c->S, st);
+        c->h_dirty_tree = false;
+    }
+    return check_launch();
+}
+
+void record(sph3_ctx *c, int k, cudaStream_t st) {
+    if (c->cfg.timing) cudaEventRecord(c->ev[k], st);
+}
+
+// One timestep, enqueued on st.  Switches the carried block half way (the
+// gather after the sort writes the other block).
+void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
+    State &S = c->S;
+    const Params &P = c->P;
+    record(c, 0, st);
+    launch_kick_drift(S, P, dt, st);
+    launch_cloud_boxes(S, P, st);
+    launch_keys(S, P, st);
+    record(c, 1, st);
+    launch_radix_sort(S, st);
+    record(c, 2, st);
+    {
+        const int other = c->cur ^ 1;
+        const int64_t n = c->cap_n;
+        const double *srcs[kCarried];
+        double *dsts[kCarried];
+        int nc[kCarried];
+        for (int k = 0; k < kCarried; ++k) {
+            srcs[k] = c->carried[c->cur] + k * n;
+            dsts[k] = c->carried[other] + k * n;
+            nc[k] = 1;
+        }
+        launch_gather(S, srcs, dsts, kCarried, nc, st);
+        launch_gather_orig(S, c->orig_blk[c->cur], c->orig_blk[other], st);
+        c->cur = other;
+        point_carried(c);
+        launch_pack(S, P, kPackPos | kPackHme | kPackVel, st);
+    }
+    record(c, 3, st);
+    launch_tree_build(S, P, st);
+    record(c, 4, st);
+    launch_h_search(S, P, st);
+    launch_tree_refit_h(S, st);
+    record(c, 5, st);
+    launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
+    record(c, 6, st);
+    if (P.gravity) launch_gravity(S, P, st);
+    record(c, 7, st);
+    const bool serial = P.step_order == SPH3_ORDER_SERIAL;
+    launch_hydro(S, P, true, serial, st);
+    record(c, 8, st);
+    if (serial) {
+        launch_kick_update(S, P, dt, true, true, st);
+    } else {
+        launch_kick_update(S, P, dt, false, true, st);
+        record(c, 9, st);
+        launch_hydro(S, P, false, true, st);
+        record(c, 10, st);
+        launch_u_update(S, P, dt, st);
+    }
+    launch_energy(S, P, st);
+    record(c, 11, st);
+    c->inv_valid = false;
+}
+
+void accumulate_times(sph3_ctx *c, bool serial) {
+    float ms;
+    auto add = [&](int slot, int a, int b) {
+        if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) == cudaSuccess) c->phase_ms[slot] += ms;
+    };
+    add(0, 0, 1);
+    add(1, 1, 2);
+    add(2, 2, 3);
+    add(3, 3, 4);
+    add(4, 4, 5);
+    add(5, 5, 6);
+    add(6, 6, 7);
+    if (serial) {
+        add(7, 7, 8);
+        add(8, 8, 11);
+    } else {
+        add(7, 7, 8);
+        add(8, 8, 9);
+        add(7, 9, 10);
+        add(8, 10, 11);
+    }
+}
+
+}  // namespace
+
+// ================================================================== ABI
+extern "C" {
+
+int sph3_version(void) { return 10000; }
+
+void sph3_default_config(sph3_config *cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->precision = SPH3_PREC_MIXED;
+    cfg->h_mode = SPH3_H_NEWTON;
+    cfg->visc = SPH3_VISC_SIGNAL;
+    cfg->step_order = SPH3_ORDER_SERIAL;
+    cfg->n_ngb = 64;
+    cfg->n_ngb_tol = 5;
+    cfg->h_max_iter = 64;
+    cfg->n_boot = 50;
+    cfg->leaf_size = 16;
+    cfg->stack_cap = 512;
+    cfg->max_level = 16;
+    cfg->gravity = 1;
+    cfg->quadrupole = 1;
+    cfg->use_graph = 1;
+    cfg->timing = 0;
+    cfg->gamma = 5.0 / 3.0;
+    cfg->alpha = 1.0;
+    cfg->beta = 2.0;
+    cfg->eta = 0.1;
+    cfg->G = 1.0;
+    cfg->theta = 0.5;
+    cfg->eps = 0.01;
+}
+
+const char *sph3_error_string(int code) {
+    switch (code) {
+        case SPH3_OK: return "ok";
+        case SPH3_ERR_INVALID_ARG: return "invalid argument";
+        case SPH3_ERR_CUDA: return "CUDA error";
+        case SPH3_ERR_NO_DEVICE: return "no CUDA device";
+        case SPH3_ERR_STATE: return "call out of order (no particles loaded?)";
+        case SPH3_ERR_UNSUPPORTED: return "unsupported combination (e.g. gravity with a periodic box)";
+        case SPH3_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case SPH3_ERR_DEVICE_STATUS: return "device status bit set";
+        default: return "unknown error";
+    }
+}
+
+int sph3_ctx_create(const sph3_config *cfg, int device, sph3_ctx **out) {
+    if (!out) return SPH3_ERR_INVALID_ARG;
+    *out = nullptr;
+    sph3_config def;
+    sph3_default_config(&def);
+    if (!cfg) cfg = &def;
+    int rc = validate(cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SPH3_ERR_NO_DEVICE;
+    }
+    if (device < 0) CK(cudaGetDevice(&device));
+    if (device >= ndev) return SPH3_ERR_INVALID_ARG;
+    CK(cudaSetDevice(device));
+    sph3_ctx *c = new (std::nothrow) sph3_ctx();
+    if (!c) return SPH3_ERR_OUT_OF_MEMORY;
+    c->cfg = *cfg;
+    c->device = device;
+    params_from(*cfg, c->P);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete c;
+        return SPH3_ERR_CUDA;
+    }
+    c->S.num_sms = prop.multiProcessorCount;
+    c->S.walk_blocks = prop.multiProcessorCount * 8;
+    c->S.max_level = cfg->max_level;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return SPH3_ERR_CUDA;
+    }
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    if (cudaMalloc(&c->S.status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&c->S.counters, sizeof(unsigned long long) * 8) != cudaSuccess ||
+        cudaMalloc(&c->S.work, sizeof(int) * 8) != cudaSuccess ||
+        cudaMalloc(&c->S.energy_part, sizeof(double) * 8 * 512) != cudaSuccess ||
+        cudaMalloc(&c->S.energy, sizeof(double) * 8) != cudaSuccess) {
+        sph3_ctx_destroy(c);
+        return SPH3_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemset(c->S.status, 0, sizeof(unsigned));
+    cudaMemset(c->S.counters, 0, sizeof(unsigned long long) * 8);
+    cudaMemset(c->S.energy, 0, sizeof(double) * 8);
+    *out = c;
+    return SPH3_OK;
+}
+
+int sph3_ctx_destroy(sph3_ctx *c) {
+    if (!c) return SPH3_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    free_buffers(c);
+    State &S = c->S;
+    if (S.status) cudaFree(S.status);
+    if (S.counters) cudaFree(S.counters);
+    if (S.work) cudaFree(S.work);
+    if (S.energy_part) cudaFree(S.energy_part);
+    if (S.energy) cudaFree(S.energy);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SPH3_OK;
+}
+
+int sph3_set_config(sph3_ctx *c, const sph3_config *cfg) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    int rc = validate(cfg);
+    if (rc) return rc;
+    const bool relevel = cfg->max_level != c->cfg.max_level || cfg->leaf_size != c->cfg.leaf_size ||
+                         cfg->theta != c->cfg.theta || cfg->quadrupole != c->cfg.quadrupole;
+    if (cfg->max_level != c->cfg.max_level && c->have) {
+        int cb = 0;
+        while ((1ll << cb) < (int64_t)c->S.ncloud) ++cb;
+        if (3 * cfg->max_level + cb > 63) return SPH3_ERR_INVALID_ARG;
+    }
+    c->cfg = *cfg;
+    params_from(*cfg, c->P);
+    drop_graphs(c);
+    if (relevel && c->have) {
+        cudaSetDevice(c->device);
+        c->S.max_level = cfg->max_level;
+        int cb = 0;
+        while ((1ll << cb) < (int64_t)c->S.ncloud) ++cb;
+        c->S.cloud_bits = cb;
+        c->S.key_bits = 3 * cfg->max_level + cb;
+        return resort_all(c, c->stream) ? SPH3_ERR_CUDA : cuda_err(cudaStreamSynchronize(c->stream));
+    }
+    c->S.max_level = cfg->max_level;
+    return SPH3_OK;
+}
+
+int sph3_get_config(const sph3_ctx *c, sph3_config *cfg) {
+    if (!c || !cfg) return SPH3_ERR_INVALID_ARG;
+    *cfg = c->cfg;
+    return SPH3_OK;
+}
+
+int sph3_set_clouds(sph3_ctx *c, const int64_t *counts, int32_t ncloud) {
+    if (!c || ncloud < 1 || !counts) return SPH3_ERR_INVALID_ARG;
+    for (int k = 0; k < ncloud; ++k)
+        if (counts[k] < 0) return SPH3_ERR_INVALID_ARG;
+    c->cloud_counts.assign(counts, counts + ncloud);
+    return SPH3_OK;
+}
+
+int64_t sph3_num_particles(const sph3_ctx *c) { return c ? c->S.n : -1; }
+
+int sph3_set_particles(sph3_ctx *c, int64_t n, const double *pos, const double *vel, const double *mass,
+                       const double *u, const double *h, const double *eps, int on_device, void *stream) {
+    if (!c || n < 0 || (n > 0 && (!pos || !mass))) return SPH3_ERR_INVALID_ARG;
+    if (n > (int64_t)INT32_MAX / 2 - 1024) return SPH3_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    // cloud layout
+    std::vector<int64_t> counts = c->cloud_counts;
+    if (counts.empty()) counts.push_back(n);
+    int64_t tot = 0;
+    for (auto k : counts) tot += k;
+    if (tot != n) return SPH3_ERR_INVALID_ARG;
+    const int ncloud = (int)counts.size();
+    int cb = 0;
+    while ((1ll << cb) < (int64_t)ncloud) ++cb;
+    if (3 * c->cfg.max_level + cb > 63) return SPH3_ERR_INVALID_ARG;
+    std::vector<Cloud> cl(ncloud);
+    std::vector<int2> groups;
+    std::vector<int> gcl;
+    int64_t at = 0;
+    for (int k = 0; k < ncloud; ++k) {
+        std::memset(&cl[k], 0, sizeof(Cloud));
+        cl[k].begin = at;
+        cl[k].end = at + counts[k];
+        for (int64_t g = at; g < at + counts[k]; g += kGroup) {
+            groups.push_back(make_int2((int)g, (int)std::min<int64_t>(kGroup, at + counts[k] - g)));
+            gcl.push_back(k);
+        }
+        at += counts[k];
+    }
+    drop_graphs(c);
+    int rc = alloc_for(c, n, ncloud, (int)groups.size());
+    if (rc) return rc;
+    State &S = c->S;
+    S.n = n;
+    S.ncloud = ncloud;
+    S.ngroups = (int)groups.size();
+    S.cloud_bits = cb;
+    S.max_level = c->cfg.max_level;
+    S.key_bits = 3 * c->cfg.max_level + cb;
+    c->cur_counts = counts;
+    CK(cudaMemcpyAsync(S.clouds, cl.data(), sizeof(Cloud) * ncloud, cudaMemcpyHostToDevice, st));
+    if (!groups.empty()) {
+        CK(cudaMemcpyAsync(S.groups, groups.data(), sizeof(int2) * groups.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.group_cloud, gcl.data(), sizeof(int) * gcl.size(), cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemsetAsync(S.status, 0, sizeof(unsigned), st));
+    CK(cudaMemsetAsync(c->fixed, 0, sizeof(double) * kFixed * std::max<int64_t>(n, 1), st));
+    CK(cudaMemsetAsync(c->carried[c->cur], 0, sizeof(double) * kCarried * std::max<int64_t>(n, 1), st));
+    if (n > 0) {
+        k_iota64<<<blocks_for(c, n), 256, 0, st>>>(S.orig, n);
+        const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        auto put = [&](const double *src, double *dst, int ncomp) -> int {
+            CK(cudaMemcpyAsync(c->staging, src, sizeof(double) * n * ncomp, kind, st));
+            k_scatter_in<<<blocks_for(c, n), 256, 0, st>>>(c->staging, dst, S.orig, n, ncomp);
+            return check_launch();
+        };
+        if ((rc = put(pos, S.pos, 3))) return rc;
+        if ((rc = put(mass, S.m, 1))) return rc;
+        if (vel && (rc = put(vel, S.vel, 3))) return rc;
+        if (u && (rc = put(u, S.u, 1))) return rc;
+        if (u) CK(cudaMemcpyAsync(S.u_prev, S.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        if (h && (rc = put(h, S.h, 1))) return rc;
+        if (eps) {
+            if ((rc = put(eps, S.eps, 1))) return rc;
+        } else {
+            k_fill<<<blocks_for(c, n), 256, 0, st>>>(S.eps, n, c->cfg.eps);
+        }
+        launch_check_finite(S, st);
+    }
+    c->have = true;
+    rc = resort_all(c, st);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_set_field(sph3_ctx *c, int field, const double *src, int on_device, void *stream) {
+    if (!c || !src) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int ncomp;
+    double *dst = field_ptr(c, field, &ncomp);
+    if (!dst) return SPH3_ERR_INVALID_ARG;
+    const int64_t n = c->S.n;
+    if (n == 0) return SPH3_OK;
+    drop_graphs(c);
+    CK(cudaMemcpyAsync(c->staging, src, sizeof(double) * n * ncomp,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    k_scatter_in<<<blocks_for(c, n), 256, 0, st>>>(c->staging, dst, c->S.orig, n, ncomp);
+    int rc = check_launch();
+    if (rc) return rc;
+    switch (field) {
+        case SPH3_FIELD_POS:
+            rc = resort_all(c, st);
+            if (rc) return rc;
+            break;
+        case SPH3_FIELD_VEL: c->pack_dirty |= kPackVel; break;
+        case SPH3_FIELD_MASS:
+        case SPH3_FIELD_EPS: c->pack_dirty |= kPackHme; c->tree_dirty = true; break;
+        case SPH3_FIELD_H: c->pack_dirty |= kPackHme; c->h_dirty_tree = true; c->bal_dirty = true; break;
+        case SPH3_FIELD_RHO:
+        case SPH3_FIELD_P: c->pack_dirty |= kPackThm; break;
+        case SPH3_FIELD_C:
+        case SPH3_FIELD_DIVV:
+        case SPH3_FIELD_CURLV: c->pack_dirty |= kPackThm; c->bal_dirty = true; break;
+        case SPH3_FIELD_BALSARA: c->pack_dirty |= kPackThm; break;
+        default: break;
+    }
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_get_field(sph3_ctx *c, int field, double *dst, int64_t row_begin, int64_t row_end, int on_device,
+                   void *stream) {
+    if (!c || (!dst && row_end > row_begin)) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    const int64_t n = c->S.n;
+    if (row_begin < 0 || row_end > n || row_begin > row_end) return SPH3_ERR_INVALID_ARG;
+    if (row_end == row_begin) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int rc = ensure_inv(c, st);
+    if (rc) return rc;
+    const int64_t cnt = row_end - row_begin;
+    int ncomp = 1;
+    if (field == SPH3_FIELD_NNGB) {
+        k_gather_out_int<<<blocks_for(c, cnt), 256, 0, st>>>(c->S.nngb, c->staging, c->inv, row_begin, row_end);
+    } else {
+        double *src = field_ptr(c, field, &ncomp);
+        if (!src) return SPH3_ERR_INVALID_ARG;
+        k_gather_out<<<blocks_for(c, cnt), 256, 0, st>>>(src, c->staging, c->inv, n, ncomp, row_begin, row_end);
+    }
+    rc = check_launch();
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(dst, c->staging, sizeof(double) * cnt * ncomp,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    if (!on_device) CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    State &S = c->S;
+    const Params &P = c->P;
+    if (S.n == 0) return SPH3_OK;
+    if ((what & SPH3_DO_GRAVITY) && P.periodic) return SPH3_ERR_UNSUPPORTED;
+    int rc = sync_packs(c, st);
+    if (rc) return rc;
+    if (what & SPH3_DO_BOOT_H) {
+        launch_boot_h(S, P, st);
+        c->h_dirty_tree = true;
+        c->bal_dirty = true;
+    }
+    if (what & SPH3_DO_H) {
+        launch_h_search(S, P, st);
+        c->h_dirty_tree = true;
+        c->bal_dirty = true;
+    }
+    if ((rc = sync_packs(c, st))) return rc;
+    if (what & SPH3_DO_DENSITY) {
+        launch_density(S, P, (what & SPH3_DO_DIVCURL) != 0, st);
+        c->bal_dirty = false;
+    } else if (what & SPH3_DO_DIVCURL) {
+        // div/curl alone (div_curlVel): keep the stored rho, P, c
+        launch_density(S, P, true, st, true);
+        c->bal_dirty = false;
+    }
+    if (what & SPH3_DO_EOS) {
+        launch_eos(S, P, st);
+        c->bal_dirty = false;
+    }
+    if ((rc = sync_packs(c, st))) return rc;
+    if (what & SPH3_DO_GRAVITY) launch_gravity(S, P, st);
+    if (what & (SPH3_DO_ACC_SPH | SPH3_DO_DUDT))
+        launch_hydro(S, P, (what & SPH3_DO_ACC_SPH) != 0, (what & SPH3_DO_DUDT) != 0, st);
+    rc = check_launch();
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_first_step(sph3_ctx *c, double dt, void *stream) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    State &S = c->S;
+    const Params &P = c->P;
+    if (S.n == 0) return SPH3_OK;
+    int rc = sync_packs(c, st);
+    if (rc) return rc;
+    // bootstrap h where none was given (h <= 0 everywhere is the signal)
+    std::vector<double> h0(1);
+    CK(cudaMemcpyAsync(h0.data(), S.h, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!(h0[0] > 0.0)) launch_boot_h(S, P, st);
+    launch_h_search(S, P, st);
+    launch_tree_refit_h(S, st);
+    launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
+    if (P.gravity) launch_gravity(S, P, st);
+    else cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st);
+    launch_hydro(S, P, true, true, st);
+    launch_first_u(S, P, dt, st);
+    launch_energy(S, P, st);
+    c->h_dirty_tree = false;
+    c->bal_dirty = false;
+    rc = check_launch();
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
+    if (!c || nsteps < 0) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    State &S = c->S;
+    if (S.n == 0) return SPH3_OK;
+    int rc = sync_packs(c, st);
+    if (rc) return rc;
+    if (!c->P.gravity) cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st);
+    const bool serial = c->P.step_order == SPH3_ORDER_SERIAL;
+    for (int s = 0; s < nsteps; ++s) {
+        const bool graph_ok = c->cfg.use_graph && !c->cfg.timing && c->warm_steps >= 2;
+        if (!graph_ok) {
+            enqueue_step(c, dt, st);
+            rc = check_launch();
+            if (rc) return rc;
+            if (c->cfg.timing) {
+                CK(cudaEventSynchronize(c->ev[11]));
+                accumulate_times(c, serial);
+            }
+            ++c->warm_steps;
+            continue;
+        }
+        const int par = c->cur;
+        if (c->graph[par] && c->graph_dt[par] != dt) {
+            cudaGraphExecDestroy(c->graph[par]);
+            c->graph[par] = nullptr;
+        }
+        if (!c->graph[par]) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(c, dt, st);
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess) return SPH3_ERR_CUDA;
+            e = cudaGraphInstantiate(&c->graph[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return SPH3_ERR_CUDA;
+            c->graph_dt[par] = dt;
+            // capture switched the carried block without running: switch back
+            c->cur = par;
+            point_carried(c);
+        }
+        CK(cudaGraphLaunch(c->graph[par], st));
+        c->cur = par ^ 1;
+        point_carried(c);
+        c->inv_valid = false;
+    }
+    return SPH3_OK;
+}
+
+int sph3_energy(sph3_ctx *c, double out[8], void *stream) {
+    if (!c || !out) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    launch_energy(c->S, c->P, st);
+    CK(cudaMemcpyAsync(out, c->S.energy, sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_status(sph3_ctx *c, uint32_t *status, int clear) {
+    if (!c || !status) return SPH3_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaDeviceSynchronize());
+    unsigned v = 0;
+    CK(cudaMemcpy(&v, c->S.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (clear) CK(cudaMemset(c->S.status, 0, sizeof(unsigned)));
+    *status = v;
+    return SPH3_OK;
+}
+
+static int rows_to_sorted(sph3_ctx *c, const int64_t *rows, int64_t nrows, std::vector<int64_t> &sorted) {
+    cudaStream_t st = c->stream;
+    int rc = ensure_inv(c, st);
+    if (rc) return rc;
+    std::vector<int64_t> inv(c->S.n);
+    CK(cudaMemcpyAsync(inv.data(), c->inv, sizeof(int64_t) * c->S.n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    sorted.resize(nrows);
+    for (int64_t r = 0; r < nrows; ++r) {
+        if (rows[r] < 0 || rows[r] >= c->S.n) return SPH3_ERR_INVALID_ARG;
+        sorted[r] = inv[rows[r]];
+    }
+    return SPH3_OK;
+}
+
+int sph3_gravity_direct_rows(sph3_ctx *c, const int64_t *rows, int64_t nrows, double *acc, double *phi) {
+    if (!c || nrows < 0 || (nrows > 0 && (!rows || !acc))) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    if (nrows == 0) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    std::vector<int64_t> srt;
+    int rc = rows_to_sorted(c, rows, nrows, srt);
+    if (rc) return rc;
+    cudaStream_t st = c->stream;
+    int64_t *drows = nullptr;
+    double *dacc = nullptr, *dphi = nullptr;
+    CK(cudaMalloc(&drows, sizeof(int64_t) * nrows));
+    CK(cudaMalloc(&dacc, sizeof(double) * 3 * nrows));
+    CK(cudaMalloc(&dphi, sizeof(double) * nrows));
+    CK(cudaMemcpyAsync(drows, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
+    launch_gravity_direct(c->S, c->P, drows, nrows, dacc, dphi, st);
+    rc = check_launch();
+    if (!rc) {
+        CK(cudaMemcpyAsync(acc, dacc, sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, st));
+        if (phi) CK(cudaMemcpyAsync(phi, dphi, sizeof(double) * nrows, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    cudaFree(drows);
+    cudaFree(dacc);
+    cudaFree(dphi);
+    return rc;
+}
+
+int sph3_neighbours(sph3_ctx *c, const int64_t *rows, int64_t nrows, int64_t *offsets, int64_t *idx, int64_t cap) {
+    if (!c || nrows < 0 || !offsets || (nrows > 0 && !rows) || cap < 0 || (cap > 0 && !idx))
+        return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    offsets[0] = 0;
+    if (nrows == 0) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    int rc = sync_packs(c, st);
+    if (rc) return rc;
+    std::vector<int64_t> srt;
+    rc = rows_to_sorted(c, rows, nrows, srt);
+    if (rc) return rc;
+    int64_t *drows = nullptr, *doff = nullptr, *didx = nullptr;
+    CK(cudaMalloc(&drows, sizeof(int64_t) * nrows));
+    CK(cudaMalloc(&doff, sizeof(int64_t) * (nrows + 1)));
+    CK(cudaMalloc(&didx, sizeof(int64_t) * std::max<int64_t>(cap, 1)));
+    CK(cudaMemcpyAsync(drows, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
+    launch_neighbours(c->S, c->P, drows, nrows, doff, didx, cap, st);
+    rc = check_launch();
+    if (!rc) {
+        CK(cudaMemcpyAsync(offsets, doff, sizeof(int64_t) * (nrows + 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const int64_t tot = std::min(offsets[nrows], cap);
+        if (tot > 0) CK(cudaMemcpy(idx, didx, sizeof(int64_t) * tot, cudaMemcpyDeviceToHost));
+        for (int64_t r = 0; r < nrows; ++r) {
+            const int64_t b = std::min(offsets[r], cap), e = std::min(offsets[r + 1], cap);
+            std::sort(idx + b, idx + e);
+        }
+    }
+    cudaFree(drows);
+    cudaFree(doff);
+    cudaFree(didx);
+    return rc;
+}
+
+int sph3_morton_order(sph3_ctx *c, int64_t *order, uint64_t *keys) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    if (c->S.n == 0) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (order) CK(cudaMemcpy(order, c->S.orig, sizeof(int64_t) * c->S.n, cudaMemcpyDeviceToHost));
+    if (keys) CK(cudaMemcpy(keys, c->S.key, sizeof(uint64_t) * c->S.n, cudaMemcpyDeviceToHost));
+    return SPH3_OK;
+}
+
+int sph3_counters(sph3_ctx *c, int64_t out[8], int clear) {
+    if (!c || !out) return SPH3_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned long long v[8];
+    CK(cudaMemcpy(v, c->S.counters, sizeof(v), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 8; ++k) out[k] = (int64_t)v[k];
+    if (clear) CK(cudaMemset(c->S.counters, 0, sizeof(v)));
+    return SPH3_OK;
+}
+
+int sph3_phase_times(sph3_ctx *c, double out[9], int clear) {
+    if (!c || !out) return SPH3_ERR_INVALID_ARG;
+    for (int k = 0; k < 9; ++k) out[k] = c->phase_ms[k];
+    if (clear)
+        for (double &v : c->phase_ms) v = 0;
+    return SPH3_OK;
+}
+
+}  // extern "C"

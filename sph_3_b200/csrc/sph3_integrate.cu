@@ -1,0 +1,186 @@
+// Leapfrog kick-drift-kick, the trapezoidal u update and the FP64 global sums.
+// All FP64 (the time-integration accumulators), all HBM-bound streaming.
+//
+// Step order of the reference serial driver (sph_code/sph_serial.py:142-193):
+//   v += a dt/2; r += v dt                       -> k_kick_drift
+//   h, rho, a_g, P, c, du/dt(v_half)             -> walks
+//   u = u_prev + dt/2 (ut + ut_prev)             -> k_kick_update (update_u)
+//   a_sph; a = a_g + a_sph; v += a dt/2          -> k_kick_update (second_kick)
+// The MPI driver (sph_code/sph_mpi4_v4.py:380-427) kicks first and computes
+// du/dt with the full-step v; both orders are available.
+#include "sph3_internal.cuh"
+
+namespace sph3 {
+
+static int grid_for(const State &S, int64_t n) {
+    return (int)std::min<int64_t>((n + 255) / 256, (int64_t)S.num_sms * 8);
+}
+
+__global__ void k_kick_drift(int64_t n, double dt, double *pos, double *vel, const double *acc,
+                             double Lx, double Ly, double Lz) {
+    const double L[3] = {Lx, Ly, Lz};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            // v + acc * dt / 2.0 and r + v * dt, rounded as NumPy does (no FMA)
+            double v = __dadd_rn(vel[d * n + i], __dmul_rn(__dmul_rn(acc[d * n + i], dt), 0.5));
+            double x = __dadd_rn(pos[d * n + i], __dmul_rn(v, dt));
+            if (L[d] > 0.0) {
+                if (x < 0.0) x += L[d];
+                if (x >= L[d]) x -= L[d];
+            }
+            vel[d * n + i] = v;
+            pos[d * n + i] = x;
+        }
+    }
+}
+
+void launch_kick_drift(State &S, const Params &P, double dt, cudaStream_t st) {
+    if (S.n == 0) return;
+    k_kick_drift<<<grid_for(S, S.n), 256, 0, st>>>(S.n, dt, S.pos, S.vel, S.acc, P.box[0], P.box[1], P.box[2]);
+}
+
+__global__ void k_kick_update(int64_t n, double dt, int update_u, int second_kick, double *u,
+                              double *u_prev, const double *dudt, double *dudt_prev, double *acc,
+                              const double *acc_g, const double *acc_sph, double *vel, float4 *pk_vel) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (update_u) {
+            const double ut = dudt[i];
+            const double un = __dadd_rn(u_prev[i], __dmul_rn(__dmul_rn(0.5, dt), __dadd_rn(ut, dudt_prev[i])));
+            u[i] = un;
+            u_prev[i] = un;
+            dudt_prev[i] = ut;
+        }
+        if (second_kick) {
+            float v3[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double a = acc_g[d * n + i] + acc_sph[d * n + i];
+                acc[d * n + i] = a;
+                const double v = __dadd_rn(vel[d * n + i], __dmul_rn(__dmul_rn(a, dt), 0.5));
+                vel[d * n + i] = v;
+                v3[d] = (float)v;
+            }
+            pk_vel[i] = make_float4(v3[0], v3[1], v3[2], 0.f);
+        }
+    }
+}
+
+void launch_kick_update(State &S, const Params &P, double dt, bool update_u, bool second_kick,
+                        cudaStream_t st) {
+    (void)P;
+    if (S.n == 0) return;
+    k_kick_update<<<grid_for(S, S.n), 256, 0, st>>>(S.n, dt, update_u, second_kick, S.u, S.u_prev, S.dudt,
+                                                   S.dudt_prev, S.acc, S.acc_g, S.acc_sph, S.vel, S.pk_vel);
+}
+
+void launch_u_update(State &S, const Params &P, double dt, cudaStream_t st) {
+    launch_kick_update(S, P, dt, true, false, st);
+}
+
+// first step (sph_serial.py:123-134): a = a_g + a_sph; u += du/dt dt;
+// u_prev = u; dudt_prev = du/dt
+__global__ void k_first_u(int64_t n, double dt, double *u, double *u_prev, const double *dudt,
+                          double *dudt_prev, double *acc, const double *acc_g, const double *acc_sph) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) acc[d * n + i] = acc_g[d * n + i] + acc_sph[d * n + i];
+        const double un = __dadd_rn(u[i], __dmul_rn(dudt[i], dt));
+        u[i] = un;
+        u_prev[i] = un;
+        dudt_prev[i] = dudt[i];
+    }
+}
+
+void launch_first_u(State &S, const Params &P, double dt, cudaStream_t st) {
+    (void)P;
+    if (S.n == 0) return;
+    k_first_u<<<grid_for(S, S.n), 256, 0, st>>>(S.n, dt, S.u, S.u_prev, S.dudt, S.dudt_prev, S.acc, S.acc_g,
+                                               S.acc_sph);
+}
+
+__global__ void k_sum_acc(int64_t n, double *acc, const double *acc_g, const double *acc_sph) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * n; i += (int64_t)gridDim.x * blockDim.x)
+        acc[i] = acc_g[i] + acc_sph[i];
+}
+
+void launch_sum_acc(State &S, cudaStream_t st) {
+    if (S.n == 0) return;
+    k_sum_acc<<<grid_for(S, 3 * S.n), 256, 0, st>>>(S.n, S.acc, S.acc_g, S.acc_sph);
+}
+
+// ------------------------------------------------------------ energy
+// Deterministic two-stage FP64 reduction: each of kEnergyBlocks blocks sums a
+// fixed contiguous chunk, one block adds the partials in order.
+constexpr int kEnergyBlocks = 296;
+
+__global__ void __launch_bounds__(256) k_energy_part(int64_t n, const double *vel, const double *m,
+                                                     const double *u, const double *phi, double *part) {
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t beg = (int64_t)blockIdx.x * chunk;
+    const int64_t end = min(beg + chunk, n);
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        const double mi = m[i];
+        const double vx = vel[i], vy = vel[n + i], vz = vel[2 * n + i];
+        s[0] += 0.5 * mi * (vx * vx + vy * vy + vz * vz);
+        s[1] += mi * u[i];
+        s[2] += 0.5 * mi * phi[i];
+        s[4] += mi * vx;
+        s[5] += mi * vy;
+        s[6] += mi * vz;
+        s[7] += mi;
+    }
+    __shared__ double red[8][8];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double v = warp_sum(s[q]);
+        if (lane == 0) red[q][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double t = 0;
+        for (int k = 0; k < 8; ++k) t += red[threadIdx.x][k];
+        part[blockIdx.x * 8 + threadIdx.x] = t;
+    }
+}
+
+__global__ void k_energy_final(const double *part, int nb, double *out) {
+    if (threadIdx.x < 8) {
+        double t = 0;
+        for (int b = 0; b < nb; ++b) t += part[b * 8 + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) out[3] = out[0] + out[1] + out[2];
+}
+
+void launch_energy(State &S, const Params &P, cudaStream_t st) {
+    (void)P;
+    if (S.n == 0) {
+        cudaMemsetAsync(S.energy, 0, sizeof(double) * 8, st);
+        return;
+    }
+    k_energy_part<<<kEnergyBlocks, 256, 0, st>>>(S.n, S.vel, S.m, S.u, S.phi, S.energy_part);
+    k_energy_final<<<1, 32, 0, st>>>(S.energy_part, kEnergyBlocks, S.energy);
+}
+
+// non-finite velocity, mass, u or h -> SPH3_STATUS_NAN_INPUT (positions are
+// checked while the root cubes are computed)
+__global__ void k_check_finite(int64_t n, const double *vel, const double *m, const double *u,
+                               const double *h, unsigned *status) {
+    int bad = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        bad |= !isfinite(vel[i]) | !isfinite(vel[n + i]) | !isfinite(vel[2 * n + i]);
+        bad |= !isfinite(m[i]) | !isfinite(u[i]) | !isfinite(h[i]);
+    }
+    if (__any_sync(kFull, bad) && (threadIdx.x & 31) == 0) atomicOr(status, SPH3_STATUS_NAN_INPUT);
+}
+
+void launch_check_finite(State &S, cudaStream_t st) {
+    if (S.n == 0) return;
+    k_check_finite<<<grid_for(S, S.n), 256, 0, st>>>(S.n, S.vel, S.m, S.u, S.h, S.status);
+}
+
+}  // namespace sph3

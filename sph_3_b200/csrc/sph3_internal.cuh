@@ -1,0 +1,269 @@
+// Internal definitions shared by the CUDA translation units of libsph3.
+//
+// Data layout in HBM (all arrays indexed by the Morton-sorted position k,
+// particles of one cloud contiguous, clouds in input order):
+//   FP64 masters, component-major ([3][n] for vectors):  pos, vel, acc,
+//     acc_g, acc_sph, u, u_prev, dudt, dudt_prev, m, h, eps, rho, P, c,
+//     divV, curlV, bal, phi                                (the state)
+//   FP32 packs for the mixed-precision walks:
+//     pk_pos   float4 {x - corner, y - corner, z - corner, cell}  where
+//              corner is the corner of the particle's level-10 cell of its
+//              cloud's root cube and cell = ix | iy << 10 | iz << 20
+//     pk_hme   float4 {h, m, eps, 0}
+//     pk_vel   float4 {vx, vy, vz, 0}
+//     pk_thm   float4 {rho, P / rho^2, c, Balsara f}
+//   keys (uint64: cloud id above 3 * max_level Morton bits), orig (int64:
+//   the caller's index of the sorted particle).
+// Octree (compressed: every internal node has 2..8 children, which are
+// stored contiguously; nodes laid out depth by depth):
+//   nd_range int2 {first particle, count}, nd_child int2 {first child,
+//   nchild | level << 8} (nchild 0 = leaf), FP64 moments and FP32 packs
+//   (bbox centre, half size + hmax, centre of mass, mass / opening radii,
+//   traceless quadrupole).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/sph3.h"
+
+namespace sph3 {
+
+constexpr int kWarp = 32;
+constexpr int kGroup = 32;        // target particles per walk group (one warp)
+constexpr int kCellBits = 10;     // level of the FP32 cell-relative frame
+constexpr int kWalkWarps = 4;     // warps per walk block
+constexpr int kLeafQ = 96;        // queued leaves per warp before a flush
+constexpr int kNodeQ = 64;        // queued multipole nodes per warp (gravity)
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------ per cloud
+struct Cloud {
+    int64_t begin, end;  // sorted particle range
+    double origin[3];    // root cube corner
+    double size;         // root cube edge (power of two)
+    double inv_cell;     // 2^max_level / size
+    float s10;           // size / 1024 (exact power of two)
+    int root;            // root node id
+};
+
+// ------------------------------------------------------------ tree view
+struct Tree {
+    int2 *range;        // {first, count}
+    int2 *child;        // {first child, nchild | level << 8}
+    // FP64 moments
+    double *mass;       // [cap]
+    double *com;        // [3][cap]
+    double *bmin;       // [3][cap]
+    double *bmax;       // [3][cap]
+    double *hmax;       // [cap]
+    double *epsmax;     // [cap]
+    double *quad;       // [6][cap] xx xy xz yy yz zz (traceless)
+    // FP32 packs for the walks
+    float4 *box_c;      // {centre - corner, cell}
+    float4 *box_h;      // {half extents, hmax}
+    float4 *com_c;      // {com - corner, cell}
+    float4 *mono;       // {mass, r_open, r_soft (bmax + epsmax), 0}
+    float4 *quad4;      // {xx, xy, xz, yy}
+    float *quad1;       // {yz}
+    int cap;
+    int *depth_begin;   // [max_depth + 2] node id where each depth starts
+    int *nchild_tmp;    // [cap] scan input
+    int *scan_tmp;      // [cap] scan output
+    int *total;         // [4] scratch counters
+};
+
+// ------------------------------------------------------------ state
+struct State {
+    int64_t n = 0;
+    int ncloud = 0;
+    int ngroups = 0;
+    Cloud *clouds = nullptr;  // device [ncloud]
+    int2 *groups = nullptr;   // device [ngroups] {first, count}
+    int *group_cloud = nullptr;
+    // FP64 masters
+    double *pos = nullptr, *vel = nullptr, *acc = nullptr, *acc_g = nullptr, *acc_sph = nullptr;
+    double *u = nullptr, *u_prev = nullptr, *dudt = nullptr, *dudt_prev = nullptr;
+    double *m = nullptr, *h = nullptr, *eps = nullptr, *rho = nullptr, *P = nullptr, *c = nullptr;
+    double *divV = nullptr, *curlV = nullptr, *bal = nullptr, *phi = nullptr;
+    int *nngb = nullptr;
+    int64_t *orig = nullptr;
+    // keys / sort
+    uint64_t *key = nullptr, *key_alt = nullptr;
+    uint32_t *perm = nullptr, *perm_alt = nullptr;
+    // FP32 packs
+    float4 *pk_pos = nullptr, *pk_hme = nullptr, *pk_vel = nullptr, *pk_thm = nullptr;
+    Tree tree{};
+    // bookkeeping
+    unsigned *status = nullptr;        // device status word
+    unsigned long long *counters = nullptr;  // [8]
+    int *work = nullptr;               // [8] work-queue counters of the walks
+    double *energy_part = nullptr;     // per-block FP64 partial sums [nblk][8]
+    double *energy = nullptr;          // [8]
+    // scratch for the sort
+    uint32_t *sort_hist = nullptr;     // [256 * nblocks]
+    int sort_blocks = 0;
+    int key_bits = 0;
+    int max_level = 0;
+    int cloud_bits = 0;
+    // launch geometry
+    int num_sms = 0;
+    int walk_blocks = 0;
+};
+
+struct Params {
+    int precision, h_mode, visc, step_order, n_ngb, n_ngb_tol, h_max_iter, n_boot;
+    int leaf_size, stack_cap, max_level, gravity, quadrupole;
+    double gamma, alpha, beta, eta, G, theta, eps;
+    double box[3];
+    int periodic;
+};
+
+// ------------------------------------------------------------ device helpers
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(kFull, v, o);
+        v = v > w ? v : w;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(kFull, v, o);
+        v = v < w ? v : w;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// inclusive scan of ints across the warp
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    const int lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int w = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += w;
+    }
+    return v;
+}
+
+__device__ __forceinline__ void set_status(unsigned *status, unsigned bit) {
+    atomicOr(status, bit);
+}
+
+// Morton interleave of a 21-bit integer into every third bit
+__host__ __device__ __forceinline__ uint64_t spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+// Quantises one coordinate to [0, 2^L) on the cloud's root cube exactly as
+// the NumPy restatement does: floor((x - origin) * inv_cell), clamped.
+__host__ __device__ __forceinline__ uint32_t quantise(double x, double origin, double inv_cell,
+                                                      uint32_t maxq) {
+    double t = (x - origin) * inv_cell;
+    if (!(t > 0.0)) return 0u;  // also catches NaN
+    double f = floor(t);
+    if (f >= (double)maxq) return maxq;
+    return (uint32_t)f;
+}
+
+// level-10 cell of a point in its cloud's root cube, and the FP32 offset from
+// that cell's corner
+struct CellRel {
+    int cell;
+    float ox, oy, oz;
+};
+
+__device__ __forceinline__ CellRel make_cellrel(double x, double y, double z, const Cloud &cl) {
+    const double s = (double)cl.s10;
+    const double inv = 1.0 / s;  // power of two: exact
+    int ix = (int)floor((x - cl.origin[0]) * inv);
+    int iy = (int)floor((y - cl.origin[1]) * inv);
+    int iz = (int)floor((z - cl.origin[2]) * inv);
+    ix = min(max(ix, 0), 1023);
+    iy = min(max(iy, 0), 1023);
+    iz = min(max(iz, 0), 1023);
+    CellRel r;
+    r.cell = ix | (iy << 10) | (iz << 20);
+    r.ox = (float)((x - cl.origin[0]) - ix * s);
+    r.oy = (float)((y - cl.origin[1]) - iy * s);
+    r.oz = (float)((z - cl.origin[2]) - iz * s);
+    return r;
+}
+
+// position of a packed point relative to the corner of reference cell `ref`
+__device__ __forceinline__ float3 rel_to(float4 p, int ref, float s10) {
+    const int c = __float_as_int(p.w);
+    const int dx = (c & 1023) - (ref & 1023);
+    const int dy = ((c >> 10) & 1023) - ((ref >> 10) & 1023);
+    const int dz = (c >> 20) - (ref >> 20);
+    return make_float3(fmaf((float)dx, s10, p.x), fmaf((float)dy, s10, p.y),
+                       fmaf((float)dz, s10, p.z));
+}
+
+// ------------------------------------------------------------ launchers
+// sort.cu
+void launch_cloud_boxes(State &S, const Params &P, cudaStream_t st);
+void launch_keys(State &S, const Params &P, cudaStream_t st);
+void launch_radix_sort(State &S, cudaStream_t st);  // sorts key/perm in place (ends in key/perm)
+void launch_gather(State &S, const double *const *src, double *const *dst, int nfields,
+                   const int *ncomp, cudaStream_t st);
+void launch_gather_orig(State &S, const int64_t *src, int64_t *dst, cudaStream_t st);
+void launch_pack(State &S, const Params &P, unsigned which, cudaStream_t st);
+void launch_identity_perm(State &S, cudaStream_t st);
+// tree.cu
+void launch_tree_build(State &S, const Params &P, cudaStream_t st);
+void launch_tree_refit_h(State &S, cudaStream_t st);
+// walk_sph.cu
+void launch_boot_h(State &S, const Params &P, cudaStream_t st);
+void launch_h_search(State &S, const Params &P, cudaStream_t st);
+void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bool keep_rho = false);
+void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cudaStream_t st);
+void launch_eos(State &S, const Params &P, cudaStream_t st);
+int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
+                      int64_t *offsets_dev, int64_t *idx_dev, int64_t cap, cudaStream_t st);
+// walk_grav.cu
+void launch_gravity(State &S, const Params &P, cudaStream_t st);
+void launch_gravity_direct(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
+                           double *acc_dev, double *phi_dev, cudaStream_t st);
+// integrate.cu
+void launch_kick_drift(State &S, const Params &P, double dt, cudaStream_t st);
+void launch_kick_update(State &S, const Params &P, double dt, bool update_u, bool second_kick,
+                        cudaStream_t st);
+void launch_u_update(State &S, const Params &P, double dt, cudaStream_t st);
+void launch_first_u(State &S, const Params &P, double dt, cudaStream_t st);
+void launch_sum_acc(State &S, cudaStream_t st);
+void launch_energy(State &S, const Params &P, cudaStream_t st);
+void launch_check_finite(State &S, cudaStream_t st);
+
+// pack selectors for launch_pack
+constexpr unsigned kPackPos = 1, kPackHme = 2, kPackVel = 4, kPackThm = 8;
+
+}  // namespace sph3

@@ -1,0 +1,357 @@
+// Root cubes, Morton keys, LSD radix sort and the permutation gather.
+//
+// All of these are HBM/L2-bound integer and byte moves: coalesced loads,
+// grid sizes in multiples of the SM count, no tensor-core reshaping.
+#include <cfloat>
+
+#include "sph3_internal.cuh"
+
+namespace sph3 {
+
+// ------------------------------------------------------------ root cubes
+// One block per cloud: FP64 bbox of its particles (sorted range), then a
+// power-of-two cube [origin, origin + size) that contains them, with origin
+// on the size/2 grid.  Periodic runs use the fixed cube [0, 2^ceil(log2 L)).
+__global__ void k_cloud_boxes(Cloud *clouds, const double *pos, int64_t n, int max_level,
+                              int periodic, double Lx, double Ly, double Lz, unsigned *status) {
+    Cloud &cl = clouds[blockIdx.x];
+    __shared__ double smin[3][32], smax[3][32];
+    __shared__ int sbad;
+    if (threadIdx.x == 0) sbad = 0;
+    __syncthreads();
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    int bad = 0;
+    for (int64_t k = cl.begin + threadIdx.x; k < cl.end; k += blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double x = pos[d * n + k];
+            if (!isfinite(x)) {
+                bad = 1;
+                continue;
+            }
+            mn[d] = fmin(mn[d], x);
+            mx[d] = fmax(mx[d], x);
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double a = warp_min(mn[d]), b = warp_max(mx[d]);
+        if (lane == 0) {
+            smin[d][wid] = a;
+            smax[d][wid] = b;
+        }
+    }
+    if (bad) atomicOr(&sbad, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = DBL_MAX;
+            hi[d] = -DBL_MAX;
+            for (int w = 0; w < nw; ++w) {
+                lo[d] = fmin(lo[d], smin[d][w]);
+                hi[d] = fmax(hi[d], smax[d][w]);
+            }
+            if (lo[d] > hi[d]) lo[d] = hi[d] = 0.0;  // empty cloud
+        }
+        if (sbad) atomicOr(status, SPH3_STATUS_NAN_INPUT);
+        double size;
+        double org[3];
+        if (periodic) {
+            double L = fmax(Lx, fmax(Ly, Lz));
+            int e;
+            frexp(L, &e);  // L = f * 2^e, f in [0.5, 1)
+            size = ldexp(1.0, e);
+            if (size * 0.5 >= L) size *= 0.5;
+            org[0] = org[1] = org[2] = 0.0;
+        } else {
+            double ext = fmax(hi[0] - lo[0], fmax(hi[1] - lo[1], hi[2] - lo[2]));
+            if (!(ext > 0.0) || !isfinite(ext)) ext = 1.0;
+            int e;
+            frexp(ext, &e);
+            size = ldexp(1.0, e);  // >= ext
+            for (int attempt = 0; attempt < 64; ++attempt) {
+                double half = 0.5 * size;
+                bool ok = true;
+                for (int d = 0; d < 3; ++d) {
+                    org[d] = floor(lo[d] / half) * half;
+                    if (!(org[d] + size > hi[d])) ok = false;
+                }
+                if (ok) break;
+                size *= 2.0;
+            }
+        }
+        for (int d = 0; d < 3; ++d) cl.origin[d] = org[d];
+        cl.size = size;
+        cl.inv_cell = ldexp(1.0, max_level) / size;
+        cl.s10 = (float)(size / 1024.0);
+    }
+}
+
+void launch_cloud_boxes(State &S, const Params &P, cudaStream_t st) {
+    if (S.ncloud == 0) return;
+    k_cloud_boxes<<<S.ncloud, 256, 0, st>>>(S.clouds, S.pos, S.n, S.max_level, P.periodic,
+                                            P.box[0], P.box[1], P.box[2], S.status);
+}
+
+// ------------------------------------------------------------ keys
+__device__ __forceinline__ int cloud_of_sorted(const Cloud *clouds, int ncloud, int64_t k) {
+    int lo = 0, hi = ncloud - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (clouds[mid].begin <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_keys(const Cloud *clouds, int ncloud, const double *pos, int64_t n,
+                       int max_level, uint64_t *key, uint32_t *perm) {
+    const uint32_t maxq = (1u << max_level) - 1u;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int c = cloud_of_sorted(clouds, ncloud, k);
+        const Cloud &cl = clouds[c];
+        uint32_t ix = quantise(pos[k], cl.origin[0], cl.inv_cell, maxq);
+        uint32_t iy = quantise(pos[n + k], cl.origin[1], cl.inv_cell, maxq);
+        uint32_t iz = quantise(pos[2 * n + k], cl.origin[2], cl.inv_cell, maxq);
+        uint64_t mort = spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2);
+        key[k] = ((uint64_t)c << (3 * max_level)) | mort;
+        perm[k] = (uint32_t)k;
+    }
+}
+
+void launch_keys(State &S, const Params &P, cudaStream_t st) {
+    if (S.n == 0) return;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_keys<<<blocks, 256, 0, st>>>(S.clouds, S.ncloud, S.pos, S.n, S.max_level, S.key, S.perm);
+}
+
+__global__ void k_identity(uint32_t *perm, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        perm[k] = (uint32_t)k;
+}
+
+void launch_identity_perm(State &S, cudaStream_t st) {
+    if (S.n == 0) return;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_identity<<<blocks, 256, 0, st>>>(S.perm, S.n);
+}
+
+// ------------------------------------------------------------ radix sort
+// LSD, 8-bit digits, stable.  Per pass: a tile histogram, one scan of the
+// digit-major histogram table, and a stable scatter that ranks each key
+// within its tile with warp match (order = memory order inside a warp's
+// segment, then warp order).
+constexpr int kRsThreads = 256;
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys per block
+constexpr int kRsWarps = kRsThreads / 32;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t *key, int64_t n, int shift,
+                                                        uint32_t *hist, int nblocks) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kRsTile;
+#pragma unroll
+    for (int t = 0; t < kRsItems; ++t) {
+        int64_t k = base + t * kRsThreads + threadIdx.x;
+        if (k < n) atomicAdd(&h[(key[k] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan of m entries by one block of 1024 threads
+__global__ void __launch_bounds__(1024) k_scan_excl(uint32_t *a, int m) {
+    __shared__ uint32_t part[1024];
+    const int per = (m + 1023) / 1024;
+    const int beg = threadIdx.x * per;
+    const int end = min(beg + per, m);
+    uint32_t s = 0;
+    for (int i = beg; i < end; ++i) s += a[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    // Hillis-Steele over 1024 partial sums
+    for (int o = 1; o < 1024; o <<= 1) {
+        uint32_t v = threadIdx.x >= o ? part[threadIdx.x - o] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    for (int i = beg; i < end; ++i) {
+        uint32_t v = a[i];
+        a[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
+                                                           const uint32_t *val_in, uint64_t *key_out,
+                                                           uint32_t *val_out, int64_t n, int shift,
+                                                           const uint32_t *hist, int nblocks) {
+    __shared__ uint32_t wcnt[kRsWarps][256];
+    __shared__ uint32_t goff[256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
+    goff[threadIdx.x] = hist[threadIdx.x * nblocks + blockIdx.x];
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (kRsItems * 32);
+    uint64_t kk[kRsItems];
+    uint32_t vv[kRsItems];
+    uint32_t rank[kRsItems];
+    int dig[kRsItems];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int t = 0; t < kRsItems; ++t) {
+        int64_t k = base + t * 32 + lane;
+        bool ok = k < n;
+        kk[t] = ok ? key_in[k] : 0ull;
+        vv[t] = ok ? val_in[k] : 0u;
+        int d = ok ? (int)((kk[t] >> shift) & 255u) : 256;
+        dig[t] = d;
+        unsigned peers = __match_any_sync(kFull, d);
+        uint32_t b = d < 256 ? wcnt[w][d] : 0u;
+        __syncwarp();
+        if (d < 256 && (peers & lt) == 0) wcnt[w][d] = b + __popc(peers);
+        __syncwarp();
+        rank[t] = b + __popc(peers & lt);
+    }
+    __syncthreads();
+    // prefix over warps for each digit
+    {
+        const int d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int ww = 0; ww < kRsWarps; ++ww) {
+            uint32_t c = wcnt[ww][d];
+            wcnt[ww][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < kRsItems; ++t) {
+        int d = dig[t];
+        if (d < 256) {
+            uint32_t pos = goff[d] + wcnt[w][d] + rank[t];
+            key_out[pos] = kk[t];
+            val_out[pos] = vv[t];
+        }
+    }
+}
+
+void launch_radix_sort(State &S, cudaStream_t st) {
+    if (S.n <= 1) return;
+    const int nb = (int)((S.n + kRsTile - 1) / kRsTile);
+    const int passes = (S.key_bits + 7) / 8;
+    uint64_t *kin = S.key, *kout = S.key_alt;
+    uint32_t *vin = S.perm, *vout = S.perm_alt;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        k_rs_hist<<<nb, kRsThreads, 0, st>>>(kin, S.n, shift, S.sort_hist, nb);
+        k_scan_excl<<<1, 1024, 0, st>>>(S.sort_hist, 256 * nb);
+        k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kin, vin, kout, vout, S.n, shift, S.sort_hist, nb);
+        uint64_t *tk = kin;
+        kin = kout;
+        kout = tk;
+        uint32_t *tv = vin;
+        vin = vout;
+        vout = tv;
+    }
+    if (kin != S.key) {  // odd pass count: copy back so the result is in key/perm
+        cudaMemcpyAsync(S.key, kin, sizeof(uint64_t) * S.n, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(S.perm, vin, sizeof(uint32_t) * S.n, cudaMemcpyDeviceToDevice, st);
+    }
+}
+
+// ------------------------------------------------------------ gather
+constexpr int kMaxGather = 40;
+struct GatherArgs {
+    const double *src[kMaxGather];
+    double *dst[kMaxGather];
+    int nf;
+};
+
+__global__ void k_gather(const uint32_t *perm, GatherArgs a, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = perm[k];
+        for (int f = 0; f < a.nf; ++f) a.dst[f][k] = a.src[f][j];
+    }
+}
+
+void launch_gather(State &S, const double *const *src, double *const *dst, int nfields,
+                   const int *ncomp, cudaStream_t st) {
+    if (S.n == 0) return;
+    GatherArgs a;
+    a.nf = 0;
+    for (int f = 0; f < nfields; ++f) {
+        for (int c = 0; c < ncomp[f]; ++c) {
+            if (a.nf == kMaxGather) {
+                int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+                k_gather<<<blocks, 256, 0, st>>>(S.perm, a, S.n);
+                a.nf = 0;
+            }
+            a.src[a.nf] = src[f] + (int64_t)c * S.n;
+            a.dst[a.nf] = dst[f] + (int64_t)c * S.n;
+            ++a.nf;
+        }
+    }
+    if (a.nf) {
+        int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+        k_gather<<<blocks, 256, 0, st>>>(S.perm, a, S.n);
+    }
+}
+
+__global__ void k_gather_i64(const uint32_t *perm, const int64_t *src, int64_t *dst, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[perm[k]];
+}
+
+void launch_gather_orig(State &S, const int64_t *src, int64_t *dst, cudaStream_t st) {
+    if (S.n == 0) return;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_gather_i64<<<blocks, 256, 0, st>>>(S.perm, src, dst, S.n);
+}
+
+// ------------------------------------------------------------ packs
+__global__ void k_pack(const Cloud *clouds, const uint64_t *key, int max_level, int64_t n,
+                       const double *pos, const double *vel, const double *h, const double *m,
+                       const double *eps, const double *rho, const double *P, const double *c,
+                       const double *bal, float4 *pk_pos, float4 *pk_hme, float4 *pk_vel,
+                       float4 *pk_thm, unsigned which) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (which & kPackPos) {
+            const Cloud &cl = clouds[(int)(key[k] >> (3 * max_level))];
+            CellRel r = make_cellrel(pos[k], pos[n + k], pos[2 * n + k], cl);
+            pk_pos[k] = make_float4(r.ox, r.oy, r.oz, __int_as_float(r.cell));
+        }
+        if (which & kPackHme) pk_hme[k] = make_float4((float)h[k], (float)m[k], (float)eps[k], 0.f);
+        if (which & kPackVel)
+            pk_vel[k] = make_float4((float)vel[k], (float)vel[n + k], (float)vel[2 * n + k], 0.f);
+        if (which & kPackThm) {
+            double r = rho[k];
+            double pr = r > 0.0 ? P[k] / (r * r) : 0.0;
+            pk_thm[k] = make_float4((float)r, (float)pr, (float)c[k], (float)bal[k]);
+        }
+    }
+}
+
+void launch_pack(State &S, const Params &P, unsigned which, cudaStream_t st) {
+    if (S.n == 0 || which == 0) return;
+    (void)P;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_pack<<<blocks, 256, 0, st>>>(S.clouds, S.key, S.max_level, S.n, S.pos, S.vel, S.h, S.m,
+                                   S.eps, S.rho, S.P, S.c, S.bal, S.pk_pos, S.pk_hme, S.pk_vel,
+                                   S.pk_thm, which);
+}
+
+}  // namespace sph3

@@ -1,0 +1,323 @@
+// Linear octree from Morton-sorted keys, built top-down one depth at a time,
+// then moments bottom-up.
+//
+// A node is a contiguous run [first, first + count) of sorted particles whose
+// keys share a common prefix; its level is the deepest level whose cell holds
+// the whole run.  A node with more than leaf_size particles (and level below
+// max_level) is split on the next 3-bit digit into its 2..8 non-empty
+// sub-runs, found by binary search (digits are non-decreasing inside a run).
+// Single-child chains never appear, so nodes < 2 * particles.  Children of a
+// node are stored contiguously and each depth is compacted with an exclusive
+// scan, so the layout, and every sum over it, is deterministic.
+// Compared with the reference's pointer octree (bh_tree_iteration_v2.h:149-450:
+// one block, atomicCAS locks, a DFS sort that spins on its parent) there are
+// no locks and no waits.
+#include <cfloat>
+
+#include "sph3_internal.cuh"
+
+namespace sph3 {
+
+__device__ __forceinline__ int common_level(uint64_t a, uint64_t b, int max_level) {
+    uint64_t x = a ^ b;
+    if (x == 0) return max_level;
+    int hb = 63 - __clzll((long long)x);
+    return max_level - 1 - hb / 3;
+}
+
+__global__ void k_tree_roots(Tree T, Cloud *clouds, int ncloud, const uint64_t *key, int max_level) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c == 0) {
+        T.depth_begin[0] = 0;
+        T.depth_begin[1] = ncloud;
+    }
+    if (c >= ncloud) return;
+    Cloud &cl = clouds[c];
+    int first = (int)cl.begin, count = (int)(cl.end - cl.begin);
+    int lvl = count > 0 ? common_level(key[first], key[first + count - 1], max_level) : max_level;
+    T.range[c] = make_int2(first, count);
+    T.child[c] = make_int2(-1, lvl << 8);
+    cl.root = c;
+}
+
+// number of children of each node of depth d (0 for a leaf)
+__global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
+    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        int2 r = T.range[i];
+        int lvl = T.child[i].y >> 8;
+        int nch = 0;
+        if (r.y > leaf_size && lvl < max_level) {
+            const int shift = 3 * (max_level - lvl - 1);
+            int lo = r.x;
+            const int e = r.x + r.y;
+            int prev_digit = -1;
+            // walk the distinct digits by successive binary searches
+            while (lo < e) {
+                int dg = (int)((key[lo] >> shift) & 7u);
+                if (dg != prev_digit) ++nch;
+                prev_digit = dg;
+                // first index with digit > dg
+                int a = lo, b = e;
+                while (a < b) {
+                    int mid = (a + b) >> 1;
+                    if ((int)((key[mid] >> shift) & 7u) <= dg) a = mid + 1;
+                    else b = mid;
+                }
+                lo = a;
+            }
+        }
+        T.nchild_tmp[i - beg] = nch;
+    }
+}
+
+// exclusive scan of the child counts of depth d; sets depth_begin[d + 2]
+__global__ void __launch_bounds__(1024) k_tree_scan(Tree T, int d, unsigned *status) {
+    __shared__ int part[1024];
+    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    const int m = end - beg;
+    const int per = (m + 1023) / 1024;
+    const int b = threadIdx.x * per;
+    const int e = min(b + per, m);
+    int s = 0;
+    for (int i = b; i < e; ++i) s += T.nchild_tmp[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (int i = b; i < e; ++i) {
+        int v = T.nchild_tmp[i];
+        T.scan_tmp[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == 1023) {
+        int total = part[1023];
+        int next = end + total;
+        if (next > T.cap) {
+            atomicOr(status, SPH3_STATUS_TREE_CAPACITY);
+            next = end;  // emit nothing: the affected nodes stay leaves
+        }
+        T.depth_begin[d + 2] = next;
+    }
+}
+
+__global__ void k_tree_emit(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
+    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    const bool room = T.depth_begin[d + 2] > end || end == beg;
+    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const int nch = T.nchild_tmp[i - beg];
+        int lvl = T.child[i].y >> 8;
+        if (nch == 0 || !room) {
+            T.child[i] = make_int2(-1, lvl << 8);
+            continue;
+        }
+        const int cf = end + T.scan_tmp[i - beg];
+        T.child[i] = make_int2(cf, nch | (lvl << 8));
+        int2 r = T.range[i];
+        const int shift = 3 * (max_level - lvl - 1);
+        int lo = r.x, c = 0;
+        const int e = r.x + r.y;
+        while (lo < e && c < nch) {
+            int dg = (int)((key[lo] >> shift) & 7u);
+            int a = lo, b = e;
+            while (a < b) {
+                int mid = (a + b) >> 1;
+                if ((int)((key[mid] >> shift) & 7u) <= dg) a = mid + 1;
+                else b = mid;
+            }
+            const int cnt = a - lo;
+            const int cl = common_level(key[lo], key[a - 1], max_level);
+            T.range[cf + c] = make_int2(lo, cnt);
+            T.child[cf + c] = make_int2(-1, cl << 8);
+            ++c;
+            lo = a;
+        }
+    }
+}
+
+// ------------------------------------------------------------ moments
+struct MomArgs {
+    const double *pos, *m, *h, *eps;
+    int64_t n;
+    const Cloud *clouds;
+    const uint64_t *key;
+    int max_level;
+    double inv_theta;  // 1/theta (inf for theta = 0)
+};
+
+__global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
+    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    const int cap = T.cap;
+    const int64_t n = a.n;
+    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const int2 r = T.range[i];
+        const int2 ch = T.child[i];
+        const int nch = ch.y & 255;
+        double M = 0, sx = 0, sy = 0, sz = 0;
+        double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        double hm = 0, em = 0;
+        if (nch == 0) {
+            for (int k = r.x; k < r.x + r.y; ++k) {
+                const double mk = a.m[k];
+                const double x = a.pos[k], y = a.pos[n + k], z = a.pos[2 * n + k];
+                M += mk;
+                sx += mk * x;
+                sy += mk * y;
+                sz += mk * z;
+                lo[0] = fmin(lo[0], x); hi[0] = fmax(hi[0], x);
+                lo[1] = fmin(lo[1], y); hi[1] = fmax(hi[1], y);
+                lo[2] = fmin(lo[2], z); hi[2] = fmax(hi[2], z);
+                hm = fmax(hm, a.h[k]);
+                em = fmax(em, a.eps[k]);
+            }
+        } else {
+            for (int c = ch.x; c < ch.x + nch; ++c) {
+                const double mc = T.mass[c];
+                M += mc;
+                sx += mc * T.com[c];
+                sy += mc * T.com[cap + c];
+                sz += mc * T.com[2 * cap + c];
+                for (int q = 0; q < 3; ++q) {
+                    lo[q] = fmin(lo[q], T.bmin[q * cap + c]);
+                    hi[q] = fmax(hi[q], T.bmax[q * cap + c]);
+                }
+                hm = fmax(hm, T.hmax[c]);
+                em = fmax(em, T.epsmax[c]);
+            }
+        }
+        if (r.y == 0) {
+            lo[0] = lo[1] = lo[2] = 0.0;
+            hi[0] = hi[1] = hi[2] = 0.0;
+        }
+        double cx, cy, cz;
+        if (M > 0) {
+            cx = sx / M; cy = sy / M; cz = sz / M;
+        } else {
+            cx = 0.5 * (lo[0] + hi[0]); cy = 0.5 * (lo[1] + hi[1]); cz = 0.5 * (lo[2] + hi[2]);
+        }
+        T.mass[i] = M;
+        T.com[i] = cx; T.com[cap + i] = cy; T.com[2 * cap + i] = cz;
+        for (int q = 0; q < 3; ++q) {
+            T.bmin[q * cap + i] = lo[q];
+            T.bmax[q * cap + i] = hi[q];
+        }
+        T.hmax[i] = hm;
+        T.epsmax[i] = em;
+        double Q[6] = {0, 0, 0, 0, 0, 0};
+        if (quad) {
+            if (nch == 0) {
+                for (int k = r.x; k < r.x + r.y; ++k) {
+                    const double mk = a.m[k];
+                    const double dx = a.pos[k] - cx, dy = a.pos[n + k] - cy, dz = a.pos[2 * n + k] - cz;
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    Q[0] += mk * (3 * dx * dx - d2);
+                    Q[1] += mk * (3 * dx * dy);
+                    Q[2] += mk * (3 * dx * dz);
+                    Q[3] += mk * (3 * dy * dy - d2);
+                    Q[4] += mk * (3 * dy * dz);
+                    Q[5] += mk * (3 * dz * dz - d2);
+                }
+            } else {
+                for (int c = ch.x; c < ch.x + nch; ++c) {
+                    const double mc = T.mass[c];
+                    const double dx = T.com[c] - cx, dy = T.com[cap + c] - cy, dz = T.com[2 * cap + c] - cz;
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    Q[0] += T.quad[c] + mc * (3 * dx * dx - d2);
+                    Q[1] += T.quad[cap + c] + mc * (3 * dx * dy);
+                    Q[2] += T.quad[2 * cap + c] + mc * (3 * dx * dz);
+                    Q[3] += T.quad[3 * cap + c] + mc * (3 * dy * dy - d2);
+                    Q[4] += T.quad[4 * cap + c] + mc * (3 * dy * dz);
+                    Q[5] += T.quad[5 * cap + c] + mc * (3 * dz * dz - d2);
+                }
+            }
+        }
+        for (int q = 0; q < 6; ++q) T.quad[q * cap + i] = Q[q];
+
+        // FP32 packs for the walks
+        const Cloud &cl = a.clouds[r.y > 0 ? (int)(a.key[r.x] >> (3 * a.max_level)) : 0];
+        const double bcx = 0.5 * (lo[0] + hi[0]), bcy = 0.5 * (lo[1] + hi[1]), bcz = 0.5 * (lo[2] + hi[2]);
+        const double hx = 0.5 * (hi[0] - lo[0]), hy = 0.5 * (hi[1] - lo[1]), hz = 0.5 * (hi[2] - lo[2]);
+        const double pad = 1e-6 * cl.size;
+        CellRel b = make_cellrel(bcx, bcy, bcz, cl);
+        T.box_c[i] = make_float4(b.ox, b.oy, b.oz, __int_as_float(b.cell));
+        T.box_h[i] = make_float4((float)(hx + pad), (float)(hy + pad), (float)(hz + pad),
+                                 (float)(hm * (1.0 + 1e-6)));
+        CellRel cm = make_cellrel(cx, cy, cz, cl);
+        T.com_c[i] = make_float4(cm.ox, cm.oy, cm.oz, __int_as_float(cm.cell));
+        const double ex = fmax(fabs(hi[0] - cx), fabs(cx - lo[0]));
+        const double ey = fmax(fabs(hi[1] - cy), fabs(cy - lo[1]));
+        const double ez = fmax(fabs(hi[2] - cz), fabs(cz - lo[2]));
+        const double bmax = sqrt(ex * ex + ey * ey + ez * ez);
+        const double side = 2.0 * fmax(hx, fmax(hy, hz));
+        const double delta = sqrt((cx - bcx) * (cx - bcx) + (cy - bcy) * (cy - bcy) + (cz - bcz) * (cz - bcz));
+        // s/d < theta with the offset of the centre of mass (d > s/theta + delta);
+        // theta = 0 never accepts a node (exact sum)
+        double r_open = isinf(a.inv_theta) ? (double)FLT_MAX : side * a.inv_theta + delta;
+        r_open = fmin(r_open * (1.0 + 1e-5) + pad, (double)FLT_MAX);
+        const double r_soft = fmin((bmax + em) * (1.0 + 1e-5) + pad, (double)FLT_MAX);
+        T.mono[i] = make_float4((float)M, (float)r_open, (float)r_soft, 0.f);
+        T.quad4[i] = make_float4((float)Q[0], (float)Q[1], (float)Q[2], (float)Q[3]);
+        T.quad1[i] = (float)Q[4];
+    }
+}
+
+__global__ void k_tree_totals(Tree T, int max_depth, unsigned long long *counters) {
+    // counters[6] = nodes, counters[7] = leaves
+    const int nn = T.depth_begin[max_depth];
+    unsigned long long leaves = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+        leaves += (T.child[i].y & 255) == 0;
+    leaves = warp_sum(leaves);
+    if ((threadIdx.x & 31) == 0 && leaves) atomicAdd(&counters[7], leaves);
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[6] = (unsigned long long)nn;
+}
+
+// hmax of every node from the current h (after an h search), bottom-up
+__global__ void k_tree_refit_h(Tree T, const double *h, int d) {
+    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const int2 r = T.range[i];
+        const int2 ch = T.child[i];
+        const int nch = ch.y & 255;
+        double hm = 0;
+        if (nch == 0) {
+            for (int k = r.x; k < r.x + r.y; ++k) hm = fmax(hm, h[k]);
+        } else {
+            for (int c = ch.x; c < ch.x + nch; ++c) hm = fmax(hm, T.hmax[c]);
+        }
+        T.hmax[i] = hm;
+        T.box_h[i].w = (float)(hm * (1.0 + 1e-6));
+    }
+}
+
+void launch_tree_refit_h(State &S, cudaStream_t st) {
+    if (S.ncloud == 0) return;
+    const int blocks = S.num_sms * 4;
+    for (int d = S.max_level + 1; d >= 0; --d) k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d);
+}
+
+void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
+    if (S.ncloud == 0) return;
+    Tree &T = S.tree;
+    const int maxd = S.max_level + 1;  // depths 0..max_level
+    k_tree_roots<<<(S.ncloud + 127) / 128, 128, 0, st>>>(T, S.clouds, S.ncloud, S.key, S.max_level);
+    const int blocks = S.num_sms * 4;
+    for (int d = 0; d < maxd; ++d) {
+        k_tree_count<<<blocks, 256, 0, st>>>(T, S.key, d, P.leaf_size, S.max_level);
+        k_tree_scan<<<1, 1024, 0, st>>>(T, d, S.status);
+        k_tree_emit<<<blocks, 256, 0, st>>>(T, S.key, d, P.leaf_size, S.max_level);
+    }
+    MomArgs a;
+    a.pos = S.pos; a.m = S.m; a.h = S.h; a.eps = S.eps; a.n = S.n;
+    a.clouds = S.clouds; a.key = S.key; a.max_level = S.max_level;
+    a.inv_theta = P.theta > 0 ? 1.0 / P.theta : __builtin_inf();
+    for (int d = maxd; d >= 0; --d) k_tree_moments<<<blocks, 128, 0, st>>>(T, a, d, P.quadrupole);
+    k_tree_totals<<<blocks, 256, 0, st>>>(T, maxd + 1, S.counters);
+}
+
+}  // namespace sph3

@@ -1,0 +1,395 @@
+// Barnes-Hut gravity with spline softening, and the FP64 direct sum.
+//
+// One warp per 32-particle group walks the octree once.  A node is accepted
+// as a multipole for the whole group when the distance d from its centre of
+// mass to the group's bounding box satisfies
+//     d > s / theta + delta          (s: node bbox side, delta: |com - bbox centre|)
+//     d > b_max + eps_max_node + eps_max_group   (outside every softening kernel)
+// otherwise a leaf is opened into particle-particle terms with the reference's
+// softened kernel (sph_code/libsx.py:640-652 force, :609-616 potential) and an
+// internal node is opened into its children.  theta = 0 never accepts a node,
+// so the walk becomes the exact direct sum.  Multipoles are monopole +
+// traceless quadrupole about the centre of mass.
+#include <cfloat>
+#include <mutex>
+#include <set>
+
+#include "sph3_walk.cuh"
+
+namespace sph3 {
+
+struct GArgs {
+    const int2 *groups;
+    int ngroups;
+    const int *group_cloud;
+    const Cloud *clouds;
+    const int2 *range;
+    const int2 *child;
+    const float4 *com_c;
+    const float4 *mono;
+    const float4 *quad4;
+    const float *quad1;
+    const double *tcom;   // FP64 node com [3][cap]
+    const double *tmass;
+    const double *tquad;  // [6][cap]
+    int cap;
+    const float4 *pk_pos;
+    const float4 *pk_hme;  // {h, m, eps}
+    const double *pos, *m, *eps;
+    int64_t n;
+    double G;
+    int quad;
+    int stack_cap, max_depth;
+    double *acc_g, *phi;
+    int *work;
+    unsigned *status;
+    unsigned long long *counters;
+};
+
+template <typename R>
+struct GNodeTile {
+    R x[32], y[32], z[32], m[32], qxx[32], qxy[32], qxz[32], qyy[32], qyz[32];
+};
+
+template <typename R>
+struct GPartTile {
+    R x[32], y[32], z[32], m[32], e[32];
+};
+
+template <typename R>
+struct GTile {
+    GNodeTile<R> nd;
+    GPartTile<R> pt;
+    int nodeq[kNodeQ];
+};
+
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsq(double x) { return 1.0 / sqrt(x); }
+
+template <typename R>
+__device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R epsij, R &ax, R &ay,
+                                             R &az, R &ph) {
+    // r2 > 0 here
+    const R rinv = rsq(r2);
+    const R r = r2 * rinv;
+    const R rinv3 = rinv * rinv * rinv;
+    R fk, pk;
+    if (r >= (R)2 * epsij) {
+        fk = rinv3;
+        pk = rinv;
+    } else {
+        const R ie = (R)1 / epsij;
+        const R q = r * ie;
+        const R q2 = q * q, q3 = q2 * q;
+        if (q <= (R)1) {
+            fk = ie * ie * ie * ((R)(4.0 / 3.0) - (R)(6.0 / 5.0) * q2 + (R)0.5 * q3);
+            pk = (R)-2 * ie * ((R)(1.0 / 3.0) * q2 - (R)(3.0 / 20.0) * q2 * q2 + (R)(1.0 / 20.0) * q2 * q3) +
+                 (R)(7.0 / 5.0) * ie;
+        } else {
+            const R q4 = q2 * q2;
+            fk = rinv3 * ((R)(-1.0 / 15.0) + (R)(8.0 / 3.0) * q3 - (R)3 * q4 + (R)(6.0 / 5.0) * q4 * q -
+                          (R)(1.0 / 6.0) * q3 * q3);
+            pk = (R)(-1.0 / 15.0) * rinv - ie * ((R)(4.0 / 3.0) * q2 - q3 + (R)(3.0 / 10.0) * q4 - (R)(1.0 / 30.0) * q4 * q) +
+                 (R)(8.0 / 5.0) * ie;
+        }
+    }
+    const R mf = mj * fk;
+    ax -= mf * dx;
+    ay -= mf * dy;
+    az -= mf * dz;
+    ph -= mj * pk;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTile<R>));
+    GTile<R> &tile = *reinterpret_cast<GTile<R> *>(wm.tile);
+    const int lane = lane_id();
+    unsigned long long n_node = 0, n_part = 0;
+    for (int g = next_group(A.work); g < A.ngroups; g = next_group(A.work)) {
+        const int2 gr = A.groups[g];
+        const Cloud &cl = A.clouds[A.group_cloud[g]];
+        const int ref = __float_as_int(A.pk_pos[gr.x].w);
+        const bool active = lane < gr.y;
+        const int i = gr.x + (active ? lane : 0);
+        const float3 prel = rel_to(A.pk_pos[i], ref, cl.s10);
+        GroupBox gb = group_box(prel, active, ref, cl.s10);
+        R tx, ty, tz, te;
+        if (sizeof(R) == 8) {
+            tx = (R)A.pos[i]; ty = (R)A.pos[A.n + i]; tz = (R)A.pos[2 * A.n + i];
+            te = (R)A.eps[i];
+        } else {
+            tx = (R)prel.x; ty = (R)prel.y; tz = (R)prel.z;
+            te = (R)A.pk_hme[i].z;
+        }
+        const float eps_g = warp_max(active ? (float)te : 0.f);
+        R ax = 0, ay = 0, az = 0, ph = 0;
+
+        // ---- flushes
+        auto flush_nodes = [&](int nq) {
+            for (int base = 0; base < nq; base += 32) {
+                const int ne = min(32, nq - base);
+                if (lane < ne) {
+                    const int nd = tile.nodeq[base + lane];
+                    if (sizeof(R) == 8) {
+                        tile.nd.x[lane] = (R)A.tcom[nd];
+                        tile.nd.y[lane] = (R)A.tcom[A.cap + nd];
+                        tile.nd.z[lane] = (R)A.tcom[2 * A.cap + nd];
+                        tile.nd.m[lane] = (R)A.tmass[nd];
+                        tile.nd.qxx[lane] = (R)A.tquad[nd];
+                        tile.nd.qxy[lane] = (R)A.tquad[A.cap + nd];
+                        tile.nd.qxz[lane] = (R)A.tquad[2 * A.cap + nd];
+                        tile.nd.qyy[lane] = (R)A.tquad[3 * A.cap + nd];
+                        tile.nd.qyz[lane] = (R)A.tquad[4 * A.cap + nd];
+                    } else {
+                        const float3 c = rel_to(A.com_c[nd], ref, cl.s10);
+                        tile.nd.x[lane] = (R)c.x;
+                        tile.nd.y[lane] = (R)c.y;
+                        tile.nd.z[lane] = (R)c.z;
+                        tile.nd.m[lane] = (R)A.mono[nd].x;
+                        const float4 q = A.quad4[nd];
+                        tile.nd.qxx[lane] = (R)q.x;
+                        tile.nd.qxy[lane] = (R)q.y;
+                        tile.nd.qxz[lane] = (R)q.z;
+                        tile.nd.qyy[lane] = (R)q.w;
+                        tile.nd.qyz[lane] = (R)A.quad1[nd];
+                    }
+                }
+                __syncwarp();
+                if (active) {
+                    n_node += ne;
+                    for (int e = 0; e < ne; ++e) {
+                        const R dx = tx - tile.nd.x[e], dy = ty - tile.nd.y[e], dz = tz - tile.nd.z[e];
+                        const R r2 = dx * dx + dy * dy + dz * dz;
+                        const R rinv = rsq(r2);
+                        const R rinv2 = rinv * rinv;
+                        const R M = tile.nd.m[e];
+                        const R mr3 = M * rinv * rinv2;
+                        ax -= mr3 * dx;
+                        ay -= mr3 * dy;
+                        az -= mr3 * dz;
+                        ph -= M * rinv;
+                        if (A.quad) {
+                            const R qxx = tile.nd.qxx[e], qxy = tile.nd.qxy[e], qxz = tile.nd.qxz[e];
+                            const R qyy = tile.nd.qyy[e], qyz = tile.nd.qyz[e];
+                            const R qzz = -qxx - qyy;
+                            const R Qx = qxx * dx + qxy * dy + qxz * dz;
+                            const R Qy = qxy * dx + qyy * dy + qyz * dz;
+                            const R Qz = qxz * dx + qyz * dy + qzz * dz;
+                            const R rQr = dx * Qx + dy * Qy + dz * Qz;
+                            const R rinv5 = rinv2 * rinv2 * rinv;
+                            const R t = (R)2.5 * rQr * rinv5 * rinv2;
+                            ax += Qx * rinv5 - t * dx;
+                            ay += Qy * rinv5 - t * dy;
+                            az += Qz * rinv5 - t * dz;
+                            ph -= (R)0.5 * rQr * rinv5;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        };
+        auto stage = [&](int slot, int j) {
+            if (sizeof(R) == 8) {
+                tile.pt.x[slot] = (R)A.pos[j];
+                tile.pt.y[slot] = (R)A.pos[A.n + j];
+                tile.pt.z[slot] = (R)A.pos[2 * A.n + j];
+                tile.pt.m[slot] = (R)A.m[j];
+                tile.pt.e[slot] = (R)A.eps[j];
+            } else {
+                const float3 p = rel_to(A.pk_pos[j], ref, cl.s10);
+                tile.pt.x[slot] = (R)p.x;
+                tile.pt.y[slot] = (R)p.y;
+                tile.pt.z[slot] = (R)p.z;
+                const float4 hm = A.pk_hme[j];
+                tile.pt.m[slot] = (R)hm.y;
+                tile.pt.e[slot] = (R)hm.z;
+            }
+        };
+        auto interact = [&](int ne) {
+            if (!active) return;
+            n_part += ne;
+            for (int e = 0; e < ne; ++e) {
+                const R dx = tx - tile.pt.x[e], dy = ty - tile.pt.y[e], dz = tz - tile.pt.z[e];
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > (R)0)
+                    spline_force<R>(r2, dx, dy, dz, tile.pt.m[e], (R)0.5 * (te + tile.pt.e[e]), ax, ay, az, ph);
+            }
+        };
+
+        // ---- walk
+        int top = 1;
+        if (lane == 0) wm.stack[0] = cl.root;
+        __syncwarp();
+        int nleaf = 0, nnode = 0;
+        while (top > 0) {
+            const int p = pop_width(top, A.stack_cap, A.max_depth);
+            int node = -1;
+            if (lane < p) node = wm.stack[top - 1 - lane];
+            __syncwarp();
+            top -= p;
+            bool take_leaf = false, take_node = false;
+            int nch = 0, cf = 0;
+            if (node >= 0 && A.range[node].y > 0) {
+                const float4 mo = A.mono[node];
+                const float3 c = rel_to(A.com_c[node], ref, cl.s10);
+                const float d2 = point_gap2(gb, c);
+                const float rs = mo.z + eps_g;
+                if (d2 > mo.y * mo.y && d2 > rs * rs) {
+                    take_node = true;
+                } else {
+                    const int2 ch = A.child[node];
+                    const int k = ch.y & 255;
+                    if (k == 0) take_leaf = true;
+                    else {
+                        nch = k;
+                        cf = ch.x;
+                    }
+                }
+            }
+            const unsigned nb = __ballot_sync(kFull, take_node);
+            if (take_node) tile.nodeq[nnode + __popc(nb & lanemask_lt())] = node;
+            nnode += __popc(nb);
+            const unsigned lb = __ballot_sync(kFull, take_leaf);
+            if (take_leaf) wm.leafq[nleaf + __popc(lb & lanemask_lt())] = node;
+            nleaf += __popc(lb);
+            top = push_children(wm.stack, top, A.stack_cap, nch, cf, A.status);
+            __syncwarp();
+            if (nnode > kNodeQ - 32) {
+                flush_nodes(nnode);
+                nnode = 0;
+            }
+            if (nleaf > kLeafQ - 32) {
+                flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, stage, interact);
+                nleaf = 0;
+            }
+        }
+        __syncwarp();
+        if (nnode > 0) flush_nodes(nnode);
+        if (nleaf > 0) flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, stage, interact);
+        if (active) {
+            A.acc_g[i] = A.G * (double)ax;
+            A.acc_g[A.n + i] = A.G * (double)ay;
+            A.acc_g[2 * A.n + i] = A.G * (double)az;
+            A.phi[i] = A.G * (double)ph;
+        }
+    }
+    n_node = warp_sum(n_node);
+    n_part = warp_sum(n_part);
+    if (lane == 0) {
+        atomicAdd(&A.counters[0], n_node);
+        atomicAdd(&A.counters[1], n_part);
+    }
+}
+
+static void allow_smem_g(const void *kern) {
+    static std::mutex mu;
+    static std::set<const void *> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.insert(kern).second)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+void launch_gravity(State &S, const Params &P, cudaStream_t st) {
+    if (S.ngroups == 0) return;
+    GArgs A;
+    A.groups = S.groups;
+    A.ngroups = S.ngroups;
+    A.group_cloud = S.group_cloud;
+    A.clouds = S.clouds;
+    A.range = S.tree.range;
+    A.child = S.tree.child;
+    A.com_c = S.tree.com_c;
+    A.mono = S.tree.mono;
+    A.quad4 = S.tree.quad4;
+    A.quad1 = S.tree.quad1;
+    A.tcom = S.tree.com;
+    A.tmass = S.tree.mass;
+    A.tquad = S.tree.quad;
+    A.cap = S.tree.cap;
+    A.pk_pos = S.pk_pos;
+    A.pk_hme = S.pk_hme;
+    A.pos = S.pos;
+    A.m = S.m;
+    A.eps = S.eps;
+    A.n = S.n;
+    A.G = P.G;
+    A.quad = P.quadrupole;
+    A.stack_cap = P.stack_cap;
+    A.max_depth = S.max_level + 1;
+    A.acc_g = S.acc_g;
+    A.phi = S.phi;
+    A.work = S.work + 5;
+    A.status = S.status;
+    A.counters = S.counters;
+    cudaMemsetAsync(A.work, 0, sizeof(int), st);
+    if (P.precision == SPH3_PREC_FP64) {
+        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<double>)) * kWalkWarps;
+        allow_smem_g((const void *)k_gravity<double>);
+        k_gravity<double><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+    } else {
+        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<float>)) * kWalkWarps;
+        allow_smem_g((const void *)k_gravity<float>);
+        k_gravity<float><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+    }
+}
+
+// ------------------------------------------------------------ FP64 direct sum
+// One block per requested row: getAcc_g_smth_mpi's inner loop
+// (sph_code/libsx.py:677-703) over the row's own system, in FP64.
+__global__ void k_grav_direct(const int64_t *rows, int64_t nrows, const Cloud *clouds, int ncloud,
+                              const double *pos, const double *m, const double *eps, int64_t n,
+                              double G, double *acc, double *phi) {
+    __shared__ double red[4][32];
+    for (int64_t r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int64_t i = rows[r];
+        int lo = 0, hi = ncloud - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (clouds[mid].begin <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const Cloud &cl = clouds[lo];
+        const double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i], ei = eps[i];
+        double fx = 0, fy = 0, fz = 0, ph = 0;
+        for (int64_t j = cl.begin + threadIdx.x; j < cl.end; j += blockDim.x) {
+            if (j == i) continue;
+            const double dx = xi - pos[j], dy = yi - pos[n + j], dz = zi - pos[2 * n + j];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > 0.0) spline_force<double>(r2, dx, dy, dz, m[j], 0.5 * (ei + eps[j]), fx, fy, fz, ph);
+        }
+        fx = warp_sum(fx);
+        fy = warp_sum(fy);
+        fz = warp_sum(fz);
+        ph = warp_sum(ph);
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            red[0][w] = fx;
+            red[1][w] = fy;
+            red[2][w] = fz;
+            red[3][w] = ph;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s[4] = {0, 0, 0, 0};
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k)
+                for (int q = 0; q < 4; ++q) s[q] += red[q][k];
+            acc[3 * r + 0] = G * s[0];
+            acc[3 * r + 1] = G * s[1];
+            acc[3 * r + 2] = G * s[2];
+            if (phi) phi[r] = G * s[3];
+        }
+        __syncthreads();
+    }
+}
+
+void launch_gravity_direct(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
+                           double *acc_dev, double *phi_dev, cudaStream_t st) {
+    if (nrows == 0) return;
+    int blocks = (int)std::min<int64_t>(nrows, (int64_t)S.num_sms * 16);
+    k_grav_direct<<<blocks, 256, 0, st>>>(rows_sorted_dev, nrows, S.clouds, S.ncloud, S.pos, S.m, S.eps,
+                                          S.n, P.G, acc_dev, phi_dev);
+}
+
+}  // namespace sph3

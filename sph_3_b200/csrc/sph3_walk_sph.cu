@@ -1,0 +1,1062 @@
+// SPH walks: bootstrap h, h search, density (+ div/curl v, EOS) and the fused
+// hydro acceleration + du/dt pass, plus the neighbour-set export used by the
+// parity tests.
+//
+// Every pass is one persistent kernel: warps pull 32-particle groups from an
+// atomic counter, walk the octree once per group (sph3_walk.cuh) and stream
+// the candidate leaves through a 32-entry shared-memory tile.  Two
+// instantiations per pass:
+//   float  -- mixed precision: positions in the FP32 frame of the group's
+//             reference cell (exact integer cell offsets + FP32 in-cell
+//             offsets), FP32 kernel arithmetic, FP64 results;
+//   double -- the plain FP64 path: absolute FP64 positions and the
+//             reference's own expressions for every predicate (no FMA
+//             contraction in them), so neighbour sets and the reference h
+//             rule are bit-exact.
+// The kernel formulas follow sph_code/libsx.py (M4 kernel, sigma = 1/pi,
+// hbar_ij = (h_i + h_j) / 2, support q <= 2) and sph_code/shear.py.
+#include <cfloat>
+#include <mutex>
+#include <set>
+#include <vector>
+
+#include "sph3_walk.cuh"
+
+namespace sph3 {
+
+constexpr double kSig = 0.31830988618379067154;  // 1/pi
+constexpr float kSigF = 0.31830988618379067154f;
+
+// ------------------------------------------------------------ arguments
+struct WalkArgs {
+    const int2 *groups;
+    int ngroups;
+    const int *group_cloud;
+    const Cloud *clouds;
+    int ncloud;
+    const int2 *range;
+    const int2 *child;
+    const float4 *box_c;
+    const float4 *box_h;
+    const float4 *pk_pos;
+    const double *pos;
+    int64_t n;
+    int stack_cap;
+    int max_depth;
+    int periodic;
+    double box[3];
+    int *work;
+    unsigned *status;
+    unsigned long long *counters;
+};
+
+// division and reciprocal in the pass precision: the FP32 path uses the
+// approximate hardware reciprocal, the FP64 path IEEE division
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+
+// exact FP64 distance as the reference writes it: sqrt(dx*dx + dy*dy + dz*dz)
+__device__ __forceinline__ double exact_dist(double dx, double dy, double dz) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+}
+
+// Walk the tree for one group, calling flush(leafq, nleaf) on full queues.
+// reach(node) = Rg + (node_h ? hmax_node : 0); images shift the nodes.
+template <class Flush>
+__device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, const GroupBox &gb,
+                               float Rg, bool node_h, float3 shift, Flush &flush) {
+    const int lane = lane_id();
+    int top = 1;
+    if (lane == 0) wm.stack[0] = root;
+    __syncwarp();
+    int nleaf = 0;
+    const float margin = 1.0f + 4e-5f;
+    while (top > 0) {
+        const int p = pop_width(top, a.stack_cap, a.max_depth);
+        int node = -1;
+        if (lane < p) node = wm.stack[top - 1 - lane];
+        __syncwarp();
+        top -= p;
+        bool take = false;
+        int nch = 0, cf = 0;
+        if (node >= 0) {
+            const float4 bc = a.box_c[node];
+            const float4 bh = a.box_h[node];
+            float3 c = rel_to(bc, gb.ref, gb.s10);
+            c.x += shift.x;
+            c.y += shift.y;
+            c.z += shift.z;
+            const float reach = (Rg + (node_h ? bh.w : 0.f)) * margin;
+            const float g2 = box_gap2(gb, c, make_float3(bh.x, bh.y, bh.z));
+            if (g2 <= reach * reach) {
+                const int2 ch = a.child[node];
+                const int k = ch.y & 255;
+                if (k == 0) {
+                    take = a.range[node].y > 0;
+                } else {
+                    nch = k;
+                    cf = ch.x;
+                }
+            }
+        }
+        const unsigned tb = __ballot_sync(kFull, take);
+        if (take) wm.leafq[nleaf + __popc(tb & lanemask_lt())] = node;
+        nleaf += __popc(tb);
+        top = push_children(wm.stack, top, a.stack_cap, nch, cf, a.status);
+        if (nleaf > kLeafQ - 32) {
+            __syncwarp();
+            flush(nleaf);
+            nleaf = 0;
+        }
+    }
+    __syncwarp();
+    if (nleaf > 0) flush(nleaf);
+}
+
+// ------------------------------------------------------------ group setup
+template <typename R>
+struct Target {
+    R x, y, z;
+};
+
+__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+
+struct GroupInfo {
+    int first, count, cloud, i;
+    bool active;
+    int ref;
+    float s10;
+    int root;
+    float3 prel;  // target in the group frame (FP32)
+};
+
+__device__ __forceinline__ GroupInfo group_info(const WalkArgs &a, int g) {
+    GroupInfo gi;
+    const int2 gr = a.groups[g];
+    gi.first = gr.x;
+    gi.count = gr.y;
+    gi.cloud = a.group_cloud[g];
+    const Cloud &cl = a.clouds[gi.cloud];
+    gi.s10 = cl.s10;
+    gi.root = cl.root;
+    gi.ref = __float_as_int(a.pk_pos[gi.first].w);
+    const int lane = lane_id();
+    gi.active = lane < gi.count;
+    gi.i = gi.first + (gi.active ? lane : 0);
+    gi.prel = rel_to(a.pk_pos[gi.i], gi.ref, gi.s10);
+    return gi;
+}
+
+// ================================================================= h search
+struct HArgs {
+    WalkArgs w;
+    double *h;
+    float4 *pk_hme;
+    int *nngb;
+    int n_ngb, tol, max_iter;
+};
+
+template <typename R>
+struct HTile {
+    R x[32], y[32], z[32];
+};
+
+constexpr int kHK = 16;          // thresholds per pass in the reference-step mode
+constexpr double kNewtonDelta = 0.08;
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WalkArgs &a = A.w;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<R>));
+    HTile<R> &tile = *reinterpret_cast<HTile<R> *>(wm.tile);
+    const int lane = lane_id();
+    constexpr int K = MODE == SPH3_H_REFSTEP ? kHK : 2;
+    const int up = A.n_ngb + A.tol, low = A.n_ngb - A.tol;
+    unsigned long long pairs = 0, passes = 0;
+    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+        GroupInfo gi = group_info(a, g);
+        const Cloud &cl = a.clouds[gi.cloud];
+        const int64_t ncl = cl.end - cl.begin;
+        GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        // target position in the pass precision
+        R tx, ty, tz;
+        if (sizeof(R) == 8) {
+            tx = (R)a.pos[gi.i];
+            ty = (R)a.pos[a.n + gi.i];
+            tz = (R)a.pos[2 * a.n + gi.i];
+        } else {
+            tx = (R)gi.prel.x;
+            ty = (R)gi.prel.y;
+            tz = (R)gi.prel.z;
+        }
+        double h = A.h[gi.i];
+        if (!(h > 0.0) || !isfinite(h)) h = (double)gi.s10;  // no usable start: one level-10 cell
+        bool conv = !gi.active;
+        int ncount = 0;
+        int steps = 0;      // reference-rule steps taken
+        int dir = 0;        // reference rule: -1 down, +1 up, 0 unknown (first pass)
+        double lb = 0.0, hb = DBL_MAX;
+        bool failed = false;
+        const double hcap = 4.0 * cl.size;
+        for (int pass = 0; pass < A.max_iter + 2; ++pass) {
+            if (__all_sync(kFull, conv)) break;
+            // thresholds for this pass
+            double thr[K];
+            if (MODE == SPH3_H_REFSTEP) {
+                if (dir == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) thr[k] = __dmul_rn(2.0, h);
+                } else {
+                    double hk = h;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const double t = __dmul_rn(0.003, hk);
+                        hk = dir < 0 ? __dsub_rn(hk, t) : __dadd_rn(hk, t);
+                        thr[k] = __dmul_rn(2.0, hk);
+                    }
+                }
+            } else {
+                thr[0] = 2.0 * h;
+                thr[1] = 2.0 * h * (1.0 + kNewtonDelta);
+            }
+            float reach = 0.f;
+            if (!conv) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) reach = fmaxf(reach, (float)thr[k]);
+            }
+            reach = warp_max(reach) * (1.0f + 1e-5f);
+            float thr2f[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) thr2f[k] = (float)(thr[k] * thr[k]);
+            int cnt[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) cnt[k] = 0;
+            // images (periodic) and the walk
+            float3 sh[27];
+            const int nim = group_images(gb, reach, a.box, a.periodic, sh);
+            for (int im = 0; im < nim; ++im) {
+                const float3 s = sh[im];
+                auto stage = [&](int slot, int j) {
+                    if (sizeof(R) == 8) {
+                        tile.x[slot] = (R)(a.pos[j] + (double)s.x);
+                        tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
+                        tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
+                    } else {
+                        float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+                        tile.x[slot] = (R)(p.x + s.x);
+                        tile.y[slot] = (R)(p.y + s.y);
+                        tile.z[slot] = (R)(p.z + s.z);
+                    }
+                };
+                auto interact = [&](int ne) {
+                    if (conv) return;
+                    pairs += ne;
+                    for (int e = 0; e < ne; ++e) {
+                        if (sizeof(R) == 8) {
+                            const double d = exact_dist((double)tile.x[e] - (double)tx,
+                                                        (double)tile.y[e] - (double)ty,
+                                                        (double)tile.z[e] - (double)tz);
+#pragma unroll
+                            for (int k = 0; k < K; ++k) cnt[k] += d < thr[k];
+                        } else {
+                            const float dx = (float)tile.x[e] - (float)tx;
+                            const float dy = (float)tile.y[e] - (float)ty;
+                            const float dz = (float)tile.z[e] - (float)tz;
+                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+#pragma unroll
+                            for (int k = 0; k < K; ++k) cnt[k] += d2 < thr2f[k];
+                        }
+                    }
+                };
+                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+                collect_leaves(a, wm, gi.root, gb, reach, false, s, flush);
+            }
+            ++passes;
+            if (conv) continue;
+            // ---- update
+            if (MODE == SPH3_H_REFSTEP) {
+                if (dir == 0) {
+                    ncount = cnt[0];
+                    if (ncount <= up && ncount >= low) {
+                        conv = true;
+                    } else {
+                        dir = ncount > up ? -1 : 1;
+                    }
+                } else {
+                    double hk = h;
+                    for (int k = 0; k < K; ++k) {
+                        if (steps >= A.max_iter) {
+                            failed = true;
+                            conv = true;
+                            break;
+                        }
+                        const double t = __dmul_rn(0.003, hk);
+                        hk = dir < 0 ? __dsub_rn(hk, t) : __dadd_rn(hk, t);
+                        ++steps;
+                        ncount = cnt[k];
+                        h = hk;
+                        if (ncount <= up && ncount >= low) {
+                            conv = true;
+                            break;
+                        }
+                        const int nd = ncount > up ? -1 : 1;
+                        if (nd != dir) {  // crossed the window: the rule turns around
+                            dir = nd;
+                            break;
+                        }
+                    }
+                }
+            } else {
+                const int n0 = cnt[0], n1 = cnt[1];
+                ncount = n0;
+                if (n0 <= up && n0 >= low) {
+                    conv = true;
+                } else if (pass >= A.max_iter || (n0 < low && (int64_t)n0 >= ncl)) {
+                    // out of iterations, or the whole system is inside 2h already
+                    failed = true;
+                    conv = true;
+                } else {
+                    if (n0 > up) hb = fmin(hb, h);
+                    else lb = fmax(lb, h);
+                    double hn;
+                    if (n0 == 0) {
+                        hn = 2.0 * h;
+                    } else {
+                        double s = n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
+                        s = fmin(fmax(s, 1.0), 6.0);
+                        hn = h * exp((log((double)A.n_ngb) - log((double)n0)) / s);
+                    }
+                    hn = fmin(fmax(hn, 0.5 * h), 2.0 * h);
+                    if (!(hn > lb && hn < hb)) {
+                        if (lb > 0.0 && hb < DBL_MAX) hn = sqrt(lb * hb);
+                        else if (hb < DBL_MAX) hn = hb * 0.8;
+                        else hn = lb * 1.25;
+                    }
+                    h = fmin(hn, hcap);
+                }
+            }
+        }
+        if (!conv) failed = true;
+        if (gi.active) {
+            A.h[gi.i] = h;
+            A.nngb[gi.i] = ncount;
+            A.pk_hme[gi.i].x = (float)h;
+        }
+        const unsigned fb = __ballot_sync(kFull, gi.active && failed);
+        if (fb && lane == 0) set_status(a.status, SPH3_STATUS_H_NOT_CONVERGED);
+    }
+    pairs = warp_sum(pairs);
+    if (lane == 0) {
+        atomicAdd(&a.counters[4], pairs);
+        atomicAdd(&a.counters[5], passes);
+    }
+}
+
+// ============================================================ bootstrap h
+// h = 0.5 * (k-th smallest distance, self included), the reference's
+// smoothing_length_mpi / do_smoothingX (sph_code/libsx.py:752-800), exact:
+// a radius that holds k+1 particles, then a 17-way bisection on the bit
+// pattern of the FP64 distance.
+struct BootArgs {
+    WalkArgs w;
+    double *h;
+    float4 *pk_hme;
+    int k;
+};
+
+__global__ void __launch_bounds__(kWalkWarps * 32) k_boot_h(BootArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WalkArgs &a = A.w;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<double>));
+    HTile<double> &tile = *reinterpret_cast<HTile<double> *>(wm.tile);
+    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+        GroupInfo gi = group_info(a, g);
+        const Cloud &cl = a.clouds[gi.cloud];
+        const int64_t ncl = cl.end - cl.begin;
+        const int need = (int)std::min<int64_t>((int64_t)A.k, ncl - 1) + 1;
+        GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        const double tx = a.pos[gi.i], ty = a.pos[a.n + gi.i], tz = a.pos[2 * a.n + gi.i];
+        // phase 1: grow a common radius until every target has `need` particles within it
+        double Rg = 2.0 * (double)fmaxf(gb.hw.x, fmaxf(gb.hw.y, gb.hw.z)) + (double)gi.s10;
+        for (int it = 0; it < 64; ++it) {
+            int cnt = 0;
+            float3 sh[27];
+            const int nim = group_images(gb, (float)Rg, a.box, a.periodic, sh);
+            for (int im = 0; im < nim; ++im) {
+                const float3 s = sh[im];
+                auto stage = [&](int slot, int j) {
+                    tile.x[slot] = a.pos[j] + (double)s.x;
+                    tile.y[slot] = a.pos[a.n + j] + (double)s.y;
+                    tile.z[slot] = a.pos[2 * a.n + j] + (double)s.z;
+                };
+                auto interact = [&](int ne) {
+                    for (int e = 0; e < ne; ++e)
+                        cnt += exact_dist(tile.x[e] - tx, tile.y[e] - ty, tile.z[e] - tz) <= Rg;
+                };
+                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+                collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
+            }
+            if (__all_sync(kFull, !gi.active || cnt >= need)) break;
+            Rg *= 2.0;
+        }
+        // phase 2: bisection on the distance bits, 16 thresholds per pass
+        unsigned long long lo = 0ull, hi = (unsigned long long)__double_as_longlong(Rg);
+        for (int it = 0; it < 40; ++it) {
+            if (__all_sync(kFull, !gi.active || lo == hi)) break;
+            unsigned long long t[16];
+            const unsigned long long span = hi - lo;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                if (span > 16ull) t[m] = lo + (span / 17ull) * (unsigned long long)(m + 1);
+                else t[m] = (unsigned long long)m < span ? lo + m : hi;
+            }
+            double tv[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) tv[m] = __longlong_as_double((long long)t[m]);
+            int c[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) c[m] = 0;
+            float3 sh[27];
+            const int nim = group_images(gb, (float)Rg, a.box, a.periodic, sh);
+            for (int im = 0; im < nim; ++im) {
+                const float3 s = sh[im];
+                auto stage = [&](int slot, int j) {
+                    tile.x[slot] = a.pos[j] + (double)s.x;
+                    tile.y[slot] = a.pos[a.n + j] + (double)s.y;
+                    tile.z[slot] = a.pos[2 * a.n + j] + (double)s.z;
+                };
+                auto interact = [&](int ne) {
+                    if (lo == hi) return;
+                    for (int e = 0; e < ne; ++e) {
+                        const double d = exact_dist(tile.x[e] - tx, tile.y[e] - ty, tile.z[e] - tz);
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) c[m] += d <= tv[m];
+                    }
+                };
+                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+                collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
+            }
+            if (lo != hi) {
+                int m = 0;
+                while (m < 16 && c[m] < need) ++m;
+                if (m == 16) lo = t[15] + 1;
+                else {
+                    unsigned long long nlo = m > 0 ? t[m - 1] + 1 : lo;
+                    hi = t[m];
+                    lo = nlo;
+                }
+                if (lo > hi) lo = hi;
+            }
+        }
+        if (gi.active) {
+            const double hv = __longlong_as_double((long long)hi) * 0.5;
+            A.h[gi.i] = hv;
+            A.pk_hme[gi.i].x = (float)hv;
+        }
+    }
+}
+
+// =================================================== density, EOS, div/curl
+struct DArgs {
+    WalkArgs w;
+    const float4 *pk_hme, *pk_vel;
+    const double *h, *m, *vel, *u;
+    double *rho, *P, *c, *divV, *curlV, *bal;
+    float4 *pk_thm;
+    double gamma;
+    int keep_rho;
+};
+
+template <typename R, bool DC>
+struct DTile {
+    R x[32], y[32], z[32], h[32], m[32];
+    R vx[DC ? 32 : 1], vy[DC ? 32 : 1], vz[DC ? 32 : 1];
+};
+
+template <typename R, bool DC>
+__global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WalkArgs &a = A.w;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(DTile<R, DC>));
+    DTile<R, DC> &tile = *reinterpret_cast<DTile<R, DC> *>(wm.tile);
+    const int lane = lane_id();
+    unsigned long long pairs = 0;
+    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+        GroupInfo gi = group_info(a, g);
+        GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        R tx, ty, tz, th, tvx = 0, tvy = 0, tvz = 0;
+        if (sizeof(R) == 8) {
+            tx = (R)a.pos[gi.i]; ty = (R)a.pos[a.n + gi.i]; tz = (R)a.pos[2 * a.n + gi.i];
+            th = (R)A.h[gi.i];
+            if (DC) { tvx = (R)A.vel[gi.i]; tvy = (R)A.vel[a.n + gi.i]; tvz = (R)A.vel[2 * a.n + gi.i]; }
+        } else {
+            tx = (R)gi.prel.x; ty = (R)gi.prel.y; tz = (R)gi.prel.z;
+            th = (R)A.pk_hme[gi.i].x;
+            if (DC) { float4 v = A.pk_vel[gi.i]; tvx = (R)v.x; tvy = (R)v.y; tvz = (R)v.z; }
+        }
+        const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
+        R rho = 0, sdiv = 0, cx = 0, cy = 0, cz = 0;
+        float3 sh[27];
+        const int nim = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic, sh);
+        for (int im = 0; im < nim; ++im) {
+            const float3 s = sh[im];
+            auto stage = [&](int slot, int j) {
+                if (sizeof(R) == 8) {
+                    tile.x[slot] = (R)(a.pos[j] + (double)s.x);
+                    tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
+                    tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
+                    tile.h[slot] = (R)A.h[j];
+                    tile.m[slot] = (R)A.m[j];
+                    if (DC) {
+                        tile.vx[slot] = (R)A.vel[j];
+                        tile.vy[slot] = (R)A.vel[a.n + j];
+                        tile.vz[slot] = (R)A.vel[2 * a.n + j];
+                    }
+                } else {
+                    float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+                    tile.x[slot] = (R)(p.x + s.x);
+                    tile.y[slot] = (R)(p.y + s.y);
+                    tile.z[slot] = (R)(p.z + s.z);
+                    float4 hm = A.pk_hme[j];
+                    tile.h[slot] = (R)hm.x;
+                    tile.m[slot] = (R)hm.y;
+                    if (DC) {
+                        float4 v = A.pk_vel[j];
+                        tile.vx[slot] = (R)v.x;
+                        tile.vy[slot] = (R)v.y;
+                        tile.vz[slot] = (R)v.z;
+                    }
+                }
+            };
+            auto interact = [&](int ne) {
+                if (!gi.active) return;
+                pairs += ne;
+                for (int e = 0; e < ne; ++e) {
+                    if (sizeof(R) == 8) {
+                        // reference order: dx = x_i - x_j, q = |r| / hbar
+                        const double dx = __dsub_rn((double)tx, (double)tile.x[e]);
+                        const double dy = __dsub_rn((double)ty, (double)tile.y[e]);
+                        const double dz = __dsub_rn((double)tz, (double)tile.z[e]);
+                        const double rr = exact_dist(dx, dy, dz);
+                        const double hij = __dmul_rn(0.5, __dadd_rn((double)th, (double)tile.h[e]));
+                        const double q = __ddiv_rn(rr, hij);
+                        if (q <= 2.0) {
+                            const double ih = 1.0 / hij;
+                            const double ih3 = ih * ih * ih;
+                            double W;
+                            if (q <= 1.0) W = kSig * ih3 * (1.0 - 1.5 * q * q + 0.75 * q * q * q);
+                            else { const double t = 2.0 - q; W = kSig * ih3 * 0.25 * t * t * t; }
+                            rho += (R)((double)tile.m[e] * W);
+                            if (DC) {
+                                double nW;
+                                const double ih5 = ih3 * ih * ih;
+                                if (q <= 1.0) nW = kSig * ih5 * (-3.0 + 2.25 * q);
+                                else { const double t = 2.0 - q; nW = -0.75 * kSig * ih5 * t * t / (q + 1e-20); }
+                                const double gx = nW * dx, gy = nW * dy, gz = nW * dz;
+                                const double vx = (double)tvx - (double)tile.vx[e];
+                                const double vy = (double)tvy - (double)tile.vy[e];
+                                const double vz = (double)tvz - (double)tile.vz[e];
+                                const double mj = (double)tile.m[e];
+                                sdiv += (R)(-mj * (vx * gx + vy * gy + vz * gz));
+                                cx += (R)(mj * (vy * gz - vz * gy));
+                                cy += (R)(mj * (vz * gx - vx * gz));
+                                cz += (R)(mj * (vx * gy - vy * gx));
+                            }
+                        }
+                    } else {
+                        const float dx = (float)tx - (float)tile.x[e];
+                        const float dy = (float)ty - (float)tile.y[e];
+                        const float dz = (float)tz - (float)tile.z[e];
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float hs = (float)th + (float)tile.h[e];  // = 2 hbar
+                        if (d2 <= hs * hs) {
+                            const float ih = __fdividef(2.0f, hs);
+                            const float q = sqrtf(d2) * ih;
+                            const float ih3 = ih * ih * ih;
+                            float W;
+                            if (q <= 1.0f) W = kSigF * ih3 * fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
+                            else { const float t = 2.0f - q; W = kSigF * ih3 * 0.25f * t * t * t; }
+                            rho = fmaf((float)tile.m[e], W, (float)rho);
+                            if (DC) {
+                                float nW;
+                                const float ih5 = ih3 * ih * ih;
+                                if (q <= 1.0f) nW = kSigF * ih5 * fmaf(2.25f, q, -3.0f);
+                                else { const float t = 2.0f - q; nW = -0.75f * kSigF * ih5 * t * t * __fdividef(1.0f, q + 1e-20f); }
+                                const float mj = (float)tile.m[e] * nW;
+                                const float vx = (float)tvx - (float)tile.vx[e];
+                                const float vy = (float)tvy - (float)tile.vy[e];
+                                const float vz = (float)tvz - (float)tile.vz[e];
+                                sdiv -= mj * fmaf(vx, dx, fmaf(vy, dy, vz * dz));
+                                cx += mj * (vy * dz - vz * dy);
+                                cy += mj * (vz * dx - vx * dz);
+                                cz += mj * (vx * dy - vy * dx);
+                            }
+                        }
+                    }
+                }
+            };
+            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
+        }
+        if (gi.active) {
+            const int i = gi.i;
+            double r, P, c;
+            if (A.keep_rho) {  // div/curl only: divide by the caller's rho
+                r = A.rho[i];
+                P = A.P[i];
+                c = A.c[i];
+            } else {
+                r = (double)rho;
+                const double u = A.u[i];
+                P = (A.gamma - 1.0) * r * u;
+                c = sqrt(A.gamma * (A.gamma - 1.0) * u);
+                A.rho[i] = r;
+                A.P[i] = P;
+                A.c[i] = c;
+            }
+            double f = 0.0;
+            if (DC) {
+                const double inv = r > 0.0 ? 1.0 / r : 0.0;
+                const double dv = fabs((double)sdiv) * inv;
+                const double cv = sqrt((double)cx * (double)cx + (double)cy * (double)cy + (double)cz * (double)cz) * inv;
+                A.divV[i] = dv;
+                A.curlV[i] = cv;
+                const double hh = A.h[i];
+                f = dv / (dv + cv + 0.0001 * c / hh);
+                A.bal[i] = f;
+            }
+            const double pr = r > 0.0 ? P / (r * r) : 0.0;
+            A.pk_thm[i] = make_float4((float)r, (float)pr, (float)c, (float)f);
+            if (!(r > 0.0)) set_status(a.status, SPH3_STATUS_ZERO_DENSITY);
+        }
+    }
+    pairs = warp_sum(pairs);
+    if (lane == 0) atomicAdd(&a.counters[2], pairs);
+}
+
+// ============================================================ hydro
+struct YArgs {
+    WalkArgs w;
+    const float4 *pk_hme, *pk_vel, *pk_thm;
+    const double *h, *m, *vel, *rho, *P, *c, *bal;
+    double *acc_sph, *dudt;
+    double alpha, beta, eta;
+};
+
+template <typename R>
+struct YTile {
+    R x[32], y[32], z[32], vx[32], vy[32], vz[32], h[32], m[32], rho[32], pr[32], c[32], f[32];
+};
+
+template <typename R, int VISC, bool ACC, bool DU>
+__global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WalkArgs &a = A.w;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(YTile<R>));
+    YTile<R> &tile = *reinterpret_cast<YTile<R> *>(wm.tile);
+    const int lane = lane_id();
+    unsigned long long pairs = 0;
+    const R alpha = (R)A.alpha, beta = (R)A.beta, eta2 = (R)(A.eta * A.eta);
+    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+        GroupInfo gi = group_info(a, g);
+        GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        const int i = gi.i;
+        R tx, ty, tz, tvx, tvy, tvz, th, trho, tpr, tc, tf;
+        if (sizeof(R) == 8) {
+            tx = (R)a.pos[i]; ty = (R)a.pos[a.n + i]; tz = (R)a.pos[2 * a.n + i];
+            tvx = (R)A.vel[i]; tvy = (R)A.vel[a.n + i]; tvz = (R)A.vel[2 * a.n + i];
+            th = (R)A.h[i]; trho = (R)A.rho[i];
+            tpr = (R)(A.P[i] / (A.rho[i] * A.rho[i]));
+            tc = (R)A.c[i]; tf = (R)A.bal[i];
+        } else {
+            tx = (R)gi.prel.x; ty = (R)gi.prel.y; tz = (R)gi.prel.z;
+            float4 v = A.pk_vel[i];
+            tvx = (R)v.x; tvy = (R)v.y; tvz = (R)v.z;
+            th = (R)A.pk_hme[i].x;
+            float4 t = A.pk_thm[i];
+            trho = (R)t.x; tpr = (R)t.y; tc = (R)t.z; tf = (R)t.w;
+        }
+        const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
+        R ax = 0, ay = 0, az = 0, du = 0;
+        float3 sh[27];
+        const int nim = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic, sh);
+        for (int im = 0; im < nim; ++im) {
+            const float3 s = sh[im];
+            auto stage = [&](int slot, int j) {
+                if (sizeof(R) == 8) {
+                    tile.x[slot] = (R)(a.pos[j] + (double)s.x);
+                    tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
+                    tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
+                    tile.vx[slot] = (R)A.vel[j];
+                    tile.vy[slot] = (R)A.vel[a.n + j];
+                    tile.vz[slot] = (R)A.vel[2 * a.n + j];
+                    tile.h[slot] = (R)A.h[j];
+                    tile.m[slot] = (R)A.m[j];
+                    const double rj = A.rho[j];
+                    tile.rho[slot] = (R)rj;
+                    tile.pr[slot] = (R)(A.P[j] / (rj * rj));
+                    tile.c[slot] = (R)A.c[j];
+                    tile.f[slot] = (R)A.bal[j];
+                } else {
+                    float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+                    tile.x[slot] = (R)(p.x + s.x);
+                    tile.y[slot] = (R)(p.y + s.y);
+                    tile.z[slot] = (R)(p.z + s.z);
+                    float4 v = A.pk_vel[j];
+                    tile.vx[slot] = (R)v.x; tile.vy[slot] = (R)v.y; tile.vz[slot] = (R)v.z;
+                    float4 hm = A.pk_hme[j];
+                    tile.h[slot] = (R)hm.x; tile.m[slot] = (R)hm.y;
+                    float4 t = A.pk_thm[j];
+                    tile.rho[slot] = (R)t.x; tile.pr[slot] = (R)t.y; tile.c[slot] = (R)t.z; tile.f[slot] = (R)t.w;
+                }
+            };
+            auto interact = [&](int ne) {
+                if (!gi.active) return;
+                pairs += ne;
+                for (int e = 0; e < ne; ++e) {
+                    R dx, dy, dz, rr, hij, q;
+                    bool in;
+                    if (sizeof(R) == 8) {
+                        const double ddx = __dsub_rn((double)tx, (double)tile.x[e]);
+                        const double ddy = __dsub_rn((double)ty, (double)tile.y[e]);
+                        const double ddz = __dsub_rn((double)tz, (double)tile.z[e]);
+                        const double drr = exact_dist(ddx, ddy, ddz);
+                        const double dh = __dmul_rn(0.5, __dadd_rn((double)th, (double)tile.h[e]));
+                        const double dq = __ddiv_rn(drr, dh);
+                        in = dq <= 2.0;
+                        dx = (R)ddx; dy = (R)ddy; dz = (R)ddz; rr = (R)drr; hij = (R)dh; q = (R)dq;
+                    } else {
+                        dx = tx - tile.x[e];
+                        dy = ty - tile.y[e];
+                        dz = tz - tile.z[e];
+                        const R d2 = dx * dx + dy * dy + dz * dz;
+                        const R hs = th + tile.h[e];
+                        in = d2 <= hs * hs;
+                        rr = (R)sqrtf((float)d2);
+                        hij = (R)0.5 * hs;
+                        q = (R)((float)rr * __fdividef(1.0f, (float)hij));
+                    }
+                    if (!in) continue;
+                    const R ih = fdiv((R)1, hij);
+                    const R ih5 = ih * ih * ih * ih * ih;
+                    R nW;
+                    if (q <= (R)1) nW = (R)kSig * ih5 * ((R)-3 + (R)2.25 * q);
+                    else { const R t = (R)2 - q; nW = fdiv((R)(-0.75 * kSig) * ih5 * t * t, q + (R)1e-20); }
+                    const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+                    const R vx = tvx - tile.vx[e], vy = tvy - tile.vy[e], vz = tvz - tile.vz[e];
+                    const R vr = vx * dx + vy * dy + vz * dz;
+                    const R rhoij = (R)0.5 * (trho + tile.rho[e]);
+                    R PI = 0;
+                    if (VISC == SPH3_VISC_MG83) {
+                        const R cij = (R)0.5 * (tc + tile.c[e]);
+                        const R mu = fdiv(hij * vr, rr * rr + hij * hij * eta2);
+                        if (vr <= (R)0) PI = fdiv(-alpha * cij * mu + beta * mu * mu, rhoij);
+                    } else {
+                        const R w = fdiv(vr, rr + (R)1e-5);
+                        const R vsig = tc + tile.c[e] - (R)3 * w;
+                        if (vr <= (R)0) PI = fdiv((R)-0.5 * alpha * vsig * w, rhoij);
+                        if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + tile.f[e]) * PI;
+                    }
+                    const R mj = tile.m[e];
+                    if (ACC) {
+                        const R pt = mj * (tpr + tile.pr[e] + PI);
+                        ax -= pt * gx;
+                        ay -= pt * gy;
+                        az -= pt * gz;
+                    }
+                    if (DU) du += mj * (tpr + (R)0.5 * PI) * (vx * gx + vy * gy + vz * gz);
+                }
+            };
+            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
+        }
+        if (gi.active) {
+            if (ACC) {
+                A.acc_sph[i] = (double)ax;
+                A.acc_sph[a.n + i] = (double)ay;
+                A.acc_sph[2 * a.n + i] = (double)az;
+            }
+            if (DU) A.dudt[i] = (double)du;
+        }
+    }
+    pairs = warp_sum(pairs);
+    if (lane == 0) atomicAdd(&a.counters[3], pairs);
+}
+
+// ============================================================ neighbours
+// Exact FP64 neighbour sets {j : q_ij <= 2} of selected particles; pass 0
+// counts, pass 1 writes caller indices at the given offsets.
+struct NArgs {
+    WalkArgs w;
+    const double *h;
+    const int64_t *orig;
+    const int64_t *rows;  // sorted indices
+    int64_t nrows;
+    int64_t *offsets;     // [nrows + 1]
+    int64_t *out;
+    int64_t cap;
+    int *cursor;          // [nrows]
+    int pass;
+};
+
+__global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WalkArgs &a = A.w;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<double>));
+    const int lane = lane_id();
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = gw; r < A.nrows; r += nw) {
+        const int i = (int)A.rows[r];
+        int cloud = 0;
+        {
+            int lo = 0, hi = a.ncloud - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (a.clouds[mid].begin <= i) lo = mid;
+                else hi = mid - 1;
+            }
+            cloud = lo;
+        }
+        const Cloud &cl = a.clouds[cloud];
+        const int ref = __float_as_int(a.pk_pos[i].w);
+        const float3 prel = rel_to(a.pk_pos[i], ref, cl.s10);
+        GroupBox gb = group_box(prel, lane == 0, ref, cl.s10);
+        const double tx = a.pos[i], ty = a.pos[a.n + i], tz = a.pos[2 * a.n + i];
+        const double th = A.h[i];
+        float3 sh[27];
+        const int nim = group_images(gb, (float)th + a.box_h[cl.root].w, a.box, a.periodic, sh);
+        int found = 0;
+        for (int im = 0; im < nim; ++im) {
+            const float3 s = sh[im];
+            auto stage = [&](int slot, int j) {
+                const double dx = __dsub_rn(tx, a.pos[j] + (double)s.x);
+                const double dy = __dsub_rn(ty, a.pos[a.n + j] + (double)s.y);
+                const double dz = __dsub_rn(tz, a.pos[2 * a.n + j] + (double)s.z);
+                const double rr = exact_dist(dx, dy, dz);
+                const double hij = __dmul_rn(0.5, __dadd_rn(th, A.h[j]));
+                if (__ddiv_rn(rr, hij) <= 2.0) {
+                    ++found;
+                    if (A.pass == 1) {
+                        const int k = atomicAdd(&A.cursor[r], 1);
+                        const int64_t at = A.offsets[r] + k;
+                        if (at < A.cap) A.out[at] = A.orig[j];
+                        else set_status(a.status, SPH3_STATUS_LIST_OVERFLOW);
+                    }
+                }
+                (void)slot;
+            };
+            auto interact = [&](int ne) { (void)ne; };
+            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            collect_leaves(a, wm, cl.root, gb, (float)th, true, s, flush);
+        }
+        found = warp_sum(found);
+        if (A.pass == 0 && lane == 0) A.offsets[r] = found;
+    }
+}
+
+// ============================================================ launchers
+static WalkArgs walk_args(State &S, const Params &P, int slot) {
+    WalkArgs a;
+    a.groups = S.groups;
+    a.ngroups = S.ngroups;
+    a.group_cloud = S.group_cloud;
+    a.clouds = S.clouds;
+    a.ncloud = S.ncloud;
+    a.range = S.tree.range;
+    a.child = S.tree.child;
+    a.box_c = S.tree.box_c;
+    a.box_h = S.tree.box_h;
+    a.pk_pos = S.pk_pos;
+    a.pos = S.pos;
+    a.n = S.n;
+    a.stack_cap = P.stack_cap;
+    a.max_depth = S.max_level + 1;
+    a.periodic = P.periodic;
+    for (int d = 0; d < 3; ++d) a.box[d] = P.box[d];
+    a.work = S.work + slot;
+    a.status = S.status;
+    a.counters = S.counters;
+    return a;
+}
+
+static size_t walk_smem(const Params &P, size_t tile_bytes) {
+    return warp_mem_bytes(P.stack_cap, tile_bytes) * kWalkWarps;
+}
+
+static void allow_smem(const void *kern) {
+    static std::mutex mu;
+    static std::set<const void *> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.insert(kern).second)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+template <typename Args>
+static void run_walk(void (*kern)(Args), const Args &args, size_t smem, State &S, cudaStream_t st, int slot) {
+    allow_smem((const void *)kern);
+    cudaMemsetAsync(S.work + slot, 0, sizeof(int), st);
+    kern<<<S.walk_blocks, kWalkWarps * 32, smem, st>>>(args);
+}
+
+void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
+    if (S.ngroups == 0) return;
+    BootArgs A;
+    A.w = walk_args(S, P, 0);
+    A.h = S.h;
+    A.pk_hme = S.pk_hme;
+    A.k = P.n_boot;
+    run_walk(k_boot_h, A, walk_smem(P, sizeof(HTile<double>)), S, st, 0);
+}
+
+void launch_h_search(State &S, const Params &P, cudaStream_t st) {
+    if (S.ngroups == 0) return;
+    HArgs A;
+    A.w = walk_args(S, P, 1);
+    A.h = S.h;
+    A.pk_hme = S.pk_hme;
+    A.nngb = S.nngb;
+    A.n_ngb = P.n_ngb;
+    A.tol = P.n_ngb_tol;
+    A.max_iter = P.h_max_iter;
+    if (P.precision == SPH3_PREC_FP64) {
+        if (P.h_mode == SPH3_H_REFSTEP)
+            run_walk(k_h_search<double, SPH3_H_REFSTEP>, A, walk_smem(P, sizeof(HTile<double>)), S, st, 1);
+        else
+            run_walk(k_h_search<double, SPH3_H_NEWTON>, A, walk_smem(P, sizeof(HTile<double>)), S, st, 1);
+    } else {
+        if (P.h_mode == SPH3_H_REFSTEP)
+            run_walk(k_h_search<float, SPH3_H_REFSTEP>, A, walk_smem(P, sizeof(HTile<float>)), S, st, 1);
+        else
+            run_walk(k_h_search<float, SPH3_H_NEWTON>, A, walk_smem(P, sizeof(HTile<float>)), S, st, 1);
+    }
+}
+
+void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bool keep_rho) {
+    if (S.ngroups == 0) return;
+    DArgs A;
+    A.keep_rho = keep_rho ? 1 : 0;
+    A.w = walk_args(S, P, 2);
+    A.pk_hme = S.pk_hme; A.pk_vel = S.pk_vel;
+    A.h = S.h; A.m = S.m; A.vel = S.vel; A.u = S.u;
+    A.rho = S.rho; A.P = S.P; A.c = S.c; A.divV = S.divV; A.curlV = S.curlV; A.bal = S.bal;
+    A.pk_thm = S.pk_thm;
+    A.gamma = P.gamma;
+    if (P.precision == SPH3_PREC_FP64) {
+        if (divcurl) run_walk(k_density<double, true>, A, walk_smem(P, sizeof(DTile<double, true>)), S, st, 2);
+        else run_walk(k_density<double, false>, A, walk_smem(P, sizeof(DTile<double, false>)), S, st, 2);
+    } else {
+        if (divcurl) run_walk(k_density<float, true>, A, walk_smem(P, sizeof(DTile<float, true>)), S, st, 2);
+        else run_walk(k_density<float, false>, A, walk_smem(P, sizeof(DTile<float, false>)), S, st, 2);
+    }
+}
+
+template <typename R, int V>
+static void hydro_dispatch(const YArgs &A, bool acc, bool du, const Params &P, State &S, cudaStream_t st) {
+    const size_t sm = walk_smem(P, sizeof(YTile<R>));
+    if (acc && du) run_walk(k_hydro<R, V, true, true>, A, sm, S, st, 3);
+    else if (acc) run_walk(k_hydro<R, V, true, false>, A, sm, S, st, 3);
+    else run_walk(k_hydro<R, V, false, true>, A, sm, S, st, 3);
+}
+
+void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cudaStream_t st) {
+    if (S.ngroups == 0 || (!want_acc && !want_dudt)) return;
+    YArgs A;
+    A.w = walk_args(S, P, 3);
+    A.pk_hme = S.pk_hme; A.pk_vel = S.pk_vel; A.pk_thm = S.pk_thm;
+    A.h = S.h; A.m = S.m; A.vel = S.vel; A.rho = S.rho; A.P = S.P; A.c = S.c; A.bal = S.bal;
+    A.acc_sph = S.acc_sph; A.dudt = S.dudt;
+    A.alpha = P.alpha; A.beta = P.beta; A.eta = P.eta;
+    if (P.precision == SPH3_PREC_FP64) {
+        if (P.visc == SPH3_VISC_MG83) hydro_dispatch<double, SPH3_VISC_MG83>(A, want_acc, want_dudt, P, S, st);
+        else if (P.visc == SPH3_VISC_BALSARA) hydro_dispatch<double, SPH3_VISC_BALSARA>(A, want_acc, want_dudt, P, S, st);
+        else hydro_dispatch<double, SPH3_VISC_SIGNAL>(A, want_acc, want_dudt, P, S, st);
+    } else {
+        if (P.visc == SPH3_VISC_MG83) hydro_dispatch<float, SPH3_VISC_MG83>(A, want_acc, want_dudt, P, S, st);
+        else if (P.visc == SPH3_VISC_BALSARA) hydro_dispatch<float, SPH3_VISC_BALSARA>(A, want_acc, want_dudt, P, S, st);
+        else hydro_dispatch<float, SPH3_VISC_SIGNAL>(A, want_acc, want_dudt, P, S, st);
+    }
+}
+
+// P and c from the stored rho and u (getPressure, sph_serial.py:116), plus
+// the Balsara factor from the stored div/curl (shear.py:212-213)
+__global__ void k_eos(int64_t n, double gamma, const double *rho, const double *u, const double *divV,
+                      const double *curlV, const double *h, double *P, double *c, double *bal,
+                      float4 *pk_thm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double r = rho[i];
+        const double p = (gamma - 1.0) * r * u[i];
+        const double cc = sqrt(gamma * (gamma - 1.0) * u[i]);
+        P[i] = p;
+        c[i] = cc;
+        const double f = divV[i] / (divV[i] + curlV[i] + 0.0001 * cc / h[i]);
+        bal[i] = f;
+        pk_thm[i] = make_float4((float)r, (float)(r > 0 ? p / (r * r) : 0.0), (float)cc, (float)f);
+    }
+}
+
+void launch_eos(State &S, const Params &P, cudaStream_t st) {
+    if (S.n == 0) return;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_eos<<<blocks, 256, 0, st>>>(S.n, P.gamma, S.rho, S.u, S.divV, S.curlV, S.h, S.P, S.c, S.bal, S.pk_thm);
+}
+
+__global__ void k_balsara(int64_t n, const double *divV, const double *curlV, const double *c,
+                          const double *h, double *bal, float4 *pk_thm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double f = divV[i] / (divV[i] + curlV[i] + 0.0001 * c[i] / h[i]);
+        bal[i] = f;
+        pk_thm[i].w = (float)f;
+    }
+}
+
+void launch_balsara(State &S, cudaStream_t st) {
+    if (S.n == 0) return;
+    int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+    k_balsara<<<blocks, 256, 0, st>>>(S.n, S.divV, S.curlV, S.c, S.h, S.bal, S.pk_thm);
+}
+
+int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
+                      int64_t *offsets_dev, int64_t *idx_dev, int64_t cap, cudaStream_t st) {
+    if (nrows == 0) return 0;
+    NArgs A;
+    A.w = walk_args(S, P, 4);
+    A.h = S.h;
+    A.orig = S.orig;
+    A.rows = rows_sorted_dev;
+    A.nrows = nrows;
+    A.offsets = offsets_dev;
+    A.out = idx_dev;
+    A.cap = cap;
+    A.cursor = nullptr;
+    const size_t sm = walk_smem(P, sizeof(HTile<double>));
+    allow_smem((const void *)k_neighbours);
+    int blocks = (int)std::min<int64_t>((nrows + kWalkWarps - 1) / kWalkWarps, (int64_t)S.num_sms * 8);
+    // pass 0: counts into offsets[0..nrows)
+    A.pass = 0;
+    k_neighbours<<<blocks, kWalkWarps * 32, sm, st>>>(A);
+    // exclusive scan on the host (few rows)
+    std::vector<int64_t> h(nrows + 1);
+    cudaMemcpyAsync(h.data(), offsets_dev, sizeof(int64_t) * nrows, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    int64_t run = 0;
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t v = h[r];
+        h[r] = run;
+        run += v;
+    }
+    h[nrows] = run;
+    cudaMemcpyAsync(offsets_dev, h.data(), sizeof(int64_t) * (nrows + 1), cudaMemcpyHostToDevice, st);
+    int *cursor = nullptr;
+    cudaMallocAsync(&cursor, sizeof(int) * nrows, st);
+    cudaMemsetAsync(cursor, 0, sizeof(int) * nrows, st);
+    A.cursor = cursor;
+    A.pass = 1;
+    k_neighbours<<<blocks, kWalkWarps * 32, sm, st>>>(A);
+    cudaFreeAsync(cursor, st);
+    cudaStreamSynchronize(st);
+    return 0;
+}
+
+}  // namespace sph3
