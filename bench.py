@@ -155,6 +155,10 @@ def run_ours(args, rank, world, local_rank):
     from sph_3_b200 import Config, Context, costs
 
     torch.cuda.set_device(local_rank)
+    # a real stream: torch's legacy default stream has handle 0, which the C
+    # ABI reads as "the context's own stream"
+    bench_stream = torch.cuda.Stream()
+    torch.cuda.set_stream(bench_stream)
     dist = world > 1
     if dist:
         import torch.distributed as td

@@ -162,7 +162,8 @@ class Context:
 
     def set_particles(self, pos, m, vel=None, u=None, h=None, eps=None):
         n = int(pos.shape[0]) if hasattr(pos, "shape") else len(pos)
-        args = [self._arg(pos, 3, n), self._arg(m, 1, n), self._arg(vel, 3, n), self._arg(u, 1, n),
+        # C order: pos, vel, mass, u, h, eps
+        args = [self._arg(pos, 3, n), self._arg(vel, 3, n), self._arg(m, 1, n), self._arg(u, 1, n),
                 self._arg(h, 1, n), self._arg(eps, 1, n)]
         devs = {a[1] for a in args if a[0] is not None}
         if len(devs) > 1:

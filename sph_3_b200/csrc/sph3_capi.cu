@@ -152,7 +152,8 @@ void free_buffers(sph3_ctx *c) {
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.groups, S.group_cloud, S.clouds};
+                    S.tree.scan_tmp, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     c->carried[0] = c->carried[1] = nullptr;
@@ -167,6 +168,11 @@ void free_buffers(sph3_ctx *c) {
     S.tree = Tree{};
     S.groups = nullptr;
     S.group_cloud = nullptr;
+    S.ngroups_dev = nullptr;
+    S.box_items = nullptr;
+    S.box_item_begin = nullptr;
+    S.box_part = nullptr;
+    S.nbox_items = 0;
     S.clouds = nullptr;
     c->cap_n = -1;
     c->cap_nodes = c->cap_groups = c->cap_clouds = c->cap_sortblk = 0;
@@ -215,7 +221,7 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     CK(dalloc(&S.pk_thm, nn));
     CK(cudaMemset(S.pk_thm, 0, sizeof(float4) * nn));
     c->cap_sortblk = (int)((nn + 2047) / 2048);
-    CK(dalloc(&S.sort_hist, (size_t)256 * c->cap_sortblk));
+    CK(dalloc(&S.sort_hist, (size_t)256 * (c->cap_sortblk + 1)));
     const int cap = (int)std::min<int64_t>(2 * nn + ncloud + 64, (int64_t)INT32_MAX - 1);
     c->cap_nodes = cap;
     Tree &T = S.tree;
@@ -243,6 +249,8 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     c->cap_groups = std::max(ngroups, 1);
     CK(dalloc(&S.groups, c->cap_groups));
     CK(dalloc(&S.group_cloud, c->cap_groups));
+    CK(dalloc(&S.ngroups_dev, 1));
+    CK(cudaMemset(S.ngroups_dev, 0, sizeof(int)));
     c->cap_clouds = std::max(ncloud, 1);
     CK(dalloc(&S.clouds, c->cap_clouds));
     c->cur = 0;
@@ -663,34 +671,50 @@ int sph3_set_particles(sph3_ctx *c, int64_t n, const double *pos, const double *
     while ((1ll << cb) < (int64_t)ncloud) ++cb;
     if (3 * c->cfg.max_level + cb > 63) return SPH3_ERR_INVALID_ARG;
     std::vector<Cloud> cl(ncloud);
-    std::vector<int2> groups;
-    std::vector<int> gcl;
     int64_t at = 0;
     for (int k = 0; k < ncloud; ++k) {
         std::memset(&cl[k], 0, sizeof(Cloud));
         cl[k].begin = at;
         cl[k].end = at + counts[k];
-        for (int64_t g = at; g < at + counts[k]; g += kGroup) {
-            groups.push_back(make_int2((int)g, (int)std::min<int64_t>(kGroup, at + counts[k] - g)));
-            gcl.push_back(k);
-        }
         at += counts[k];
     }
     drop_graphs(c);
-    int rc = alloc_for(c, n, ncloud, (int)groups.size());
+    // walk groups are rebuilt with every tree; at most one per particle
+    int rc = alloc_for(c, n, ncloud, (int)std::max<int64_t>(n, 1));
     if (rc) return rc;
     State &S = c->S;
     S.n = n;
     S.ncloud = ncloud;
-    S.ngroups = (int)groups.size();
+    S.ngroups = (int)n;
     S.cloud_bits = cb;
     S.max_level = c->cfg.max_level;
     S.key_bits = 3 * c->cfg.max_level + cb;
     c->cur_counts = counts;
     CK(cudaMemcpyAsync(S.clouds, cl.data(), sizeof(Cloud) * ncloud, cudaMemcpyHostToDevice, st));
-    if (!groups.empty()) {
-        CK(cudaMemcpyAsync(S.groups, groups.data(), sizeof(int2) * groups.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(S.group_cloud, gcl.data(), sizeof(int) * gcl.size(), cudaMemcpyHostToDevice, st));
+    {
+        // root-cube reduction items: runs of <= kBoxChunk particles per cloud
+        std::vector<int4> items;
+        std::vector<int> ibeg(ncloud + 1, 0);
+        for (int k = 0; k < ncloud; ++k) {
+            ibeg[k] = (int)items.size();
+            for (int64_t b = cl[k].begin; b < cl[k].end; b += kBoxChunk)
+                items.push_back(make_int4(k, (int)b, (int)std::min<int64_t>(b + kBoxChunk, cl[k].end), 0));
+        }
+        ibeg[ncloud] = (int)items.size();
+        if (S.box_items) cudaFree(S.box_items);
+        if (S.box_item_begin) cudaFree(S.box_item_begin);
+        if (S.box_part) cudaFree(S.box_part);
+        S.box_items = nullptr;
+        S.box_item_begin = nullptr;
+        S.box_part = nullptr;
+        S.nbox_items = (int)items.size();
+        CK(dalloc(&S.box_items, items.size()));
+        CK(dalloc(&S.box_item_begin, ibeg.size()));
+        CK(dalloc(&S.box_part, 6 * items.size()));
+        if (!items.empty())
+            CK(cudaMemcpyAsync(S.box_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.box_item_begin, ibeg.data(), sizeof(int) * ibeg.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     }
     CK(cudaMemsetAsync(S.status, 0, sizeof(unsigned), st));
     CK(cudaMemsetAsync(c->fixed, 0, sizeof(double) * kFixed * std::max<int64_t>(n, 1), st));

@@ -38,6 +38,7 @@ constexpr int kWalkWarps = 4;     // warps per walk block
 constexpr int kLeafQ = 96;        // queued leaves per warp before a flush
 constexpr int kNodeQ = 64;        // queued multipole nodes per warp (gravity)
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBoxChunk = 32768;  // particles per root-cube reduction block
 
 // ------------------------------------------------------------ per cloud
 struct Cloud {
@@ -79,10 +80,17 @@ struct Tree {
 struct State {
     int64_t n = 0;
     int ncloud = 0;
-    int ngroups = 0;
+    int ngroups = 0;          // capacity of the group table (n)
     Cloud *clouds = nullptr;  // device [ncloud]
-    int2 *groups = nullptr;   // device [ngroups] {first, count}
+    int2 *groups = nullptr;   // device [n] {first, count}, rebuilt with the tree
     int *group_cloud = nullptr;
+    int *ngroups_dev = nullptr;  // device: number of groups of the current tree
+    // root-cube reduction work items: {cloud, begin, end, 0}, at most
+    // kBoxChunk particles each, items of a cloud contiguous
+    int4 *box_items = nullptr;
+    int *box_item_begin = nullptr;  // [ncloud + 1]
+    double *box_part = nullptr;     // [nbox_items][6]
+    int nbox_items = 0;
     // FP64 masters
     double *pos = nullptr, *vel = nullptr, *acc = nullptr, *acc_g = nullptr, *acc_sph = nullptr;
     double *u = nullptr, *u_prev = nullptr, *dudt = nullptr, *dudt_prev = nullptr;

@@ -9,22 +9,22 @@
 namespace sph3 {
 
 // ------------------------------------------------------------ root cubes
-// One block per cloud: FP64 bbox of its particles (sorted range), then a
-// power-of-two cube [origin, origin + size) that contains them, with origin
-// on the size/2 grid.  Periodic runs use the fixed cube [0, 2^ceil(log2 L)).
-__global__ void k_cloud_boxes(Cloud *clouds, const double *pos, int64_t n, int max_level,
-                              int periodic, double Lx, double Ly, double Lz, unsigned *status) {
-    Cloud &cl = clouds[blockIdx.x];
-    __shared__ double smin[3][32], smax[3][32];
-    __shared__ int sbad;
-    if (threadIdx.x == 0) sbad = 0;
-    __syncthreads();
+// Two kernels.  k_box_partial: one block per work item (a run of at most
+// kBoxChunk particles of one cloud; the item table is fixed per particle
+// layout) writes the FP64 min/max of its run.  k_cloud_boxes: one block per
+// cloud reduces its items and sets a power-of-two cube [origin, origin + size)
+// that contains the cloud, origin on the size/2 grid.  Periodic runs use the
+// fixed cube [0, 2^ceil(log2 L)).
+__global__ void __launch_bounds__(256) k_box_partial(const int4 *items, const double *pos, int64_t n,
+                                                     double *part, unsigned *status) {
+    const int4 it = items[blockIdx.x];  // {cloud, begin, end, 0}
+    __shared__ double smin[3][8], smax[3][8];
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     int bad = 0;
-    for (int64_t k = cl.begin + threadIdx.x; k < cl.end; k += blockDim.x) {
+    for (int64_t k = it.y + threadIdx.x; k < it.z; k += blockDim.x) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            double x = pos[d * n + k];
+            const double x = pos[d * n + k];
             if (!isfinite(x)) {
                 bad = 1;
                 continue;
@@ -36,27 +36,40 @@ __global__ void k_cloud_boxes(Cloud *clouds, const double *pos, int64_t n, int m
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        double a = warp_min(mn[d]), b = warp_max(mx[d]);
+        const double a = warp_min(mn[d]), b = warp_max(mx[d]);
         if (lane == 0) {
             smin[d][wid] = a;
             smax[d][wid] = b;
         }
     }
-    if (bad) atomicOr(&sbad, 1);
+    if (__any_sync(kFull, bad) && lane == 0) atomicOr(status, SPH3_STATUS_NAN_INPUT);
     __syncthreads();
+    if (threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        double lo = DBL_MAX, hi = -DBL_MAX;
+        for (int w = 0; w < 8; ++w) {
+            lo = fmin(lo, smin[d][w]);
+            hi = fmax(hi, smax[d][w]);
+        }
+        part[blockIdx.x * 6 + d] = lo;
+        part[blockIdx.x * 6 + 3 + d] = hi;
+    }
+}
+
+__global__ void k_cloud_boxes(Cloud *clouds, const int *item_begin, const double *part, int max_level,
+                              int periodic, double Lx, double Ly, double Lz) {
+    Cloud &cl = clouds[blockIdx.x];
     if (threadIdx.x == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
         double lo[3], hi[3];
         for (int d = 0; d < 3; ++d) {
             lo[d] = DBL_MAX;
             hi[d] = -DBL_MAX;
-            for (int w = 0; w < nw; ++w) {
-                lo[d] = fmin(lo[d], smin[d][w]);
-                hi[d] = fmax(hi[d], smax[d][w]);
+            for (int it = item_begin[blockIdx.x]; it < item_begin[blockIdx.x + 1]; ++it) {
+                lo[d] = fmin(lo[d], part[it * 6 + d]);
+                hi[d] = fmax(hi[d], part[it * 6 + 3 + d]);
             }
             if (lo[d] > hi[d]) lo[d] = hi[d] = 0.0;  // empty cloud
         }
-        if (sbad) atomicOr(status, SPH3_STATUS_NAN_INPUT);
         double size;
         double org[3];
         if (periodic) {
@@ -92,8 +105,10 @@ __global__ void k_cloud_boxes(Cloud *clouds, const double *pos, int64_t n, int m
 
 void launch_cloud_boxes(State &S, const Params &P, cudaStream_t st) {
     if (S.ncloud == 0) return;
-    k_cloud_boxes<<<S.ncloud, 256, 0, st>>>(S.clouds, S.pos, S.n, S.max_level, P.periodic,
-                                            P.box[0], P.box[1], P.box[2], S.status);
+    if (S.nbox_items > 0)
+        k_box_partial<<<S.nbox_items, 256, 0, st>>>(S.box_items, S.pos, S.n, S.box_part, S.status);
+    k_cloud_boxes<<<S.ncloud, 32, 0, st>>>(S.clouds, S.box_item_begin, S.box_part, S.max_level, P.periodic,
+                                           P.box[0], P.box[1], P.box[2]);
 }
 
 // ------------------------------------------------------------ keys
@@ -163,32 +178,40 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t *key, int
         if (k < n) atomicAdd(&h[(key[k] >> shift) & 255u], 1u);
     }
     __syncthreads();
-    hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+    hist[blockIdx.x * 256 + threadIdx.x] = h[threadIdx.x];  // block-major table
 }
 
-// exclusive scan of m entries by one block of 1024 threads
-__global__ void __launch_bounds__(1024) k_scan_excl(uint32_t *a, int m) {
-    __shared__ uint32_t part[1024];
-    const int per = (m + 1023) / 1024;
-    const int beg = threadIdx.x * per;
-    const int end = min(beg + per, m);
-    uint32_t s = 0;
-    for (int i = beg; i < end; ++i) s += a[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    // Hillis-Steele over 1024 partial sums
-    for (int o = 1; o < 1024; o <<= 1) {
-        uint32_t v = threadIdx.x >= o ? part[threadIdx.x - o] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+// Offsets from the block-major table: thread d scans digit d's column over
+// the blocks (coalesced row loads), then the digit totals are scanned; the
+// digit bases land in hist[nblocks * 256 + d].
+__global__ void __launch_bounds__(256) k_rs_offsets(uint32_t *hist, int nblocks) {
+    __shared__ uint32_t tot[256];
+    const int d = threadIdx.x;
+    uint32_t run = 0;
+    int b = 0;
+    for (; b + 4 <= nblocks; b += 4) {
+        const uint32_t v0 = hist[(b + 0) * 256 + d], v1 = hist[(b + 1) * 256 + d];
+        const uint32_t v2 = hist[(b + 2) * 256 + d], v3 = hist[(b + 3) * 256 + d];
+        hist[(b + 0) * 256 + d] = run;
+        hist[(b + 1) * 256 + d] = run + v0;
+        hist[(b + 2) * 256 + d] = run + v0 + v1;
+        hist[(b + 3) * 256 + d] = run + v0 + v1 + v2;
+        run += v0 + v1 + v2 + v3;
     }
-    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-    for (int i = beg; i < end; ++i) {
-        uint32_t v = a[i];
-        a[i] = run;
+    for (; b < nblocks; ++b) {
+        const uint32_t v = hist[b * 256 + d];
+        hist[b * 256 + d] = run;
         run += v;
     }
+    tot[d] = run;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        const uint32_t v = d >= o ? tot[d - o] : 0u;
+        __syncthreads();
+        tot[d] += v;
+        __syncthreads();
+    }
+    hist[nblocks * 256 + d] = tot[d] - run;  // exclusive digit base
 }
 
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
@@ -199,7 +222,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
     __shared__ uint32_t goff[256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
-    goff[threadIdx.x] = hist[threadIdx.x * nblocks + blockIdx.x];
+    goff[threadIdx.x] = hist[nblocks * 256 + threadIdx.x] + hist[blockIdx.x * 256 + threadIdx.x];
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (kRsItems * 32);
     uint64_t kk[kRsItems];
@@ -255,7 +278,7 @@ void launch_radix_sort(State &S, cudaStream_t st) {
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
         k_rs_hist<<<nb, kRsThreads, 0, st>>>(kin, S.n, shift, S.sort_hist, nb);
-        k_scan_excl<<<1, 1024, 0, st>>>(S.sort_hist, 256 * nb);
+        k_rs_offsets<<<1, 256, 0, st>>>(S.sort_hist, nb);
         k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kin, vin, kout, vout, S.n, shift, S.sort_hist, nb);
         uint64_t *tk = kin;
         kin = kout;

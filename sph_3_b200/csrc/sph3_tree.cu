@@ -73,30 +73,40 @@ __global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, 
 
 // exclusive scan of the child counts of depth d; sets depth_begin[d + 2]
 __global__ void __launch_bounds__(1024) k_tree_scan(Tree T, int d, unsigned *status) {
-    __shared__ int part[1024];
+    // chunks of 4096 counts: 4 consecutive per thread, coalesced
+    __shared__ int warp_tot[32];
+    __shared__ int carry_s;
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
     const int m = end - beg;
-    const int per = (m + 1023) / 1024;
-    const int b = threadIdx.x * per;
-    const int e = min(b + per, m);
-    int s = 0;
-    for (int i = b; i < e; ++i) s += T.nchild_tmp[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < m; base += 4096) {
+        const int idx = base + threadIdx.x * 4;
+        int v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = idx + k < m ? T.nchild_tmp[idx + k] : 0;
+        const int s = v[0] + v[1] + v[2] + v[3];
+        const int incl = warp_incl_scan(s);
+        if (lane == 31) warp_tot[w] = incl;
         __syncthreads();
-        part[threadIdx.x] += v;
+        if (w == 0) {
+            const int t = warp_tot[lane];
+            warp_tot[lane] = warp_incl_scan(t) - t;
+        }
+        __syncthreads();
+        int run = carry + warp_tot[w] + incl - s;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (idx + k < m) T.scan_tmp[idx + k] = run;
+            run += v[k];
+        }
+        if (threadIdx.x == 1023) carry_s = run;
+        __syncthreads();
+        carry = carry_s;
         __syncthreads();
     }
-    int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
-    for (int i = b; i < e; ++i) {
-        int v = T.nchild_tmp[i];
-        T.scan_tmp[i] = run;
-        run += v;
-    }
-    if (threadIdx.x == 1023) {
-        int total = part[1023];
+    if (threadIdx.x == 0) {
+        int total = carry;
         int next = end + total;
         if (next > T.cap) {
             atomicOr(status, SPH3_STATUS_TREE_CAPACITY);
@@ -301,6 +311,75 @@ void launch_tree_refit_h(State &S, cudaStream_t st) {
     for (int d = S.max_level + 1; d >= 0; --d) k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d);
 }
 
+// ------------------------------------------------------------ walk groups
+// Target groups for the walks: spatially compact runs of at most kGroup
+// consecutive particles.  Each internal node with more than kGroup particles
+// packs its consecutive children of <= kGroup particles greedily into groups
+// (so a group lies inside one parent cell) and splits a child leaf of more
+// than kGroup particles into kGroup-sized chunks; a small or leaf root is
+// handled the same way.  Every particle lands in exactly one group: along
+// its root-to-leaf chain the first node with <= kGroup particles is packed by
+// its parent, and a chain without one ends in an oversized leaf that is
+// chunked.  Group order in the table does not affect any result.
+__device__ __forceinline__ void emit_group(int2 *groups, int *gcl, int *ng, int first, int count, int cloud) {
+    const int g = atomicAdd(ng, 1);
+    groups[g] = make_int2(first, count);
+    gcl[g] = cloud;
+}
+
+__global__ void k_make_groups(Tree T, int ncloud, int max_depth, const uint64_t *key, int max_level,
+                              int2 *groups, int *gcl, int *ng) {
+    const int nn = T.depth_begin[max_depth];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        const int2 r = T.range[i];
+        if (r.y == 0) continue;
+        const int cloud = (int)(key[r.x] >> (3 * max_level));
+        const int2 ch = T.child[i];
+        const int nch = ch.y & 255;
+        if (i < ncloud) {  // a cloud root that nobody packs
+            if (r.y <= kGroup) {
+                emit_group(groups, gcl, ng, r.x, r.y, cloud);
+                continue;
+            }
+            if (nch == 0) {
+                for (int f = r.x; f < r.x + r.y; f += kGroup)
+                    emit_group(groups, gcl, ng, f, min(kGroup, r.x + r.y - f), cloud);
+                continue;
+            }
+        }
+        if (nch == 0 || r.y <= kGroup) continue;
+        int open_first = -1, open_count = 0;
+        for (int c = ch.x; c < ch.x + nch; ++c) {
+            const int2 cr = T.range[c];
+            const bool leaf = (T.child[c].y & 255) == 0;
+            if (cr.y <= kGroup) {
+                if (open_first >= 0 && open_count + cr.y <= kGroup) {
+                    open_count += cr.y;
+                } else {
+                    if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+                    open_first = cr.x;
+                    open_count = cr.y;
+                }
+            } else {
+                if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+                open_first = -1;
+                open_count = 0;
+                if (leaf)
+                    for (int f = cr.x; f < cr.x + cr.y; f += kGroup)
+                        emit_group(groups, gcl, ng, f, min(kGroup, cr.x + cr.y - f), cloud);
+            }
+        }
+        if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+    }
+}
+
+void launch_groups(State &S, cudaStream_t st) {
+    cudaMemsetAsync(S.ngroups_dev, 0, sizeof(int), st);
+    if (S.ncloud == 0 || S.n == 0) return;
+    k_make_groups<<<S.num_sms * 4, 256, 0, st>>>(S.tree, S.ncloud, S.max_level + 2, S.key, S.max_level,
+                                                S.groups, S.group_cloud, S.ngroups_dev);
+}
+
 void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
     if (S.ncloud == 0) return;
     Tree &T = S.tree;
@@ -318,6 +397,7 @@ void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
     a.inv_theta = P.theta > 0 ? 1.0 / P.theta : __builtin_inf();
     for (int d = maxd; d >= 0; --d) k_tree_moments<<<blocks, 128, 0, st>>>(T, a, d, P.quadrupole);
     k_tree_totals<<<blocks, 256, 0, st>>>(T, maxd + 1, S.counters);
+    launch_groups(S, st);
 }
 
 }  // namespace sph3

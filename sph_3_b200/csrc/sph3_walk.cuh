@@ -51,10 +51,15 @@ __device__ inline WarpMem carve_warp_mem(unsigned char *base, int stack_cap, siz
     return m;
 }
 
-// next group index for this warp (one atomic per group)
-__device__ __forceinline__ int next_group(int *work) {
+// next group index for this warp (one atomic per group); no work at all once
+// non-finite input has been flagged, so garbage cannot turn into an
+// all-pairs walk over a degenerate tree
+__device__ __forceinline__ int next_group(int *work, const unsigned *status) {
     int g = 0;
-    if (lane_id() == 0) g = atomicAdd(work, 1);
+    if (lane_id() == 0) {
+        const unsigned s = *reinterpret_cast<const volatile unsigned *>(status);
+        g = (s & SPH3_STATUS_NAN_INPUT) ? 0x7fffffff : atomicAdd(work, 1);
+    }
     return __shfl_sync(kFull, g, 0);
 }
 
@@ -129,12 +134,21 @@ __device__ __forceinline__ int pop_width(int top, int cap, int max_depth) {
     return p;
 }
 
-// Runs `visit` over every particle of the queued leaves in tiles of 32:
-// stage(lane_slot, j) fills the tile entry of sorted particle j, then
-// interact(ne) runs every lane's target against the ne staged entries.
-template <class Stage, class Interact>
+// 4-wide tile component: one 128-bit (FP32) or two 128-bit (FP64) shared
+// loads per entry field group; every lane reads the same entry (broadcast).
+template <typename R>
+struct alignas(4 * sizeof(R)) V4 {
+    R x, y, z, w;
+};
+
+// Streams every particle of the queued leaves through a double-buffered
+// 32-entry tile (tile[0..63]): the loads of the next 32 candidates are in
+// flight while the lanes run the current ones.  load(j) returns the tile
+// entry of sorted particle j (global loads + conversion to the group frame);
+// interact(tile, ne) runs every lane's target against ne staged entries.
+template <class E, class Load, class Interact>
 __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq, int nleaf,
-                                             int *lfirst, int *lpre, Stage &stage,
+                                             int *lfirst, int *lpre, E *tile, Load &load,
                                              Interact &interact) {
     const int lane = lane_id();
     for (int base = 0; base < nleaf; base += 32) {
@@ -151,55 +165,73 @@ __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq
         lpre[lane] = incl - cnt;
         __syncwarp();
         const int nl = min(32, nleaf - base);
-        for (int c0 = 0; c0 < tot; c0 += 32) {
+        auto fetch = [&](int c0, E &out) -> bool {
             const int t = c0 + lane;
-            if (t < tot) {
-                int lo = 0, hi = nl - 1;
-                while (lo < hi) {
-                    int mid = (lo + hi + 1) >> 1;
-                    if (lpre[mid] <= t) lo = mid;
-                    else hi = mid - 1;
-                }
-                stage(lane, lfirst[lo] + (t - lpre[lo]));
+            if (t >= tot) return false;
+            int lo = 0, hi = nl - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (lpre[mid] <= t) lo = mid;
+                else hi = mid - 1;
             }
+            out = load(lfirst[lo] + (t - lpre[lo]));
+            return true;
+        };
+        E cur;
+        bool have = fetch(0, cur);
+        int buf = 0;
+        for (int c0 = 0; c0 < tot; c0 += 32) {
+            if (have) tile[buf * 32 + lane] = cur;
             __syncwarp();
-            interact(min(32, tot - c0));
-            __syncwarp();
+            have = c0 + 32 < tot ? fetch(c0 + 32, cur) : false;
+            interact(tile + buf * 32, min(32, tot - c0));
+            buf ^= 1;
         }
+        __syncwarp();
     }
 }
 
-// Periodic images needed by a group whose reach is R: shifts in {-L, 0, L}
-// per periodic axis where the reach crosses the domain boundary.  Returns
-// the number of images and fills sh[] (first entry is the identity).
-__device__ __forceinline__ int group_images(const GroupBox &g, float R, const double *box,
-                                            int periodic, float3 *sh) {
-    if (!periodic) {
-        sh[0] = make_float3(0.f, 0.f, 0.f);
-        return 1;
-    }
-    float opt[3][3];
-    int no[3];
+// Periodic images needed by a group whose reach is R.  Per axis a 3-bit
+// mask: bit 0 the identity, bit 1 the shift -L (reach crosses 0), bit 2 the
+// shift +L (reach crosses L).  Image codes 0..26 combine one option per axis
+// (code = ox + 3 oy + 9 oz); code 0 is the identity.  No arrays, so nothing
+// lands in local memory.
+struct Images {
+    int mask;  // 3 bits per axis
+};
+
+__device__ __forceinline__ Images group_images(const GroupBox &g, float R, const double *box, int periodic) {
+    Images im;
+    im.mask = 1 | (1 << 3) | (1 << 6);
+    if (!periodic) return im;
     const float gc[3] = {g.c.x, g.c.y, g.c.z};
     const float gh[3] = {g.hw.x, g.hw.y, g.hw.z};
     const int rc[3] = {g.ref & 1023, (g.ref >> 10) & 1023, g.ref >> 20};
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
-        no[d] = 1;
-        opt[d][0] = 0.f;
         const float L = (float)box[d];
         if (L > 0.f) {
             // absolute coordinate of the box edges (periodic root cube starts at 0)
             const float corner = rc[d] * g.s10;
             const float lo = corner + gc[d] - gh[d], hi = corner + gc[d] + gh[d];
-            if (lo - R < 0.f) opt[d][no[d]++] = -L;
-            if (hi + R > L) opt[d][no[d]++] = L;
+            if (lo - R < 0.f) im.mask |= 2 << (3 * d);
+            if (hi + R > L) im.mask |= 4 << (3 * d);
         }
     }
-    int k = 0;
-    for (int a = 0; a < no[0]; ++a)
-        for (int b = 0; b < no[1]; ++b)
-            for (int c = 0; c < no[2]; ++c) sh[k++] = make_float3(opt[0][a], opt[1][b], opt[2][c]);
-    return k;
+    return im;
+}
+
+// shift of image `code` if the group needs it
+__device__ __forceinline__ bool image_shift(const Images &im, int code, const double *box, float3 &s) {
+    const int o[3] = {code % 3, (code / 3) % 3, code / 9};
+    float v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!((im.mask >> (3 * d + o[d])) & 1)) return false;
+        v[d] = o[d] == 0 ? 0.f : (o[d] == 1 ? -(float)box[d] : (float)box[d]);
+    }
+    s = make_float3(v[0], v[1], v[2]);
+    return true;
 }
 
 }  // namespace sph3

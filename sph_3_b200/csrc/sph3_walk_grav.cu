@@ -1,15 +1,17 @@
 // Barnes-Hut gravity with spline softening, and the FP64 direct sum.
 //
-// One warp per 32-particle group walks the octree once.  A node is accepted
-// as a multipole for the whole group when the distance d from its centre of
-// mass to the group's bounding box satisfies
+// One warp per compact group (<= 32 particles) walks the octree once.  A node
+// is accepted as a multipole for the whole group when the distance d from its
+// centre of mass to the group's bounding box satisfies
 //     d > s / theta + delta          (s: node bbox side, delta: |com - bbox centre|)
 //     d > b_max + eps_max_node + eps_max_group   (outside every softening kernel)
 // otherwise a leaf is opened into particle-particle terms with the reference's
 // softened kernel (sph_code/libsx.py:640-652 force, :609-616 potential) and an
 // internal node is opened into its children.  theta = 0 never accepts a node,
 // so the walk becomes the exact direct sum.  Multipoles are monopole +
-// traceless quadrupole about the centre of mass.
+// traceless quadrupole about the centre of mass.  Accepted nodes and opened
+// leaves are queued and streamed through double-buffered shared-memory tiles
+// of 4-wide entries (broadcast reads).
 #include <cfloat>
 #include <mutex>
 #include <set>
@@ -20,7 +22,7 @@ namespace sph3 {
 
 struct GArgs {
     const int2 *groups;
-    int ngroups;
+    const int *ngroups_dev;
     const int *group_cloud;
     const Cloud *clouds;
     const int2 *range;
@@ -46,20 +48,24 @@ struct GArgs {
     unsigned long long *counters;
 };
 
+// node entry: a = {com (group frame), mass}, b = {qxx, qxy, qxz, qyy}, qyz
 template <typename R>
-struct GNodeTile {
-    R x[32], y[32], z[32], m[32], qxx[32], qxy[32], qxz[32], qyy[32], qyz[32];
+struct GN {
+    V4<R> a, b;
+    R qyz;
 };
 
+// particle entry: p = {pos (group frame), mass}, e = softening length
 template <typename R>
-struct GPartTile {
-    R x[32], y[32], z[32], m[32], e[32];
+struct GP {
+    V4<R> p;
+    R e;
 };
 
 template <typename R>
 struct GTile {
-    GNodeTile<R> nd;
-    GPartTile<R> pt;
+    GN<R> nd[64];
+    GP<R> pt[64];
     int nodeq[kNodeQ];
 };
 
@@ -100,14 +106,14 @@ __device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R eps
     ph -= mj * pk;
 }
 
-template <typename R>
+template <typename R, bool QUAD>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTile<R>));
     GTile<R> &tile = *reinterpret_cast<GTile<R> *>(wm.tile);
     const int lane = lane_id();
     unsigned long long n_node = 0, n_part = 0;
-    for (int g = next_group(A.work); g < A.ngroups; g = next_group(A.work)) {
+    for (int g = next_group(A.work, A.status); g < *A.ngroups_dev; g = next_group(A.work, A.status)) {
         const int2 gr = A.groups[g];
         const Cloud &cl = A.clouds[A.group_cloud[g]];
         const int ref = __float_as_int(A.pk_pos[gr.x].w);
@@ -126,95 +132,113 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
         const float eps_g = warp_max(active ? (float)te : 0.f);
         R ax = 0, ay = 0, az = 0, ph = 0;
 
-        // ---- flushes
-        auto flush_nodes = [&](int nq) {
-            for (int base = 0; base < nq; base += 32) {
-                const int ne = min(32, nq - base);
-                if (lane < ne) {
-                    const int nd = tile.nodeq[base + lane];
-                    if (sizeof(R) == 8) {
-                        tile.nd.x[lane] = (R)A.tcom[nd];
-                        tile.nd.y[lane] = (R)A.tcom[A.cap + nd];
-                        tile.nd.z[lane] = (R)A.tcom[2 * A.cap + nd];
-                        tile.nd.m[lane] = (R)A.tmass[nd];
-                        tile.nd.qxx[lane] = (R)A.tquad[nd];
-                        tile.nd.qxy[lane] = (R)A.tquad[A.cap + nd];
-                        tile.nd.qxz[lane] = (R)A.tquad[2 * A.cap + nd];
-                        tile.nd.qyy[lane] = (R)A.tquad[3 * A.cap + nd];
-                        tile.nd.qyz[lane] = (R)A.tquad[4 * A.cap + nd];
-                    } else {
-                        const float3 c = rel_to(A.com_c[nd], ref, cl.s10);
-                        tile.nd.x[lane] = (R)c.x;
-                        tile.nd.y[lane] = (R)c.y;
-                        tile.nd.z[lane] = (R)c.z;
-                        tile.nd.m[lane] = (R)A.mono[nd].x;
-                        const float4 q = A.quad4[nd];
-                        tile.nd.qxx[lane] = (R)q.x;
-                        tile.nd.qxy[lane] = (R)q.y;
-                        tile.nd.qxz[lane] = (R)q.z;
-                        tile.nd.qyy[lane] = (R)q.w;
-                        tile.nd.qyz[lane] = (R)A.quad1[nd];
-                    }
+        // ---- multipole list: double-buffered chunks of 32 nodes
+        auto load_node = [&](int nd) {
+            GN<R> en;
+            if (sizeof(R) == 8) {
+                en.a.x = (R)A.tcom[nd];
+                en.a.y = (R)A.tcom[A.cap + nd];
+                en.a.z = (R)A.tcom[2 * A.cap + nd];
+                en.a.w = (R)A.tmass[nd];
+                if (QUAD) {
+                    en.b.x = (R)A.tquad[nd];
+                    en.b.y = (R)A.tquad[A.cap + nd];
+                    en.b.z = (R)A.tquad[2 * A.cap + nd];
+                    en.b.w = (R)A.tquad[3 * A.cap + nd];
+                    en.qyz = (R)A.tquad[4 * A.cap + nd];
                 }
-                __syncwarp();
-                if (active) {
-                    n_node += ne;
-                    for (int e = 0; e < ne; ++e) {
-                        const R dx = tx - tile.nd.x[e], dy = ty - tile.nd.y[e], dz = tz - tile.nd.z[e];
-                        const R r2 = dx * dx + dy * dy + dz * dz;
-                        const R rinv = rsq(r2);
-                        const R rinv2 = rinv * rinv;
-                        const R M = tile.nd.m[e];
-                        const R mr3 = M * rinv * rinv2;
-                        ax -= mr3 * dx;
-                        ay -= mr3 * dy;
-                        az -= mr3 * dz;
-                        ph -= M * rinv;
-                        if (A.quad) {
-                            const R qxx = tile.nd.qxx[e], qxy = tile.nd.qxy[e], qxz = tile.nd.qxz[e];
-                            const R qyy = tile.nd.qyy[e], qyz = tile.nd.qyz[e];
-                            const R qzz = -qxx - qyy;
-                            const R Qx = qxx * dx + qxy * dy + qxz * dz;
-                            const R Qy = qxy * dx + qyy * dy + qyz * dz;
-                            const R Qz = qxz * dx + qyz * dy + qzz * dz;
-                            const R rQr = dx * Qx + dy * Qy + dz * Qz;
-                            const R rinv5 = rinv2 * rinv2 * rinv;
-                            const R t = (R)2.5 * rQr * rinv5 * rinv2;
-                            ax += Qx * rinv5 - t * dx;
-                            ay += Qy * rinv5 - t * dy;
-                            az += Qz * rinv5 - t * dz;
-                            ph -= (R)0.5 * rQr * rinv5;
-                        }
-                    }
+            } else {
+                const float3 c = rel_to(A.com_c[nd], ref, cl.s10);
+                en.a.x = (R)c.x;
+                en.a.y = (R)c.y;
+                en.a.z = (R)c.z;
+                en.a.w = (R)A.mono[nd].x;
+                if (QUAD) {
+                    const float4 q = A.quad4[nd];
+                    en.b.x = (R)q.x;
+                    en.b.y = (R)q.y;
+                    en.b.z = (R)q.z;
+                    en.b.w = (R)q.w;
+                    en.qyz = (R)A.quad1[nd];
                 }
-                __syncwarp();
+            }
+            return en;
+        };
+        auto node_interact = [&](const GN<R> *t, int ne) {
+            if (!active) return;
+            n_node += ne;
+            for (int e = 0; e < ne; ++e) {
+                const V4<R> a4 = t[e].a;
+                const R dx = tx - a4.x, dy = ty - a4.y, dz = tz - a4.z;
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                const R rinv = rsq(r2);
+                const R rinv2 = rinv * rinv;
+                const R M = a4.w;
+                const R mr3 = M * rinv * rinv2;
+                ax -= mr3 * dx;
+                ay -= mr3 * dy;
+                az -= mr3 * dz;
+                ph -= M * rinv;
+                if (QUAD) {
+                    const V4<R> b4 = t[e].b;
+                    const R qyz = t[e].qyz;
+                    const R qzz = -b4.x - b4.w;
+                    const R Qx = b4.x * dx + b4.y * dy + b4.z * dz;
+                    const R Qy = b4.y * dx + b4.w * dy + qyz * dz;
+                    const R Qz = b4.z * dx + qyz * dy + qzz * dz;
+                    const R rQr = dx * Qx + dy * Qy + dz * Qz;
+                    const R rinv5 = rinv2 * rinv2 * rinv;
+                    const R tq = (R)2.5 * rQr * rinv5 * rinv2;
+                    ax += Qx * rinv5 - tq * dx;
+                    ay += Qy * rinv5 - tq * dy;
+                    az += Qz * rinv5 - tq * dz;
+                    ph -= (R)0.5 * rQr * rinv5;
+                }
             }
         };
-        auto stage = [&](int slot, int j) {
+        auto flush_nodes = [&](int nq) {
+            GN<R> cur;
+            bool have = lane < nq;
+            if (have) cur = load_node(tile.nodeq[lane]);
+            int buf = 0;
+            for (int base = 0; base < nq; base += 32) {
+                if (have) tile.nd[buf * 32 + lane] = cur;
+                __syncwarp();
+                have = base + 32 + lane < nq;
+                if (have) cur = load_node(tile.nodeq[base + 32 + lane]);
+                node_interact(tile.nd + buf * 32, min(32, nq - base));
+                buf ^= 1;
+            }
+            __syncwarp();
+        };
+        // ---- opened leaves: particle-particle terms
+        auto load_part = [&](int j) {
+            GP<R> en;
             if (sizeof(R) == 8) {
-                tile.pt.x[slot] = (R)A.pos[j];
-                tile.pt.y[slot] = (R)A.pos[A.n + j];
-                tile.pt.z[slot] = (R)A.pos[2 * A.n + j];
-                tile.pt.m[slot] = (R)A.m[j];
-                tile.pt.e[slot] = (R)A.eps[j];
+                en.p.x = (R)A.pos[j];
+                en.p.y = (R)A.pos[A.n + j];
+                en.p.z = (R)A.pos[2 * A.n + j];
+                en.p.w = (R)A.m[j];
+                en.e = (R)A.eps[j];
             } else {
                 const float3 p = rel_to(A.pk_pos[j], ref, cl.s10);
-                tile.pt.x[slot] = (R)p.x;
-                tile.pt.y[slot] = (R)p.y;
-                tile.pt.z[slot] = (R)p.z;
                 const float4 hm = A.pk_hme[j];
-                tile.pt.m[slot] = (R)hm.y;
-                tile.pt.e[slot] = (R)hm.z;
+                en.p.x = (R)p.x;
+                en.p.y = (R)p.y;
+                en.p.z = (R)p.z;
+                en.p.w = (R)hm.y;
+                en.e = (R)hm.z;
             }
+            return en;
         };
-        auto interact = [&](int ne) {
+        auto part_interact = [&](const GP<R> *t, int ne) {
             if (!active) return;
             n_part += ne;
             for (int e = 0; e < ne; ++e) {
-                const R dx = tx - tile.pt.x[e], dy = ty - tile.pt.y[e], dz = tz - tile.pt.z[e];
+                const V4<R> p4 = t[e].p;
+                const R dx = tx - p4.x, dy = ty - p4.y, dz = tz - p4.z;
                 const R r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > (R)0)
-                    spline_force<R>(r2, dx, dy, dz, tile.pt.m[e], (R)0.5 * (te + tile.pt.e[e]), ax, ay, az, ph);
+                if (r2 > (R)0) spline_force<R>(r2, dx, dy, dz, p4.w, (R)0.5 * (te + t[e].e), ax, ay, az, ph);
             }
         };
 
@@ -223,7 +247,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
         if (lane == 0) wm.stack[0] = cl.root;
         __syncwarp();
         int nleaf = 0, nnode = 0;
-        while (top > 0) {
+        // each node is popped at most once; the bound only trips on a corrupted tree
+        for (int guard = 0; top > 0; ++guard) {
+            if (guard > A.cap) {
+                if (lane == 0) set_status(A.status, SPH3_STATUS_STACK_OVERFLOW);
+                break;
+            }
             const int p = pop_width(top, A.stack_cap, A.max_depth);
             int node = -1;
             if (lane < p) node = wm.stack[top - 1 - lane];
@@ -261,13 +290,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
                 nnode = 0;
             }
             if (nleaf > kLeafQ - 32) {
-                flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, stage, interact);
+                flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
                 nleaf = 0;
             }
         }
         __syncwarp();
         if (nnode > 0) flush_nodes(nnode);
-        if (nleaf > 0) flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, stage, interact);
+        if (nleaf > 0) flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
         if (active) {
             A.acc_g[i] = A.G * (double)ax;
             A.acc_g[A.n + i] = A.G * (double)ay;
@@ -291,11 +320,18 @@ static void allow_smem_g(const void *kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
+template <typename R, bool QUAD>
+static void launch_grav_t(const GArgs &A, State &S, const Params &P, cudaStream_t st) {
+    const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<R>)) * kWalkWarps;
+    allow_smem_g((const void *)k_gravity<R, QUAD>);
+    k_gravity<R, QUAD><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+}
+
 void launch_gravity(State &S, const Params &P, cudaStream_t st) {
-    if (S.ngroups == 0) return;
+    if (S.n == 0) return;
     GArgs A;
     A.groups = S.groups;
-    A.ngroups = S.ngroups;
+    A.ngroups_dev = S.ngroups_dev;
     A.group_cloud = S.group_cloud;
     A.clouds = S.clouds;
     A.range = S.tree.range;
@@ -325,13 +361,11 @@ void launch_gravity(State &S, const Params &P, cudaStream_t st) {
     A.counters = S.counters;
     cudaMemsetAsync(A.work, 0, sizeof(int), st);
     if (P.precision == SPH3_PREC_FP64) {
-        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<double>)) * kWalkWarps;
-        allow_smem_g((const void *)k_gravity<double>);
-        k_gravity<double><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+        if (P.quadrupole) launch_grav_t<double, true>(A, S, P, st);
+        else launch_grav_t<double, false>(A, S, P, st);
     } else {
-        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<float>)) * kWalkWarps;
-        allow_smem_g((const void *)k_gravity<float>);
-        k_gravity<float><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+        if (P.quadrupole) launch_grav_t<float, true>(A, S, P, st);
+        else launch_grav_t<float, false>(A, S, P, st);
     }
 }
 

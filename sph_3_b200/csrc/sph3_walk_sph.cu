@@ -2,9 +2,10 @@
 // hydro acceleration + du/dt pass, plus the neighbour-set export used by the
 // parity tests.
 //
-// Every pass is one persistent kernel: warps pull 32-particle groups from an
-// atomic counter, walk the octree once per group (sph3_walk.cuh) and stream
-// the candidate leaves through a 32-entry shared-memory tile.  Two
+// Every pass is one persistent kernel: warps pull compact particle groups
+// (<= 32, built from the octree) from an atomic counter, walk the octree once
+// per group (sph3_walk.cuh) and stream the candidate leaves through a
+// double-buffered 32-entry shared-memory tile of 4-wide entries.  Two
 // instantiations per pass:
 //   float  -- mixed precision: positions in the FP32 frame of the group's
 //             reference cell (exact integer cell offsets + FP32 in-cell
@@ -30,7 +31,7 @@ constexpr float kSigF = 0.31830988618379067154f;
 // ------------------------------------------------------------ arguments
 struct WalkArgs {
     const int2 *groups;
-    int ngroups;
+    const int *ngroups_dev;
     const int *group_cloud;
     const Cloud *clouds;
     int ncloud;
@@ -43,6 +44,7 @@ struct WalkArgs {
     int64_t n;
     int stack_cap;
     int max_depth;
+    int node_cap;
     int periodic;
     double box[3];
     int *work;
@@ -50,8 +52,8 @@ struct WalkArgs {
     unsigned long long *counters;
 };
 
-// division and reciprocal in the pass precision: the FP32 path uses the
-// approximate hardware reciprocal, the FP64 path IEEE division
+// division in the pass precision: the FP32 path uses the approximate
+// hardware reciprocal, the FP64 path IEEE division
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 
@@ -60,8 +62,10 @@ __device__ __forceinline__ double exact_dist(double dx, double dy, double dz) {
     return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
 }
 
-// Walk the tree for one group, calling flush(leafq, nleaf) on full queues.
-// reach(node) = Rg + (node_h ? hmax_node : 0); images shift the nodes.
+// Walk the tree for one group, calling flush(nleaf) on full leaf queues.
+// A node is kept if the gap between its bbox and the group bbox is at most
+// reach = Rg + (node_h ? hmax_node : 0) (times a 4e-5 safety margin; the
+// exact pair predicate decides); images shift the nodes by `shift`.
 template <class Flush>
 __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, const GroupBox &gb,
                                float Rg, bool node_h, float3 shift, Flush &flush) {
@@ -71,7 +75,13 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
     __syncwarp();
     int nleaf = 0;
     const float margin = 1.0f + 4e-5f;
-    while (top > 0) {
+    // every node is popped at most once per walk; the bound only trips on a
+    // corrupted tree, which then raises a status bit instead of spinning
+    for (int guard = 0; top > 0; ++guard) {
+        if (guard > a.node_cap) {
+            if (lane == 0) set_status(a.status, SPH3_STATUS_STACK_OVERFLOW);
+            break;
+        }
         const int p = pop_width(top, a.stack_cap, a.max_depth);
         int node = -1;
         if (lane < p) node = wm.stack[top - 1 - lane];
@@ -114,13 +124,6 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
 }
 
 // ------------------------------------------------------------ group setup
-template <typename R>
-struct Target {
-    R x, y, z;
-};
-
-__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
-
 struct GroupInfo {
     int first, count, cloud, i;
     bool active;
@@ -147,6 +150,24 @@ __device__ __forceinline__ GroupInfo group_info(const WalkArgs &a, int g) {
     return gi;
 }
 
+// source position in the group frame: FP32 relative (mixed) or absolute FP64
+template <typename R>
+__device__ __forceinline__ V4<R> src_pos(const WalkArgs &a, const GroupInfo &gi, int j, float3 s, R w) {
+    V4<R> p;
+    if (sizeof(R) == 8) {
+        p.x = (R)(a.pos[j] + (double)s.x);
+        p.y = (R)(a.pos[a.n + j] + (double)s.y);
+        p.z = (R)(a.pos[2 * a.n + j] + (double)s.z);
+    } else {
+        const float3 q = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+        p.x = (R)(q.x + s.x);
+        p.y = (R)(q.y + s.y);
+        p.z = (R)(q.z + s.z);
+    }
+    p.w = w;
+    return p;
+}
+
 // ================================================================= h search
 struct HArgs {
     WalkArgs w;
@@ -156,30 +177,25 @@ struct HArgs {
     int n_ngb, tol, max_iter;
 };
 
-template <typename R>
-struct HTile {
-    R x[32], y[32], z[32];
-};
-
-constexpr int kHK = 16;          // thresholds per pass in the reference-step mode
+constexpr int kHK = 16;  // thresholds per pass in the reference-step mode
 constexpr double kNewtonDelta = 0.08;
 
 template <typename R, int MODE>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<R>));
-    HTile<R> &tile = *reinterpret_cast<HTile<R> *>(wm.tile);
+    using E = V4<R>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     constexpr int K = MODE == SPH3_H_REFSTEP ? kHK : 2;
     const int up = A.n_ngb + A.tol, low = A.n_ngb - A.tol;
     unsigned long long pairs = 0, passes = 0;
-    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+    for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         const Cloud &cl = a.clouds[gi.cloud];
         const int64_t ncl = cl.end - cl.begin;
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
-        // target position in the pass precision
         R tx, ty, tz;
         if (sizeof(R) == 8) {
             tx = (R)a.pos[gi.i];
@@ -194,14 +210,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
         if (!(h > 0.0) || !isfinite(h)) h = (double)gi.s10;  // no usable start: one level-10 cell
         bool conv = !gi.active;
         int ncount = 0;
-        int steps = 0;      // reference-rule steps taken
-        int dir = 0;        // reference rule: -1 down, +1 up, 0 unknown (first pass)
+        int steps = 0;  // reference-rule steps taken
+        int dir = 0;    // reference rule: -1 down, +1 up, 0 unknown (first pass)
         double lb = 0.0, hb = DBL_MAX;
         bool failed = false;
         const double hcap = 4.0 * cl.size;
         for (int pass = 0; pass < A.max_iter + 2; ++pass) {
             if (__all_sync(kFull, conv)) break;
-            // thresholds for this pass
             double thr[K];
             if (MODE == SPH3_H_REFSTEP) {
                 if (dir == 0) {
@@ -232,57 +247,44 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
             int cnt[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) cnt[k] = 0;
-            // images (periodic) and the walk
-            float3 sh[27];
-            const int nim = group_images(gb, reach, a.box, a.periodic, sh);
-            for (int im = 0; im < nim; ++im) {
-                const float3 s = sh[im];
-                auto stage = [&](int slot, int j) {
-                    if (sizeof(R) == 8) {
-                        tile.x[slot] = (R)(a.pos[j] + (double)s.x);
-                        tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
-                        tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
-                    } else {
-                        float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
-                        tile.x[slot] = (R)(p.x + s.x);
-                        tile.y[slot] = (R)(p.y + s.y);
-                        tile.z[slot] = (R)(p.z + s.z);
-                    }
-                };
-                auto interact = [&](int ne) {
+            const Images ims = group_images(gb, reach, a.box, a.periodic);
+            for (int im = 0; im < 27; ++im) {
+                float3 s;
+                if (!image_shift(ims, im, a.box, s)) continue;
+                auto load = [&](int j) { return src_pos<R>(a, gi, j, s, (R)0); };
+                auto interact = [&](const E *t, int ne) {
                     if (conv) return;
                     pairs += ne;
                     for (int e = 0; e < ne; ++e) {
+                        const E q = t[e];
                         if (sizeof(R) == 8) {
-                            const double d = exact_dist((double)tile.x[e] - (double)tx,
-                                                        (double)tile.y[e] - (double)ty,
-                                                        (double)tile.z[e] - (double)tz);
+                            const double d = exact_dist((double)q.x - (double)tx, (double)q.y - (double)ty,
+                                                        (double)q.z - (double)tz);
 #pragma unroll
                             for (int k = 0; k < K; ++k) cnt[k] += d < thr[k];
                         } else {
-                            const float dx = (float)tile.x[e] - (float)tx;
-                            const float dy = (float)tile.y[e] - (float)ty;
-                            const float dz = (float)tile.z[e] - (float)tz;
+                            const float dx = (float)q.x - (float)tx;
+                            const float dy = (float)q.y - (float)ty;
+                            const float dz = (float)q.z - (float)tz;
                             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 #pragma unroll
                             for (int k = 0; k < K; ++k) cnt[k] += d2 < thr2f[k];
                         }
                     }
                 };
-                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+                auto flush = [&](int nl) {
+                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                };
                 collect_leaves(a, wm, gi.root, gb, reach, false, s, flush);
             }
             ++passes;
-            if (conv) continue;
-            // ---- update
-            if (MODE == SPH3_H_REFSTEP) {
+            // ---- update (lanes already converged keep their h)
+            if (conv) {
+            } else if (MODE == SPH3_H_REFSTEP) {
                 if (dir == 0) {
                     ncount = cnt[0];
-                    if (ncount <= up && ncount >= low) {
-                        conv = true;
-                    } else {
-                        dir = ncount > up ? -1 : 1;
-                    }
+                    if (ncount <= up && ncount >= low) conv = true;
+                    else dir = ncount > up ? -1 : 1;
                 } else {
                     double hk = h;
                     for (int k = 0; k < K; ++k) {
@@ -317,15 +319,17 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
                     failed = true;
                     conv = true;
                 } else {
+                    // Newton step on ln N(ln h) with the slope measured between
+                    // h and h (1 + delta), safeguarded by the bracket [lb, hb]
                     if (n0 > up) hb = fmin(hb, h);
                     else lb = fmax(lb, h);
                     double hn;
                     if (n0 == 0) {
                         hn = 2.0 * h;
                     } else {
-                        double s = n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
-                        s = fmin(fmax(s, 1.0), 6.0);
-                        hn = h * exp((log((double)A.n_ngb) - log((double)n0)) / s);
+                        double sl = n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
+                        sl = fmin(fmax(sl, 1.0), 6.0);
+                        hn = h * exp((log((double)A.n_ngb) - log((double)n0)) / sl);
                     }
                     hn = fmin(fmax(hn, 0.5 * h), 2.0 * h);
                     if (!(hn > lb && hn < hb)) {
@@ -368,9 +372,10 @@ struct BootArgs {
 __global__ void __launch_bounds__(kWalkWarps * 32) k_boot_h(BootArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<double>));
-    HTile<double> &tile = *reinterpret_cast<HTile<double> *>(wm.tile);
-    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+    using E = V4<double>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    E *tile = reinterpret_cast<E *>(wm.tile);
+    for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         const Cloud &cl = a.clouds[gi.cloud];
         const int64_t ncl = cl.end - cl.begin;
@@ -381,20 +386,20 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_boot_h(BootArgs A) {
         double Rg = 2.0 * (double)fmaxf(gb.hw.x, fmaxf(gb.hw.y, gb.hw.z)) + (double)gi.s10;
         for (int it = 0; it < 64; ++it) {
             int cnt = 0;
-            float3 sh[27];
-            const int nim = group_images(gb, (float)Rg, a.box, a.periodic, sh);
-            for (int im = 0; im < nim; ++im) {
-                const float3 s = sh[im];
-                auto stage = [&](int slot, int j) {
-                    tile.x[slot] = a.pos[j] + (double)s.x;
-                    tile.y[slot] = a.pos[a.n + j] + (double)s.y;
-                    tile.z[slot] = a.pos[2 * a.n + j] + (double)s.z;
+            const Images ims = group_images(gb, (float)Rg, a.box, a.periodic);
+            for (int im = 0; im < 27; ++im) {
+                float3 s;
+                if (!image_shift(ims, im, a.box, s)) continue;
+                auto load = [&](int j) { return src_pos<double>(a, gi, j, s, 0.0); };
+                auto interact = [&](const E *t, int ne) {
+                    for (int e = 0; e < ne; ++e) {
+                        const E q = t[e];
+                        cnt += exact_dist(q.x - tx, q.y - ty, q.z - tz) <= Rg;
+                    }
                 };
-                auto interact = [&](int ne) {
-                    for (int e = 0; e < ne; ++e)
-                        cnt += exact_dist(tile.x[e] - tx, tile.y[e] - ty, tile.z[e] - tz) <= Rg;
+                auto flush = [&](int nl) {
+                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
                 };
-                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
                 collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
             }
             if (__all_sync(kFull, !gi.active || cnt >= need)) break;
@@ -417,32 +422,32 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_boot_h(BootArgs A) {
             int c[16];
 #pragma unroll
             for (int m = 0; m < 16; ++m) c[m] = 0;
-            float3 sh[27];
-            const int nim = group_images(gb, (float)Rg, a.box, a.periodic, sh);
-            for (int im = 0; im < nim; ++im) {
-                const float3 s = sh[im];
-                auto stage = [&](int slot, int j) {
-                    tile.x[slot] = a.pos[j] + (double)s.x;
-                    tile.y[slot] = a.pos[a.n + j] + (double)s.y;
-                    tile.z[slot] = a.pos[2 * a.n + j] + (double)s.z;
-                };
-                auto interact = [&](int ne) {
+            const Images ims = group_images(gb, (float)Rg, a.box, a.periodic);
+            for (int im = 0; im < 27; ++im) {
+                float3 s;
+                if (!image_shift(ims, im, a.box, s)) continue;
+                auto load = [&](int j) { return src_pos<double>(a, gi, j, s, 0.0); };
+                auto interact = [&](const E *tl, int ne) {
                     if (lo == hi) return;
                     for (int e = 0; e < ne; ++e) {
-                        const double d = exact_dist(tile.x[e] - tx, tile.y[e] - ty, tile.z[e] - tz);
+                        const E q = tl[e];
+                        const double d = exact_dist(q.x - tx, q.y - ty, q.z - tz);
 #pragma unroll
                         for (int m = 0; m < 16; ++m) c[m] += d <= tv[m];
                     }
                 };
-                auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+                auto flush = [&](int nl) {
+                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                };
                 collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
             }
             if (lo != hi) {
                 int m = 0;
                 while (m < 16 && c[m] < need) ++m;
-                if (m == 16) lo = t[15] + 1;
-                else {
-                    unsigned long long nlo = m > 0 ? t[m - 1] + 1 : lo;
+                if (m == 16) {
+                    lo = t[15] + 1;
+                } else {
+                    const unsigned long long nlo = m > 0 ? t[m - 1] + 1 : lo;
                     hi = t[m];
                     lo = nlo;
                 }
@@ -468,21 +473,22 @@ struct DArgs {
     int keep_rho;
 };
 
-template <typename R, bool DC>
-struct DTile {
-    R x[32], y[32], z[32], h[32], m[32];
-    R vx[DC ? 32 : 1], vy[DC ? 32 : 1], vz[DC ? 32 : 1];
+// tile entry: p = {x, y, z, h}, q = {m, vx, vy, vz}
+template <typename R>
+struct DE {
+    V4<R> p, q;
 };
 
 template <typename R, bool DC>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(DTile<R, DC>));
-    DTile<R, DC> &tile = *reinterpret_cast<DTile<R, DC> *>(wm.tile);
+    using E = DE<R>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     unsigned long long pairs = 0;
-    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+    for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
         R tx, ty, tz, th, tvx = 0, tvy = 0, tvz = 0;
@@ -493,71 +499,58 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
         } else {
             tx = (R)gi.prel.x; ty = (R)gi.prel.y; tz = (R)gi.prel.z;
             th = (R)A.pk_hme[gi.i].x;
-            if (DC) { float4 v = A.pk_vel[gi.i]; tvx = (R)v.x; tvy = (R)v.y; tvz = (R)v.z; }
+            if (DC) { const float4 v = A.pk_vel[gi.i]; tvx = (R)v.x; tvy = (R)v.y; tvz = (R)v.z; }
         }
         const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
         R rho = 0, sdiv = 0, cx = 0, cy = 0, cz = 0;
-        float3 sh[27];
-        const int nim = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic, sh);
-        for (int im = 0; im < nim; ++im) {
-            const float3 s = sh[im];
-            auto stage = [&](int slot, int j) {
+        const Images ims = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic);
+        for (int im = 0; im < 27; ++im) {
+            float3 s;
+            if (!image_shift(ims, im, a.box, s)) continue;
+            auto load = [&](int j) {
+                E en;
                 if (sizeof(R) == 8) {
-                    tile.x[slot] = (R)(a.pos[j] + (double)s.x);
-                    tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
-                    tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
-                    tile.h[slot] = (R)A.h[j];
-                    tile.m[slot] = (R)A.m[j];
-                    if (DC) {
-                        tile.vx[slot] = (R)A.vel[j];
-                        tile.vy[slot] = (R)A.vel[a.n + j];
-                        tile.vz[slot] = (R)A.vel[2 * a.n + j];
-                    }
+                    en.p = src_pos<R>(a, gi, j, s, (R)A.h[j]);
+                    en.q.x = (R)A.m[j];
+                    if (DC) { en.q.y = (R)A.vel[j]; en.q.z = (R)A.vel[a.n + j]; en.q.w = (R)A.vel[2 * a.n + j]; }
                 } else {
-                    float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
-                    tile.x[slot] = (R)(p.x + s.x);
-                    tile.y[slot] = (R)(p.y + s.y);
-                    tile.z[slot] = (R)(p.z + s.z);
-                    float4 hm = A.pk_hme[j];
-                    tile.h[slot] = (R)hm.x;
-                    tile.m[slot] = (R)hm.y;
-                    if (DC) {
-                        float4 v = A.pk_vel[j];
-                        tile.vx[slot] = (R)v.x;
-                        tile.vy[slot] = (R)v.y;
-                        tile.vz[slot] = (R)v.z;
-                    }
+                    const float4 hm = A.pk_hme[j];
+                    en.p = src_pos<R>(a, gi, j, s, (R)hm.x);
+                    en.q.x = (R)hm.y;
+                    if (DC) { const float4 v = A.pk_vel[j]; en.q.y = (R)v.x; en.q.z = (R)v.y; en.q.w = (R)v.z; }
                 }
+                return en;
             };
-            auto interact = [&](int ne) {
+            auto interact = [&](const E *t, int ne) {
                 if (!gi.active) return;
                 pairs += ne;
                 for (int e = 0; e < ne; ++e) {
+                    const E en = t[e];
                     if (sizeof(R) == 8) {
                         // reference order: dx = x_i - x_j, q = |r| / hbar
-                        const double dx = __dsub_rn((double)tx, (double)tile.x[e]);
-                        const double dy = __dsub_rn((double)ty, (double)tile.y[e]);
-                        const double dz = __dsub_rn((double)tz, (double)tile.z[e]);
+                        const double dx = __dsub_rn((double)tx, (double)en.p.x);
+                        const double dy = __dsub_rn((double)ty, (double)en.p.y);
+                        const double dz = __dsub_rn((double)tz, (double)en.p.z);
                         const double rr = exact_dist(dx, dy, dz);
-                        const double hij = __dmul_rn(0.5, __dadd_rn((double)th, (double)tile.h[e]));
+                        const double hij = __dmul_rn(0.5, __dadd_rn((double)th, (double)en.p.w));
                         const double q = __ddiv_rn(rr, hij);
                         if (q <= 2.0) {
                             const double ih = 1.0 / hij;
                             const double ih3 = ih * ih * ih;
                             double W;
                             if (q <= 1.0) W = kSig * ih3 * (1.0 - 1.5 * q * q + 0.75 * q * q * q);
-                            else { const double t = 2.0 - q; W = kSig * ih3 * 0.25 * t * t * t; }
-                            rho += (R)((double)tile.m[e] * W);
+                            else { const double tq = 2.0 - q; W = kSig * ih3 * 0.25 * tq * tq * tq; }
+                            const double mj = (double)en.q.x;
+                            rho += (R)(mj * W);
                             if (DC) {
                                 double nW;
                                 const double ih5 = ih3 * ih * ih;
                                 if (q <= 1.0) nW = kSig * ih5 * (-3.0 + 2.25 * q);
-                                else { const double t = 2.0 - q; nW = -0.75 * kSig * ih5 * t * t / (q + 1e-20); }
+                                else { const double tq = 2.0 - q; nW = -0.75 * kSig * ih5 * tq * tq / (q + 1e-20); }
                                 const double gx = nW * dx, gy = nW * dy, gz = nW * dz;
-                                const double vx = (double)tvx - (double)tile.vx[e];
-                                const double vy = (double)tvy - (double)tile.vy[e];
-                                const double vz = (double)tvz - (double)tile.vz[e];
-                                const double mj = (double)tile.m[e];
+                                const double vx = (double)tvx - (double)en.q.y;
+                                const double vy = (double)tvy - (double)en.q.z;
+                                const double vz = (double)tvz - (double)en.q.w;
                                 sdiv += (R)(-mj * (vx * gx + vy * gy + vz * gz));
                                 cx += (R)(mj * (vy * gz - vz * gy));
                                 cy += (R)(mj * (vz * gx - vx * gz));
@@ -565,28 +558,28 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                             }
                         }
                     } else {
-                        const float dx = (float)tx - (float)tile.x[e];
-                        const float dy = (float)ty - (float)tile.y[e];
-                        const float dz = (float)tz - (float)tile.z[e];
+                        const float dx = (float)tx - (float)en.p.x;
+                        const float dy = (float)ty - (float)en.p.y;
+                        const float dz = (float)tz - (float)en.p.z;
                         const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float hs = (float)th + (float)tile.h[e];  // = 2 hbar
+                        const float hs = (float)th + (float)en.p.w;  // = 2 hbar
                         if (d2 <= hs * hs) {
                             const float ih = __fdividef(2.0f, hs);
                             const float q = sqrtf(d2) * ih;
                             const float ih3 = ih * ih * ih;
                             float W;
                             if (q <= 1.0f) W = kSigF * ih3 * fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
-                            else { const float t = 2.0f - q; W = kSigF * ih3 * 0.25f * t * t * t; }
-                            rho = fmaf((float)tile.m[e], W, (float)rho);
+                            else { const float tq = 2.0f - q; W = kSigF * ih3 * 0.25f * tq * tq * tq; }
+                            rho = fmaf((float)en.q.x, W, (float)rho);
                             if (DC) {
                                 float nW;
                                 const float ih5 = ih3 * ih * ih;
                                 if (q <= 1.0f) nW = kSigF * ih5 * fmaf(2.25f, q, -3.0f);
-                                else { const float t = 2.0f - q; nW = -0.75f * kSigF * ih5 * t * t * __fdividef(1.0f, q + 1e-20f); }
-                                const float mj = (float)tile.m[e] * nW;
-                                const float vx = (float)tvx - (float)tile.vx[e];
-                                const float vy = (float)tvy - (float)tile.vy[e];
-                                const float vz = (float)tvz - (float)tile.vz[e];
+                                else { const float tq = 2.0f - q; nW = -0.75f * kSigF * ih5 * tq * tq * __fdividef(1.0f, q + 1e-20f); }
+                                const float mj = (float)en.q.x * nW;
+                                const float vx = (float)tvx - (float)en.q.y;
+                                const float vy = (float)tvy - (float)en.q.z;
+                                const float vz = (float)tvz - (float)en.q.w;
                                 sdiv -= mj * fmaf(vx, dx, fmaf(vy, dy, vz * dz));
                                 cx += mj * (vy * dz - vz * dy);
                                 cy += mj * (vz * dx - vx * dz);
@@ -596,7 +589,9 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                     }
                 }
             };
-            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            auto flush = [&](int nl) {
+                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+            };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
         if (gi.active) {
@@ -622,8 +617,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                 const double cv = sqrt((double)cx * (double)cx + (double)cy * (double)cy + (double)cz * (double)cz) * inv;
                 A.divV[i] = dv;
                 A.curlV[i] = cv;
-                const double hh = A.h[i];
-                f = dv / (dv + cv + 0.0001 * c / hh);
+                f = dv / (dv + cv + 0.0001 * c / A.h[i]);
                 A.bal[i] = f;
             }
             const double pr = r > 0.0 ? P / (r * r) : 0.0;
@@ -644,21 +638,23 @@ struct YArgs {
     double alpha, beta, eta;
 };
 
+// tile entry: p = {x, y, z, h}, v = {vx, vy, vz, m}, t = {rho, P/rho^2, c, f}
 template <typename R>
-struct YTile {
-    R x[32], y[32], z[32], vx[32], vy[32], vz[32], h[32], m[32], rho[32], pr[32], c[32], f[32];
+struct YE {
+    V4<R> p, v, t;
 };
 
 template <typename R, int VISC, bool ACC, bool DU>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(YTile<R>));
-    YTile<R> &tile = *reinterpret_cast<YTile<R> *>(wm.tile);
+    using E = YE<R>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     unsigned long long pairs = 0;
     const R alpha = (R)A.alpha, beta = (R)A.beta, eta2 = (R)(A.eta * A.eta);
-    for (int g = next_group(a.work); g < a.ngroups; g = next_group(a.work)) {
+    for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
         const int i = gi.i;
@@ -671,67 +667,61 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
             tc = (R)A.c[i]; tf = (R)A.bal[i];
         } else {
             tx = (R)gi.prel.x; ty = (R)gi.prel.y; tz = (R)gi.prel.z;
-            float4 v = A.pk_vel[i];
+            const float4 v = A.pk_vel[i];
             tvx = (R)v.x; tvy = (R)v.y; tvz = (R)v.z;
             th = (R)A.pk_hme[i].x;
-            float4 t = A.pk_thm[i];
+            const float4 t = A.pk_thm[i];
             trho = (R)t.x; tpr = (R)t.y; tc = (R)t.z; tf = (R)t.w;
         }
         const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
         R ax = 0, ay = 0, az = 0, du = 0;
-        float3 sh[27];
-        const int nim = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic, sh);
-        for (int im = 0; im < nim; ++im) {
-            const float3 s = sh[im];
-            auto stage = [&](int slot, int j) {
+        const Images ims = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic);
+        for (int im = 0; im < 27; ++im) {
+            float3 s;
+            if (!image_shift(ims, im, a.box, s)) continue;
+            auto load = [&](int j) {
+                E en;
                 if (sizeof(R) == 8) {
-                    tile.x[slot] = (R)(a.pos[j] + (double)s.x);
-                    tile.y[slot] = (R)(a.pos[a.n + j] + (double)s.y);
-                    tile.z[slot] = (R)(a.pos[2 * a.n + j] + (double)s.z);
-                    tile.vx[slot] = (R)A.vel[j];
-                    tile.vy[slot] = (R)A.vel[a.n + j];
-                    tile.vz[slot] = (R)A.vel[2 * a.n + j];
-                    tile.h[slot] = (R)A.h[j];
-                    tile.m[slot] = (R)A.m[j];
+                    en.p = src_pos<R>(a, gi, j, s, (R)A.h[j]);
+                    en.v.x = (R)A.vel[j]; en.v.y = (R)A.vel[a.n + j]; en.v.z = (R)A.vel[2 * a.n + j];
+                    en.v.w = (R)A.m[j];
                     const double rj = A.rho[j];
-                    tile.rho[slot] = (R)rj;
-                    tile.pr[slot] = (R)(A.P[j] / (rj * rj));
-                    tile.c[slot] = (R)A.c[j];
-                    tile.f[slot] = (R)A.bal[j];
+                    en.t.x = (R)rj;
+                    en.t.y = (R)(A.P[j] / (rj * rj));
+                    en.t.z = (R)A.c[j];
+                    en.t.w = (R)A.bal[j];
                 } else {
-                    float3 p = rel_to(a.pk_pos[j], gi.ref, gi.s10);
-                    tile.x[slot] = (R)(p.x + s.x);
-                    tile.y[slot] = (R)(p.y + s.y);
-                    tile.z[slot] = (R)(p.z + s.z);
-                    float4 v = A.pk_vel[j];
-                    tile.vx[slot] = (R)v.x; tile.vy[slot] = (R)v.y; tile.vz[slot] = (R)v.z;
-                    float4 hm = A.pk_hme[j];
-                    tile.h[slot] = (R)hm.x; tile.m[slot] = (R)hm.y;
-                    float4 t = A.pk_thm[j];
-                    tile.rho[slot] = (R)t.x; tile.pr[slot] = (R)t.y; tile.c[slot] = (R)t.z; tile.f[slot] = (R)t.w;
+                    const float4 hm = A.pk_hme[j];
+                    en.p = src_pos<R>(a, gi, j, s, (R)hm.x);
+                    const float4 v = A.pk_vel[j];
+                    en.v.x = (R)v.x; en.v.y = (R)v.y; en.v.z = (R)v.z; en.v.w = (R)hm.y;
+                    const float4 t = A.pk_thm[j];
+                    en.t.x = (R)t.x; en.t.y = (R)t.y; en.t.z = (R)t.z; en.t.w = (R)t.w;
                 }
+                return en;
             };
-            auto interact = [&](int ne) {
+            auto interact = [&](const E *tl, int ne) {
                 if (!gi.active) return;
                 pairs += ne;
                 for (int e = 0; e < ne; ++e) {
+                    const E en = tl[e];
                     R dx, dy, dz, rr, hij, q;
                     bool in;
                     if (sizeof(R) == 8) {
-                        const double ddx = __dsub_rn((double)tx, (double)tile.x[e]);
-                        const double ddy = __dsub_rn((double)ty, (double)tile.y[e]);
-                        const double ddz = __dsub_rn((double)tz, (double)tile.z[e]);
+                        const double ddx = __dsub_rn((double)tx, (double)en.p.x);
+                        const double ddy = __dsub_rn((double)ty, (double)en.p.y);
+                        const double ddz = __dsub_rn((double)tz, (double)en.p.z);
                         const double drr = exact_dist(ddx, ddy, ddz);
-                        const double dh = __dmul_rn(0.5, __dadd_rn((double)th, (double)tile.h[e]));
+                        const double dh = __dmul_rn(0.5, __dadd_rn((double)th, (double)en.p.w));
                         const double dq = __ddiv_rn(drr, dh);
                         in = dq <= 2.0;
                         dx = (R)ddx; dy = (R)ddy; dz = (R)ddz; rr = (R)drr; hij = (R)dh; q = (R)dq;
                     } else {
-                        dx = tx - tile.x[e];
-                        dy = ty - tile.y[e];
-                        dz = tz - tile.z[e];
+                        dx = tx - en.p.x;
+                        dy = ty - en.p.y;
+                        dz = tz - en.p.z;
                         const R d2 = dx * dx + dy * dy + dz * dz;
-                        const R hs = th + tile.h[e];
+                        const R hs = th + en.p.w;
                         in = d2 <= hs * hs;
                         rr = (R)sqrtf((float)d2);
                         hij = (R)0.5 * hs;
@@ -742,25 +732,25 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
                     const R ih5 = ih * ih * ih * ih * ih;
                     R nW;
                     if (q <= (R)1) nW = (R)kSig * ih5 * ((R)-3 + (R)2.25 * q);
-                    else { const R t = (R)2 - q; nW = fdiv((R)(-0.75 * kSig) * ih5 * t * t, q + (R)1e-20); }
+                    else { const R tq = (R)2 - q; nW = fdiv((R)(-0.75 * kSig) * ih5 * tq * tq, q + (R)1e-20); }
                     const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
-                    const R vx = tvx - tile.vx[e], vy = tvy - tile.vy[e], vz = tvz - tile.vz[e];
+                    const R vx = tvx - en.v.x, vy = tvy - en.v.y, vz = tvz - en.v.z;
                     const R vr = vx * dx + vy * dy + vz * dz;
-                    const R rhoij = (R)0.5 * (trho + tile.rho[e]);
+                    const R rhoij = (R)0.5 * (trho + en.t.x);
                     R PI = 0;
                     if (VISC == SPH3_VISC_MG83) {
-                        const R cij = (R)0.5 * (tc + tile.c[e]);
+                        const R cij = (R)0.5 * (tc + en.t.z);
                         const R mu = fdiv(hij * vr, rr * rr + hij * hij * eta2);
                         if (vr <= (R)0) PI = fdiv(-alpha * cij * mu + beta * mu * mu, rhoij);
                     } else {
                         const R w = fdiv(vr, rr + (R)1e-5);
-                        const R vsig = tc + tile.c[e] - (R)3 * w;
+                        const R vsig = tc + en.t.z - (R)3 * w;
                         if (vr <= (R)0) PI = fdiv((R)-0.5 * alpha * vsig * w, rhoij);
-                        if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + tile.f[e]) * PI;
+                        if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + en.t.w) * PI;
                     }
-                    const R mj = tile.m[e];
+                    const R mj = en.v.w;
                     if (ACC) {
-                        const R pt = mj * (tpr + tile.pr[e] + PI);
+                        const R pt = mj * (tpr + en.t.y + PI);
                         ax -= pt * gx;
                         ay -= pt * gy;
                         az -= pt * gz;
@@ -768,7 +758,9 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
                     if (DU) du += mj * (tpr + (R)0.5 * PI) * (vx * gx + vy * gy + vz * gz);
                 }
             };
-            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            auto flush = [&](int nl) {
+                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+            };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
         if (gi.active) {
@@ -786,7 +778,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
 
 // ============================================================ neighbours
 // Exact FP64 neighbour sets {j : q_ij <= 2} of selected particles; pass 0
-// counts, pass 1 writes caller indices at the given offsets.
+// counts, pass 1 writes caller indices at the given offsets.  One warp per
+// row, each lane testing its own staged candidate.
 struct NArgs {
     WalkArgs w;
     const double *h;
@@ -803,7 +796,9 @@ struct NArgs {
 __global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(HTile<double>));
+    using E = V4<double>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -825,12 +820,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
         GroupBox gb = group_box(prel, lane == 0, ref, cl.s10);
         const double tx = a.pos[i], ty = a.pos[a.n + i], tz = a.pos[2 * a.n + i];
         const double th = A.h[i];
-        float3 sh[27];
-        const int nim = group_images(gb, (float)th + a.box_h[cl.root].w, a.box, a.periodic, sh);
         int found = 0;
-        for (int im = 0; im < nim; ++im) {
-            const float3 s = sh[im];
-            auto stage = [&](int slot, int j) {
+        const Images ims = group_images(gb, (float)th + a.box_h[cl.root].w, a.box, a.periodic);
+        for (int im = 0; im < 27; ++im) {
+            float3 s;
+            if (!image_shift(ims, im, a.box, s)) continue;
+            auto load = [&](int j) {
                 const double dx = __dsub_rn(tx, a.pos[j] + (double)s.x);
                 const double dy = __dsub_rn(ty, a.pos[a.n + j] + (double)s.y);
                 const double dz = __dsub_rn(tz, a.pos[2 * a.n + j] + (double)s.z);
@@ -845,10 +840,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
                         else set_status(a.status, SPH3_STATUS_LIST_OVERFLOW);
                     }
                 }
-                (void)slot;
+                return E{};
             };
-            auto interact = [&](int ne) { (void)ne; };
-            auto flush = [&](int nl) { flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, stage, interact); };
+            auto interact = [&](const E *t, int ne) {
+                (void)t;
+                (void)ne;
+            };
+            auto flush = [&](int nl) {
+                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+            };
             collect_leaves(a, wm, cl.root, gb, (float)th, true, s, flush);
         }
         found = warp_sum(found);
@@ -860,7 +860,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
 static WalkArgs walk_args(State &S, const Params &P, int slot) {
     WalkArgs a;
     a.groups = S.groups;
-    a.ngroups = S.ngroups;
+    a.ngroups_dev = S.ngroups_dev;
     a.group_cloud = S.group_cloud;
     a.clouds = S.clouds;
     a.ncloud = S.ncloud;
@@ -873,6 +873,7 @@ static WalkArgs walk_args(State &S, const Params &P, int slot) {
     a.n = S.n;
     a.stack_cap = P.stack_cap;
     a.max_depth = S.max_level + 1;
+    a.node_cap = S.tree.cap;
     a.periodic = P.periodic;
     for (int d = 0; d < 3; ++d) a.box[d] = P.box[d];
     a.work = S.work + slot;
@@ -881,8 +882,10 @@ static WalkArgs walk_args(State &S, const Params &P, int slot) {
     return a;
 }
 
-static size_t walk_smem(const Params &P, size_t tile_bytes) {
-    return warp_mem_bytes(P.stack_cap, tile_bytes) * kWalkWarps;
+// dynamic shared memory of a walk block whose tile entries are E (double buffered)
+template <typename E>
+static size_t walk_smem(const Params &P) {
+    return warp_mem_bytes(P.stack_cap, sizeof(E) * 64) * kWalkWarps;
 }
 
 static void allow_smem(const void *kern) {
@@ -901,17 +904,17 @@ static void run_walk(void (*kern)(Args), const Args &args, size_t smem, State &S
 }
 
 void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
-    if (S.ngroups == 0) return;
+    if (S.n == 0) return;
     BootArgs A;
     A.w = walk_args(S, P, 0);
     A.h = S.h;
     A.pk_hme = S.pk_hme;
     A.k = P.n_boot;
-    run_walk(k_boot_h, A, walk_smem(P, sizeof(HTile<double>)), S, st, 0);
+    run_walk(k_boot_h, A, walk_smem<V4<double>>(P), S, st, 0);
 }
 
 void launch_h_search(State &S, const Params &P, cudaStream_t st) {
-    if (S.ngroups == 0) return;
+    if (S.n == 0) return;
     HArgs A;
     A.w = walk_args(S, P, 1);
     A.h = S.h;
@@ -922,19 +925,19 @@ void launch_h_search(State &S, const Params &P, cudaStream_t st) {
     A.max_iter = P.h_max_iter;
     if (P.precision == SPH3_PREC_FP64) {
         if (P.h_mode == SPH3_H_REFSTEP)
-            run_walk(k_h_search<double, SPH3_H_REFSTEP>, A, walk_smem(P, sizeof(HTile<double>)), S, st, 1);
+            run_walk(k_h_search<double, SPH3_H_REFSTEP>, A, walk_smem<V4<double>>(P), S, st, 1);
         else
-            run_walk(k_h_search<double, SPH3_H_NEWTON>, A, walk_smem(P, sizeof(HTile<double>)), S, st, 1);
+            run_walk(k_h_search<double, SPH3_H_NEWTON>, A, walk_smem<V4<double>>(P), S, st, 1);
     } else {
         if (P.h_mode == SPH3_H_REFSTEP)
-            run_walk(k_h_search<float, SPH3_H_REFSTEP>, A, walk_smem(P, sizeof(HTile<float>)), S, st, 1);
+            run_walk(k_h_search<float, SPH3_H_REFSTEP>, A, walk_smem<V4<float>>(P), S, st, 1);
         else
-            run_walk(k_h_search<float, SPH3_H_NEWTON>, A, walk_smem(P, sizeof(HTile<float>)), S, st, 1);
+            run_walk(k_h_search<float, SPH3_H_NEWTON>, A, walk_smem<V4<float>>(P), S, st, 1);
     }
 }
 
 void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bool keep_rho) {
-    if (S.ngroups == 0) return;
+    if (S.n == 0) return;
     DArgs A;
     A.keep_rho = keep_rho ? 1 : 0;
     A.w = walk_args(S, P, 2);
@@ -944,24 +947,24 @@ void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bo
     A.pk_thm = S.pk_thm;
     A.gamma = P.gamma;
     if (P.precision == SPH3_PREC_FP64) {
-        if (divcurl) run_walk(k_density<double, true>, A, walk_smem(P, sizeof(DTile<double, true>)), S, st, 2);
-        else run_walk(k_density<double, false>, A, walk_smem(P, sizeof(DTile<double, false>)), S, st, 2);
+        if (divcurl) run_walk(k_density<double, true>, A, walk_smem<DE<double>>(P), S, st, 2);
+        else run_walk(k_density<double, false>, A, walk_smem<DE<double>>(P), S, st, 2);
     } else {
-        if (divcurl) run_walk(k_density<float, true>, A, walk_smem(P, sizeof(DTile<float, true>)), S, st, 2);
-        else run_walk(k_density<float, false>, A, walk_smem(P, sizeof(DTile<float, false>)), S, st, 2);
+        if (divcurl) run_walk(k_density<float, true>, A, walk_smem<DE<float>>(P), S, st, 2);
+        else run_walk(k_density<float, false>, A, walk_smem<DE<float>>(P), S, st, 2);
     }
 }
 
 template <typename R, int V>
 static void hydro_dispatch(const YArgs &A, bool acc, bool du, const Params &P, State &S, cudaStream_t st) {
-    const size_t sm = walk_smem(P, sizeof(YTile<R>));
+    const size_t sm = walk_smem<YE<R>>(P);
     if (acc && du) run_walk(k_hydro<R, V, true, true>, A, sm, S, st, 3);
     else if (acc) run_walk(k_hydro<R, V, true, false>, A, sm, S, st, 3);
     else run_walk(k_hydro<R, V, false, true>, A, sm, S, st, 3);
 }
 
 void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cudaStream_t st) {
-    if (S.ngroups == 0 || (!want_acc && !want_dudt)) return;
+    if (S.n == 0 || (!want_acc && !want_dudt)) return;
     YArgs A;
     A.w = walk_args(S, P, 3);
     A.pk_hme = S.pk_hme; A.pk_vel = S.pk_vel; A.pk_thm = S.pk_thm;
@@ -1030,24 +1033,24 @@ int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev,
     A.out = idx_dev;
     A.cap = cap;
     A.cursor = nullptr;
-    const size_t sm = walk_smem(P, sizeof(HTile<double>));
+    const size_t sm = walk_smem<V4<double>>(P);
     allow_smem((const void *)k_neighbours);
     int blocks = (int)std::min<int64_t>((nrows + kWalkWarps - 1) / kWalkWarps, (int64_t)S.num_sms * 8);
     // pass 0: counts into offsets[0..nrows)
     A.pass = 0;
     k_neighbours<<<blocks, kWalkWarps * 32, sm, st>>>(A);
     // exclusive scan on the host (few rows)
-    std::vector<int64_t> h(nrows + 1);
-    cudaMemcpyAsync(h.data(), offsets_dev, sizeof(int64_t) * nrows, cudaMemcpyDeviceToHost, st);
+    std::vector<int64_t> hv(nrows + 1);
+    cudaMemcpyAsync(hv.data(), offsets_dev, sizeof(int64_t) * nrows, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     int64_t run = 0;
     for (int64_t r = 0; r < nrows; ++r) {
-        int64_t v = h[r];
-        h[r] = run;
+        const int64_t v = hv[r];
+        hv[r] = run;
         run += v;
     }
-    h[nrows] = run;
-    cudaMemcpyAsync(offsets_dev, h.data(), sizeof(int64_t) * (nrows + 1), cudaMemcpyHostToDevice, st);
+    hv[nrows] = run;
+    cudaMemcpyAsync(offsets_dev, hv.data(), sizeof(int64_t) * (nrows + 1), cudaMemcpyHostToDevice, st);
     int *cursor = nullptr;
     cudaMallocAsync(&cursor, sizeof(int) * nrows, st);
     cudaMemsetAsync(cursor, 0, sizeof(int) * nrows, st);
