@@ -35,6 +35,9 @@ constexpr int kWarp = 32;
 constexpr int kGroup = 32;        // target particles per walk group (one warp)
 constexpr int kCellBits = 10;     // level of the FP32 cell-relative frame
 constexpr int kWalkWarps = 4;     // warps per walk block
+// resident walk blocks per SM the register budget must allow; capping the
+// registers (e.g. 8 -> 64 regs) spilled and measured slower on B200
+constexpr int kWalkMinBlocks = 1;
 constexpr int kLeafQ = 96;        // queued leaves per warp before a flush
 constexpr int kNodeQ = 64;        // queued multipole nodes per warp (gravity)
 constexpr unsigned kFull = 0xffffffffu;

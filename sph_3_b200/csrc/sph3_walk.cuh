@@ -191,6 +191,70 @@ __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq
     }
 }
 
+// As flush_leaves, but load(j, keep) also says whether candidate j can reach
+// the group at all (tested once per candidate by the lane that loads it);
+// kept candidates are compacted so that every interact() call but the last
+// sees a full tile of 32.  The tile holds 64 entries: up to 31 left over
+// plus one freshly loaded chunk.
+template <class E, class Load, class Interact>
+__device__ __forceinline__ void flush_leaves_compact(const int2 *range, const int *leafq, int nleaf,
+                                                     int *lfirst, int *lpre, E *tile, Load &load,
+                                                     Interact &interact) {
+    const int lane = lane_id();
+    int fill = 0;
+    for (int base = 0; base < nleaf; base += 32) {
+        int cnt = 0, fst = 0;
+        if (base + lane < nleaf) {
+            int2 r = range[leafq[base + lane]];
+            fst = r.x;
+            cnt = r.y;
+        }
+        const int incl = warp_incl_scan(cnt);
+        const int tot = __shfl_sync(kFull, incl, 31);
+        __syncwarp();
+        lfirst[lane] = fst;
+        lpre[lane] = incl - cnt;
+        __syncwarp();
+        const int nl = min(32, nleaf - base);
+        auto fetch = [&](int c0, E &out) -> bool {
+            const int t = c0 + lane;
+            if (t >= tot) return false;
+            int lo = 0, hi = nl - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (lpre[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            bool keep = true;
+            out = load(lfirst[lo] + (t - lpre[lo]), keep);
+            return keep;
+        };
+        E cur;
+        bool have = fetch(0, cur);
+        for (int c0 = 0; c0 < tot; c0 += 32) {
+            const unsigned kb = __ballot_sync(kFull, have);
+            if (have) tile[fill + __popc(kb & lanemask_lt())] = cur;
+            fill += __popc(kb);
+            __syncwarp();
+            have = c0 + 32 < tot ? fetch(c0 + 32, cur) : false;
+            if (fill >= 32) {
+                interact(tile, 32);
+                __syncwarp();
+                E rest;
+                const bool mv = lane < fill - 32;
+                if (mv) rest = tile[32 + lane];
+                __syncwarp();
+                if (mv) tile[lane] = rest;
+                fill -= 32;
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+    }
+    if (fill > 0) interact(tile, fill);
+    __syncwarp();
+}
+
 // Periodic images needed by a group whose reach is R.  Per axis a 3-bit
 // mask: bit 0 the identity, bit 1 the shift -L (reach crosses 0), bit 2 the
 // shift +L (reach crosses L).  Image codes 0..26 combine one option per axis

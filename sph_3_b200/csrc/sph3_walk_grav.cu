@@ -107,7 +107,7 @@ __device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R eps
 }
 
 template <typename R, bool QUAD>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_gravity(GArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTile<R>));
     GTile<R> &tile = *reinterpret_cast<GTile<R> *>(wm.tile);

@@ -168,6 +168,19 @@ __device__ __forceinline__ V4<R> src_pos(const WalkArgs &a, const GroupInfo &gi,
     return p;
 }
 
+// group-frame FP32 position of source j shifted by s (for the reach filter)
+__device__ __forceinline__ float3 frame_pos(const WalkArgs &a, const GroupInfo &gi, int j, float3 s) {
+    const float3 q = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+    return make_float3(q.x + s.x, q.y + s.y, q.z + s.z);
+}
+
+// can a source at p with smoothing length hj reach any target of the group
+// (gap to the group box <= reach + hj, with the walk's 4e-5 safety margin)?
+__device__ __forceinline__ bool reaches(const GroupBox &gb, float3 p, float reach) {
+    const float r = reach * (1.0f + 4e-5f);
+    return point_gap2(gb, p) <= r * r;
+}
+
 // ================================================================= h search
 struct HArgs {
     WalkArgs w;
@@ -181,7 +194,7 @@ constexpr int kHK = 16;  // thresholds per pass in the reference-step mode
 constexpr double kNewtonDelta = 0.08;
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = V4<R>;
@@ -251,7 +264,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
             for (int im = 0; im < 27; ++im) {
                 float3 s;
                 if (!image_shift(ims, im, a.box, s)) continue;
-                auto load = [&](int j) { return src_pos<R>(a, gi, j, s, (R)0); };
+                auto load = [&](int j, bool &keep) {
+                    const V4<R> p = src_pos<R>(a, gi, j, s, (R)0);
+                    const float3 f = sizeof(R) == 8 ? frame_pos(a, gi, j, s)
+                                                    : make_float3((float)p.x, (float)p.y, (float)p.z);
+                    keep = reaches(gb, f, reach);
+                    return p;
+                };
                 auto interact = [&](const E *t, int ne) {
                     if (conv) return;
                     pairs += ne;
@@ -273,7 +292,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_h_search(HArgs A) {
                     }
                 };
                 auto flush = [&](int nl) {
-                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
                 };
                 collect_leaves(a, wm, gi.root, gb, reach, false, s, flush);
             }
@@ -369,7 +388,7 @@ struct BootArgs {
     int k;
 };
 
-__global__ void __launch_bounds__(kWalkWarps * 32) k_boot_h(BootArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_boot_h(BootArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = V4<double>;
@@ -480,7 +499,7 @@ struct DE {
 };
 
 template <typename R, bool DC>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = DE<R>;
@@ -507,24 +526,51 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
         for (int im = 0; im < 27; ++im) {
             float3 s;
             if (!image_shift(ims, im, a.box, s)) continue;
-            auto load = [&](int j) {
+            auto load = [&](int j, bool &keep) {
                 E en;
+                float3 f;
                 if (sizeof(R) == 8) {
                     en.p = src_pos<R>(a, gi, j, s, (R)A.h[j]);
                     en.q.x = (R)A.m[j];
                     if (DC) { en.q.y = (R)A.vel[j]; en.q.z = (R)A.vel[a.n + j]; en.q.w = (R)A.vel[2 * a.n + j]; }
+                    f = frame_pos(a, gi, j, s);
                 } else {
                     const float4 hm = A.pk_hme[j];
                     en.p = src_pos<R>(a, gi, j, s, (R)hm.x);
                     en.q.x = (R)hm.y;
                     if (DC) { const float4 v = A.pk_vel[j]; en.q.y = (R)v.x; en.q.z = (R)v.y; en.q.w = (R)v.z; }
+                    f = make_float3((float)en.p.x, (float)en.p.y, (float)en.p.z);
                 }
+                keep = reaches(gb, f, hmax_g + (float)en.p.w);
                 return en;
             };
             auto interact = [&](const E *t, int ne) {
                 if (!gi.active) return;
                 pairs += ne;
+                // pass 1: which staged sources lie inside this target's support
+                unsigned mask = 0;
                 for (int e = 0; e < ne; ++e) {
+                    const V4<R> p = t[e].p;
+                    bool in;
+                    if (sizeof(R) == 8) {
+                        const double dx = __dsub_rn((double)tx, (double)p.x);
+                        const double dy = __dsub_rn((double)ty, (double)p.y);
+                        const double dz = __dsub_rn((double)tz, (double)p.z);
+                        const double hij = __dmul_rn(0.5, __dadd_rn((double)th, (double)p.w));
+                        in = __ddiv_rn(exact_dist(dx, dy, dz), hij) <= 2.0;
+                    } else {
+                        const float dx = (float)tx - (float)p.x;
+                        const float dy = (float)ty - (float)p.y;
+                        const float dz = (float)tz - (float)p.z;
+                        const float hs = (float)th + (float)p.w;
+                        in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= hs * hs;
+                    }
+                    mask |= (unsigned)in << e;
+                }
+                // pass 2: each lane runs the kernel only on its own neighbours
+                while (mask) {
+                    const int e = __ffs(mask) - 1;
+                    mask &= mask - 1;
                     const E en = t[e];
                     if (sizeof(R) == 8) {
                         // reference order: dx = x_i - x_j, q = |r| / hbar
@@ -534,7 +580,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                         const double rr = exact_dist(dx, dy, dz);
                         const double hij = __dmul_rn(0.5, __dadd_rn((double)th, (double)en.p.w));
                         const double q = __ddiv_rn(rr, hij);
-                        if (q <= 2.0) {
+                        {
                             const double ih = 1.0 / hij;
                             const double ih3 = ih * ih * ih;
                             double W;
@@ -563,7 +609,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                         const float dz = (float)tz - (float)en.p.z;
                         const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float hs = (float)th + (float)en.p.w;  // = 2 hbar
-                        if (d2 <= hs * hs) {
+                        {
                             const float ih = __fdividef(2.0f, hs);
                             const float q = sqrtf(d2) * ih;
                             const float ih3 = ih * ih * ih;
@@ -590,7 +636,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_density(DArgs A) {
                 }
             };
             auto flush = [&](int nl) {
-                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
@@ -645,7 +691,7 @@ struct YE {
 };
 
 template <typename R, int VISC, bool ACC, bool DU>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = YE<R>;
@@ -679,9 +725,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
         for (int im = 0; im < 27; ++im) {
             float3 s;
             if (!image_shift(ims, im, a.box, s)) continue;
-            auto load = [&](int j) {
+            auto load = [&](int j, bool &keep) {
                 E en;
+                float3 f;
                 if (sizeof(R) == 8) {
+                    f = frame_pos(a, gi, j, s);
                     en.p = src_pos<R>(a, gi, j, s, (R)A.h[j]);
                     en.v.x = (R)A.vel[j]; en.v.y = (R)A.vel[a.n + j]; en.v.z = (R)A.vel[2 * a.n + j];
                     en.v.w = (R)A.m[j];
@@ -697,13 +745,38 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
                     en.v.x = (R)v.x; en.v.y = (R)v.y; en.v.z = (R)v.z; en.v.w = (R)hm.y;
                     const float4 t = A.pk_thm[j];
                     en.t.x = (R)t.x; en.t.y = (R)t.y; en.t.z = (R)t.z; en.t.w = (R)t.w;
+                    f = make_float3((float)en.p.x, (float)en.p.y, (float)en.p.z);
                 }
+                keep = reaches(gb, f, hmax_g + (float)en.p.w);
                 return en;
             };
             auto interact = [&](const E *tl, int ne) {
                 if (!gi.active) return;
                 pairs += ne;
+                // pass 1: which staged sources lie inside this target's support
+                unsigned mask = 0;
                 for (int e = 0; e < ne; ++e) {
+                    const V4<R> p = tl[e].p;
+                    bool in;
+                    if (sizeof(R) == 8) {
+                        const double ddx = __dsub_rn((double)tx, (double)p.x);
+                        const double ddy = __dsub_rn((double)ty, (double)p.y);
+                        const double ddz = __dsub_rn((double)tz, (double)p.z);
+                        const double dh = __dmul_rn(0.5, __dadd_rn((double)th, (double)p.w));
+                        in = __ddiv_rn(exact_dist(ddx, ddy, ddz), dh) <= 2.0;
+                    } else {
+                        const float fx = (float)tx - (float)p.x;
+                        const float fy = (float)ty - (float)p.y;
+                        const float fz = (float)tz - (float)p.z;
+                        const float hs = (float)th + (float)p.w;
+                        in = fmaf(fx, fx, fmaf(fy, fy, fz * fz)) <= hs * hs;
+                    }
+                    mask |= (unsigned)in << e;
+                }
+                // pass 2: each lane runs the pair terms only on its own neighbours
+                while (mask) {
+                    const int e = __ffs(mask) - 1;
+                    mask &= mask - 1;
                     const E en = tl[e];
                     R dx, dy, dz, rr, hij, q;
                     bool in;
@@ -727,7 +800,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
                         hij = (R)0.5 * hs;
                         q = (R)((float)rr * __fdividef(1.0f, (float)hij));
                     }
-                    if (!in) continue;
+                    (void)in;
                     const R ih = fdiv((R)1, hij);
                     const R ih5 = ih * ih * ih * ih * ih;
                     R nW;
@@ -759,7 +832,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_hydro(YArgs A) {
                 }
             };
             auto flush = [&](int nl) {
-                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
@@ -793,7 +866,7 @@ struct NArgs {
     int pass;
 };
 
-__global__ void __launch_bounds__(kWalkWarps * 32) k_neighbours(NArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_neighbours(NArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = V4<double>;
