@@ -66,6 +66,7 @@ extern "C" {
 #define SPH3_ERR_UNSUPPORTED 5
 #define SPH3_ERR_OUT_OF_MEMORY 6
 #define SPH3_ERR_DEVICE_STATUS 7 /* a device status bit is set, see sph3_status */
+#define SPH3_ERR_TOO_LARGE 8     /* size above the fixed maximum of sph3_morton_sort_noalloc */
 
 /* ----------------------------------------------- device status word bits */
 #define SPH3_STATUS_H_NOT_CONVERGED 0x1u  /* h search hit its iteration cap */
@@ -244,6 +245,24 @@ int sph3_counters(sph3_ctx *ctx, int64_t out[8], int clear);
  * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,
  * [5] density, [6] gravity, [7] hydro, [8] kick+u+energy.  Clears if `clear`. */
 int sph3_phase_times(sph3_ctx *ctx, double out[9], int clear);
+
+/* Morton sort that allocates no device memory -- it has no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: code running inside a
+ * caller-owned pool or arena, or under a host framework that owns the
+ * device allocator, or a loop that cannot afford cudaMalloc's latency and
+ * implicit synchronisation.  They pass device buffers only: pos ((n,3)
+ * row-major FP64, read), order (n int64: caller index of the k-th sorted
+ * particle) and keys (n uint64 Morton keys); either output may be NULL.
+ * The result equals sph3_set_particles + sph3_morton_order for one system
+ * with the same max_level (4..21).
+ * Limit: n <= 65536 (SPH3_ERR_TOO_LARGE above it).  The scratch is a fixed
+ * static device array (about 3 MB) that every GPU loading the library holds
+ * until the process exits; the first call on a device looks up its address,
+ * so make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race.  Stream-ordered on `stream`;
+ * does not synchronise.  Non-finite coordinates quantise to cell 0. */
+int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t max_level, int64_t *order,
+                             uint64_t *keys, void *stream);
 
 #ifdef __cplusplus
 }

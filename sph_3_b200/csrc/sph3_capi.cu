@@ -539,6 +539,7 @@ const char *sph3_error_string(int code) {
         case SPH3_ERR_UNSUPPORTED: return "unsupported combination (e.g. gravity with a periodic box)";
         case SPH3_ERR_OUT_OF_MEMORY: return "out of device memory";
         case SPH3_ERR_DEVICE_STATUS: return "device status bit set";
+        case SPH3_ERR_TOO_LARGE: return "size above the fixed maximum of the no-allocation entry point (65536)";
         default: return "unknown error";
     }
 }
