@@ -76,6 +76,7 @@ extern "C" {
 #define SPH3_STATUS_ZERO_DENSITY 0x10u    /* rho <= 0 where a division by rho follows */
 #define SPH3_STATUS_LIST_OVERFLOW 0x20u   /* neighbour export capacity exceeded */
 #define SPH3_STATUS_SORT 0x40u            /* radix-sort bookkeeping mismatch */
+#define SPH3_STATUS_BOX_TOO_SMALL 0x80u   /* 2h above half a periodic box length: no unique minimum image */
 
 /* ----------------------------------------------------------------- enums */
 #define SPH3_PREC_MIXED 0 /* FP32 cell-relative pair arithmetic, FP64 state/accumulators/sums */

@@ -64,7 +64,7 @@ constexpr size_t kOffCloud = kOffItemBeg + al256(sizeof(int) * 2);
 constexpr size_t kOffStatus = kOffCloud + al256(sizeof(Cloud));
 constexpr size_t kScratchBytes = kOffStatus + al256(sizeof(unsigned));
 
-__device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
+static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;

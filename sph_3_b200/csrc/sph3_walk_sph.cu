@@ -365,6 +365,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HA
             A.h[gi.i] = h;
             A.nngb[gi.i] = ncount;
             A.pk_hme[gi.i].x = (float)h;
+            // minimum-image counting needs the kernel support inside half the box
+            bool big = false;
+            for (int d = 0; d < 3; ++d) big |= a.box[d] > 0.0 && 2.0 * h > 0.5 * a.box[d];
+            if (big) set_status(a.status, SPH3_STATUS_BOX_TOO_SMALL);
         }
         const unsigned fb = __ballot_sync(kFull, gi.active && failed);
         if (fb && lane == 0) set_status(a.status, SPH3_STATUS_H_NOT_CONVERGED);
