@@ -137,13 +137,16 @@ typedef struct sph3_config {
     int32_t h_max_iter;  /* cap on h iterations (SPH3_STATUS_H_NOT_CONVERGED past it) */
     int32_t n_boot;      /* k of the bootstrap h (reference: 50, 0-based sorted index) */
     int32_t leaf_size;   /* octree leaf capacity (1..64) */
-    int32_t stack_cap;   /* walk-stack entries per warp: 256 or 512 */
+    int32_t stack_cap;   /* walk-stack entries per warp (default 2048; >= 7 (max_level + 2) + 32, <= 4096).
+                          * Wide pops need room: once the stack nears its capacity the walk pops one
+                          * node per iteration, which is exact but slow. */
     int32_t max_level;   /* octree levels (3 key bits each), 4..21 */
     int32_t gravity;     /* 0: hydro only */
     int32_t quadrupole;  /* 1: monopole + quadrupole nodes, 0: monopole only */
     int32_t use_graph;   /* 1: sph3_step replays a captured CUDA graph */
     int32_t timing;      /* 1: record per-phase CUDA events (no graph) */
-    int32_t reserved_i[5];
+    int32_t walk_warps;  /* warps per walk block: 1, 2, 4 (default) or 8; each warp walks one group of <= 32 particles */
+    int32_t reserved_i[4];
     double gamma;        /* adiabatic index (5/3) */
     double alpha;        /* artificial viscosity alpha (1) */
     double beta;         /* beta of the MG83 form (2) */
@@ -236,11 +239,14 @@ int sph3_neighbours(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *
  * keys[k] its 64-bit key (either pointer may be NULL).  Host buffers. */
 int sph3_morton_order(sph3_ctx *ctx, int64_t *order, uint64_t *keys);
 
-/* Interaction counters of the last passes: [0] gravity node interactions,
- * [1] gravity particle interactions, [2] SPH candidate pairs of the density
- * pass, [3] of the hydro pass, [4] h-search candidate pairs, [5] h passes,
- * [6] tree nodes, [7] tree leaves.  Clears them if `clear`. */
-int sph3_counters(sph3_ctx *ctx, int64_t out[8], int clear);
+/* Work counters accumulated since the last clear: [0] gravity node
+ * interactions, [1] gravity particle interactions, [2] SPH candidate pairs of
+ * the density pass, [3] of the hydro pass, [4] h-search candidate pairs,
+ * [5] h passes, [6] tree nodes (of the last build), [7] tree leaves,
+ * [8..11] tree nodes visited by the h-search / density / hydro / gravity
+ * walks, [12] the longest single walk (loop iterations), [13..15] reserved.
+ * Clears them if `clear`. */
+int sph3_counters(sph3_ctx *ctx, int64_t out[16], int clear);
 
 /* Per-phase device times in ms accumulated while cfg.timing = 1:
  * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,

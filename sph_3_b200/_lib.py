@@ -56,7 +56,8 @@ class Config(ctypes.Structure):
         ("quadrupole", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
         ("timing", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 5),
+        ("walk_warps", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 4),
         ("gamma", ctypes.c_double),
         ("alpha", ctypes.c_double),
         ("beta", ctypes.c_double),

@@ -45,12 +45,13 @@ class Config:
     h_max_iter: int = 64
     n_boot: int = 50
     leaf_size: int = 16
-    stack_cap: int = 512
+    stack_cap: int = 2048
     max_level: int = 16
     gravity: bool = True
     quadrupole: bool = True
     use_graph: bool = True
     timing: bool = False
+    walk_warps: int = 4            # warps per walk block (1, 2, 4, 8)
     gamma: float = 5.0 / 3.0
     alpha: float = 1.0
     beta: float = 2.0
@@ -66,7 +67,8 @@ class Config:
         c.h_mode = _HMODE[self.h_mode]
         c.visc = _VISC[self.visc]
         c.step_order = _ORDER[self.step_order]
-        for name in ("n_ngb", "n_ngb_tol", "h_max_iter", "n_boot", "leaf_size", "stack_cap", "max_level"):
+        for name in ("n_ngb", "n_ngb_tol", "h_max_iter", "n_boot", "leaf_size", "stack_cap", "max_level",
+                     "walk_warps"):
             setattr(c, name, int(getattr(self, name)))
         for name in ("gravity", "quadrupole", "use_graph", "timing"):
             setattr(c, name, 1 if getattr(self, name) else 0)
@@ -106,6 +108,7 @@ class Context:
         check(self.lib.sph3_ctx_create(ctypes.byref(cfg), int(device), ctypes.byref(self._ptr)),
               "ctx_create")
         self.n = 0
+        self.ncloud = 1
         self._keep = []
 
     # ------------------------------------------------------------ lifetime
@@ -159,6 +162,7 @@ class Context:
         arr = np.ascontiguousarray(counts, dtype=np.int64)
         check(self.lib.sph3_set_clouds(self._ptr, arr.ctypes.data_as(ctypes.c_void_p), int(arr.size)),
               "set_clouds")
+        self.ncloud = int(arr.size)
 
     def set_particles(self, pos, m, vel=None, u=None, h=None, eps=None):
         n = int(pos.shape[0]) if hasattr(pos, "shape") else len(pos)
@@ -227,11 +231,12 @@ class Context:
         return [k for k, b in STATUS_BITS.items() if s & b]
 
     def counters(self, clear=False):
-        out = np.zeros(8, dtype=np.int64)
+        out = np.zeros(16, dtype=np.int64)
         check(self.lib.sph3_counters(self._ptr, out.ctypes.data_as(ctypes.c_void_p), 1 if clear else 0),
               "counters")
         keys = ["grav_node", "grav_part", "density_pairs", "hydro_pairs", "h_pairs", "h_passes",
-                "tree_nodes", "tree_leaves"]
+                "tree_nodes", "tree_leaves", "visits_h", "visits_density", "visits_hydro", "visits_gravity",
+                "walk_max_iter"]
         return dict(zip(keys, out.tolist()))
 
     def phase_times(self, clear=False):

@@ -43,6 +43,7 @@ struct sph3_ctx {
     bool bal_dirty = false;
     bool tree_dirty = true;
     bool h_dirty_tree = false;  // node hmax stale
+    bool order_dirty = false;   // positions changed since the last sort
     // graphs (one per carried-block parity)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt[2] = {0, 0};
@@ -113,6 +114,7 @@ void params_from(const sph3_config &cfg, Params &P) {
     P.max_level = cfg.max_level;
     P.gravity = cfg.gravity;
     P.quadrupole = cfg.quadrupole;
+    P.walk_warps = cfg.walk_warps;
     P.gamma = cfg.gamma;
     P.alpha = cfg.alpha;
     P.beta = cfg.beta;
@@ -136,6 +138,8 @@ int validate(const sph3_config *c) {
     if (c->n_ngb < 1 || c->n_ngb_tol < 0 || c->n_ngb_tol >= c->n_ngb) return SPH3_ERR_INVALID_ARG;
     if (c->h_max_iter < 1 || c->n_boot < 0) return SPH3_ERR_INVALID_ARG;
     if (c->leaf_size < 1 || c->leaf_size > 64) return SPH3_ERR_INVALID_ARG;
+    if (c->walk_warps != 1 && c->walk_warps != 2 && c->walk_warps != 4 && c->walk_warps != 8)
+        return SPH3_ERR_INVALID_ARG;
     if (c->max_level < 4 || c->max_level > 21) return SPH3_ERR_INVALID_ARG;
     if (c->stack_cap < 7 * (c->max_level + 2) + 32 || c->stack_cap > 4096) return SPH3_ERR_INVALID_ARG;
     if (!(c->theta >= 0.0) || !(c->eps > 0.0) || !(c->gamma >= 1.0)) return SPH3_ERR_INVALID_ARG;
@@ -391,7 +395,23 @@ int ensure_inv(sph3_ctx *c, cudaStream_t st) {
     return check_launch();
 }
 
-int sync_packs(sph3_ctx *c, cudaStream_t st) {
+// Brings the FP32 packs, Balsara factors and the tree up to date with the
+// FP64 fields.  A timestep rebuilds all of them itself (after its own sort),
+// so for_step only drops the pending work.
+int sync_packs(sph3_ctx *c, cudaStream_t st, bool for_step = false) {
+    if (for_step) {
+        c->order_dirty = false;
+        c->pack_dirty = 0;
+        c->bal_dirty = false;
+        c->tree_dirty = false;
+        c->h_dirty_tree = false;
+        return SPH3_OK;
+    }
+    if (c->order_dirty) {
+        const int rc = resort_all(c, st);
+        if (rc) return rc;
+        c->order_dirty = false;
+    }
     if (c->pack_dirty) {
         launch_pack(c->S, c->P, c->pack_dirty, st);
         c->pack_dirty = 0;
@@ -514,10 +534,11 @@ void sph3_default_config(sph3_config *cfg) {
     cfg->h_max_iter = 64;
     cfg->n_boot = 50;
     cfg->leaf_size = 16;
-    cfg->stack_cap = 512;
+    cfg->stack_cap = 2048;
     cfg->max_level = 16;
     cfg->gravity = 1;
     cfg->quadrupole = 1;
+    cfg->walk_warps = 4;
     cfg->use_graph = 1;
     cfg->timing = 0;
     cfg->gamma = 5.0 / 3.0;
@@ -572,6 +593,7 @@ int sph3_ctx_create(const sph3_config *cfg, int device, sph3_ctx **out) {
     }
     c->S.num_sms = prop.multiProcessorCount;
     c->S.walk_blocks = prop.multiProcessorCount * 8;
+    c->S.walk_warps = cfg->walk_warps;
     c->S.max_level = cfg->max_level;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
@@ -579,7 +601,7 @@ int sph3_ctx_create(const sph3_config *cfg, int device, sph3_ctx **out) {
     }
     for (auto &e : c->ev) cudaEventCreate(&e);
     if (cudaMalloc(&c->S.status, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&c->S.counters, sizeof(unsigned long long) * 8) != cudaSuccess ||
+        cudaMalloc(&c->S.counters, sizeof(unsigned long long) * kNumCounters) != cudaSuccess ||
         cudaMalloc(&c->S.work, sizeof(int) * 8) != cudaSuccess ||
         cudaMalloc(&c->S.energy_part, sizeof(double) * 8 * 512) != cudaSuccess ||
         cudaMalloc(&c->S.energy, sizeof(double) * 8) != cudaSuccess) {
@@ -587,7 +609,7 @@ int sph3_ctx_create(const sph3_config *cfg, int device, sph3_ctx **out) {
         return SPH3_ERR_OUT_OF_MEMORY;
     }
     cudaMemset(c->S.status, 0, sizeof(unsigned));
-    cudaMemset(c->S.counters, 0, sizeof(unsigned long long) * 8);
+    cudaMemset(c->S.counters, 0, sizeof(unsigned long long) * kNumCounters);
     cudaMemset(c->S.energy, 0, sizeof(double) * 8);
     *out = c;
     return SPH3_OK;
@@ -625,6 +647,7 @@ int sph3_set_config(sph3_ctx *c, const sph3_config *cfg) {
     }
     c->cfg = *cfg;
     params_from(*cfg, c->P);
+    c->S.walk_warps = cfg->walk_warps;
     drop_graphs(c);
     if (relevel && c->have) {
         cudaSetDevice(c->device);
@@ -758,7 +781,7 @@ int sph3_set_field(sph3_ctx *c, int field, const double *src, int on_device, voi
     if (!dst) return SPH3_ERR_INVALID_ARG;
     const int64_t n = c->S.n;
     if (n == 0) return SPH3_OK;
-    drop_graphs(c);
+    // the captured step graphs stay valid: buffers do not move
     CK(cudaMemcpyAsync(c->staging, src, sizeof(double) * n * ncomp,
                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     k_scatter_in<<<blocks_for(c, n), 256, 0, st>>>(c->staging, dst, c->S.orig, n, ncomp);
@@ -766,8 +789,9 @@ int sph3_set_field(sph3_ctx *c, int field, const double *src, int on_device, voi
     if (rc) return rc;
     switch (field) {
         case SPH3_FIELD_POS:
-            rc = resort_all(c, st);
-            if (rc) return rc;
+            // re-sorted lazily: by the next pass that needs the tree, or by
+            // the next step, which sorts anyway
+            c->order_dirty = true;
             break;
         case SPH3_FIELD_VEL: c->pack_dirty |= kPackVel; break;
         case SPH3_FIELD_MASS:
@@ -895,7 +919,7 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
     cudaStream_t st = pick(c, stream);
     State &S = c->S;
     if (S.n == 0) return SPH3_OK;
-    int rc = sync_packs(c, st);
+    int rc = sync_packs(c, st, true);
     if (rc) return rc;
     if (!c->P.gravity) cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st);
     const bool serial = c->P.step_order == SPH3_ORDER_SERIAL;
@@ -913,24 +937,30 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
             continue;
         }
         const int par = c->cur;
-        if (c->graph[par] && c->graph_dt[par] != dt) {
-            cudaGraphExecDestroy(c->graph[par]);
-            c->graph[par] = nullptr;
-        }
-        if (!c->graph[par]) {
+        // capture the graphs of both carried-block parities together, so that
+        // later steps only replay (no capture inside a timed sequence)
+        for (int q = 0; q < 2; ++q) {
+            const int pq = par ^ q;
+            if (c->graph[pq] && c->graph_dt[pq] != dt) {
+                cudaGraphExecDestroy(c->graph[pq]);
+                c->graph[pq] = nullptr;
+            }
+            if (c->graph[pq]) continue;
+            c->cur = pq;
+            point_carried(c);
             cudaGraph_t g;
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             enqueue_step(c, dt, st);
             cudaError_t e = cudaStreamEndCapture(st, &g);
             if (e != cudaSuccess) return SPH3_ERR_CUDA;
-            e = cudaGraphInstantiate(&c->graph[par], g, 0);
+            e = cudaGraphInstantiate(&c->graph[pq], g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return SPH3_ERR_CUDA;
-            c->graph_dt[par] = dt;
-            // capture switched the carried block without running: switch back
-            c->cur = par;
-            point_carried(c);
+            c->graph_dt[pq] = dt;
         }
+        // capture switched the carried block without running: restore it
+        c->cur = par;
+        point_carried(c);
         CK(cudaGraphLaunch(c->graph[par], st));
         c->cur = par ^ 1;
         point_carried(c);
@@ -1046,19 +1076,21 @@ int sph3_morton_order(sph3_ctx *c, int64_t *order, uint64_t *keys) {
     if (!c->have) return SPH3_ERR_STATE;
     if (c->S.n == 0) return SPH3_OK;
     CK(cudaSetDevice(c->device));
+    const int rc = sync_packs(c, c->stream);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     if (order) CK(cudaMemcpy(order, c->S.orig, sizeof(int64_t) * c->S.n, cudaMemcpyDeviceToHost));
     if (keys) CK(cudaMemcpy(keys, c->S.key, sizeof(uint64_t) * c->S.n, cudaMemcpyDeviceToHost));
     return SPH3_OK;
 }
 
-int sph3_counters(sph3_ctx *c, int64_t out[8], int clear) {
+int sph3_counters(sph3_ctx *c, int64_t out[16], int clear) {
     if (!c || !out) return SPH3_ERR_INVALID_ARG;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
-    unsigned long long v[8];
+    unsigned long long v[kNumCounters];
     CK(cudaMemcpy(v, c->S.counters, sizeof(v), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < 8; ++k) out[k] = (int64_t)v[k];
+    for (int k = 0; k < kNumCounters; ++k) out[k] = (int64_t)v[k];
     if (clear) CK(cudaMemset(c->S.counters, 0, sizeof(v)));
     return SPH3_OK;
 }

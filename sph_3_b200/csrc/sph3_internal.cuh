@@ -34,7 +34,7 @@ namespace sph3 {
 constexpr int kWarp = 32;
 constexpr int kGroup = 32;        // target particles per walk group (one warp)
 constexpr int kCellBits = 10;     // level of the FP32 cell-relative frame
-constexpr int kWalkWarps = 4;     // warps per walk block
+constexpr int kWalkWarps = 8;     // largest walk block (warps); the width is a runtime tunable
 // resident walk blocks per SM the register budget must allow; capping the
 // registers (e.g. 8 -> 64 regs) spilled and measured slower on B200
 constexpr int kWalkMinBlocks = 1;
@@ -42,6 +42,16 @@ constexpr int kLeafQ = 96;        // queued leaves per warp before a flush
 constexpr int kNodeQ = 64;        // queued multipole nodes per warp (gravity)
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBoxChunk = 32768;  // particles per root-cube reduction block
+
+// device counters (sph3_counters): 0..7 as documented in sph3.h, then walk
+// statistics
+constexpr int kNumCounters = 16;
+constexpr int kCntVisitsH = 8;         // nodes popped by the h-search walks
+constexpr int kCntVisitsDensity = 9;   // ... density walks
+constexpr int kCntVisitsHydro = 10;    // ... hydro walks
+constexpr int kCntVisitsGravity = 11;  // ... gravity walks
+constexpr int kCntWalkMaxIter = 12;    // longest single walk (loop iterations)
+constexpr int kCntWalkMaxWhere = 13;   // iterations << 40 | visit slot << 32 | first particle of that walk
 
 // ------------------------------------------------------------ per cloud
 struct Cloud {
@@ -122,11 +132,13 @@ struct State {
     // launch geometry
     int num_sms = 0;
     int walk_blocks = 0;
+    int walk_warps = 4;  // warps per walk block (the config's walk_warps)
 };
 
 struct Params {
     int precision, h_mode, visc, step_order, n_ngb, n_ngb_tol, h_max_iter, n_boot;
     int leaf_size, stack_cap, max_level, gravity, quadrupole;
+    int walk_warps;  // warps per walk block (1, 2, 4 or 8)
     double gamma, alpha, beta, eta, G, theta, eps;
     double box[3];
     int periodic;

@@ -312,64 +312,121 @@ void launch_tree_refit_h(State &S, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------ walk groups
-// Target groups for the walks: spatially compact runs of at most kGroup
-// consecutive particles.  Each internal node with more than kGroup particles
-// packs its consecutive children of <= kGroup particles greedily into groups
-// (so a group lies inside one parent cell) and splits a child leaf of more
-// than kGroup particles into kGroup-sized chunks; a small or leaf root is
-// handled the same way.  Every particle lands in exactly one group: along
-// its root-to-leaf chain the first node with <= kGroup particles is packed by
-// its parent, and a chain without one ends in an oversized leaf that is
-// chunked.  Group order in the table does not affect any result.
+// Target groups for the walks: runs of at most kGroup consecutive particles
+// whose bounding box is small on the scale of their smoothing lengths (a
+// walk's work grows with (group extent + 2h)^3, so one sprawling group can
+// stall a whole persistent kernel).
+//
+// A node is *compact* if it holds <= kGroup particles and its bbox extent is
+// at most kGroupSpan * hmax (or it holds one particle, or no h is known yet).
+// Every non-compact internal node acts as a parent: it packs its consecutive
+// compact children greedily into groups while the merged bbox stays within
+// kGroupSpan * (largest hmax) and the count within kGroup; a non-compact leaf
+// child is split into kGroup-sized chunks if it is only too populous, or into
+// one group per particle if it is sprawling.  A compact root is one group.
+// Every particle lands in exactly one group: the first compact node on its
+// root-to-leaf chain is packed by its (non-compact) parent, and a chain
+// without one ends in a non-compact leaf that its parent splits.  The order
+// of the group table does not affect any result.
+constexpr double kGroupSpan = 4.0;
+
 __device__ __forceinline__ void emit_group(int2 *groups, int *gcl, int *ng, int first, int count, int cloud) {
     const int g = atomicAdd(ng, 1);
     groups[g] = make_int2(first, count);
     gcl[g] = cloud;
 }
 
+__device__ __forceinline__ double node_extent(const Tree &T, int i) {
+    const int cap = T.cap;
+    return fmax(T.bmax[i] - T.bmin[i],
+                fmax(T.bmax[cap + i] - T.bmin[cap + i], T.bmax[2 * cap + i] - T.bmin[2 * cap + i]));
+}
+
+// length scale of a node: its largest h, or "any size" before h is known
+__device__ __forceinline__ double node_scale(const Tree &T, int i) {
+    const double h = T.hmax[i];
+    return h > 0.0 ? kGroupSpan * h : DBL_MAX;
+}
+
+__device__ __forceinline__ bool compact_node(const Tree &T, int i) {
+    const int cnt = T.range[i].y;
+    return cnt <= kGroup && (cnt == 1 || node_extent(T, i) <= node_scale(T, i));
+}
+
+// a leaf that is not compact: kGroup-sized chunks if it is only too populous,
+// one group per particle if it sprawls
+__device__ __forceinline__ void split_leaf(const Tree &T, int c, int2 *groups, int *gcl, int *ng, int cloud) {
+    const int2 r = T.range[c];
+    const int step = node_extent(T, c) <= node_scale(T, c) ? kGroup : 1;
+    for (int f = r.x; f < r.x + r.y; f += step) emit_group(groups, gcl, ng, f, min(step, r.x + r.y - f), cloud);
+}
+
 __global__ void k_make_groups(Tree T, int ncloud, int max_depth, const uint64_t *key, int max_level,
                               int2 *groups, int *gcl, int *ng) {
     const int nn = T.depth_begin[max_depth];
+    const int cap = T.cap;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
         const int2 r = T.range[i];
         if (r.y == 0) continue;
         const int cloud = (int)(key[r.x] >> (3 * max_level));
         const int2 ch = T.child[i];
         const int nch = ch.y & 255;
-        if (i < ncloud) {  // a cloud root that nobody packs
-            if (r.y <= kGroup) {
+        const bool ci = compact_node(T, i);
+        if (i < ncloud) {  // a cloud root: nobody packs it
+            if (ci) {
                 emit_group(groups, gcl, ng, r.x, r.y, cloud);
                 continue;
             }
             if (nch == 0) {
-                for (int f = r.x; f < r.x + r.y; f += kGroup)
-                    emit_group(groups, gcl, ng, f, min(kGroup, r.x + r.y - f), cloud);
+                split_leaf(T, i, groups, gcl, ng, cloud);
                 continue;
             }
         }
-        if (nch == 0 || r.y <= kGroup) continue;
+        if (nch == 0 || ci) continue;  // leaves and compact nodes are handled by their parent
         int open_first = -1, open_count = 0;
+        double lo[3], hi[3], scale = 0.0;
+        auto flush = [&]() {
+            if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+            open_first = -1;
+            open_count = 0;
+        };
         for (int c = ch.x; c < ch.x + nch; ++c) {
             const int2 cr = T.range[c];
-            const bool leaf = (T.child[c].y & 255) == 0;
-            if (cr.y <= kGroup) {
+            if (cr.y == 0) continue;
+            if (compact_node(T, c)) {
+                bool merged = false;
                 if (open_first >= 0 && open_count + cr.y <= kGroup) {
-                    open_count += cr.y;
-                } else {
-                    if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+                    double ext = 0.0;
+                    for (int d = 0; d < 3; ++d)
+                        ext = fmax(ext, fmax(hi[d], T.bmax[d * cap + c]) - fmin(lo[d], T.bmin[d * cap + c]));
+                    const double sc = fmax(scale, node_scale(T, c));
+                    if (ext <= sc) {
+                        open_count += cr.y;
+                        for (int d = 0; d < 3; ++d) {
+                            lo[d] = fmin(lo[d], T.bmin[d * cap + c]);
+                            hi[d] = fmax(hi[d], T.bmax[d * cap + c]);
+                        }
+                        scale = sc;
+                        merged = true;
+                    }
+                }
+                if (!merged) {
+                    flush();
                     open_first = cr.x;
                     open_count = cr.y;
+                    for (int d = 0; d < 3; ++d) {
+                        lo[d] = T.bmin[d * cap + c];
+                        hi[d] = T.bmax[d * cap + c];
+                    }
+                    scale = node_scale(T, c);
                 }
             } else {
-                if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
-                open_first = -1;
-                open_count = 0;
-                if (leaf)
-                    for (int f = cr.x; f < cr.x + cr.y; f += kGroup)
-                        emit_group(groups, gcl, ng, f, min(kGroup, cr.x + cr.y - f), cloud);
+                flush();
+                if ((T.child[c].y & 255) == 0) split_leaf(T, c, groups, gcl, ng, cloud);
+                // a non-compact internal child packs its own children
             }
         }
-        if (open_first >= 0) emit_group(groups, gcl, ng, open_first, open_count, cloud);
+        flush();
     }
 }
 

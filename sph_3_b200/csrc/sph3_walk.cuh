@@ -69,6 +69,7 @@ struct GroupBox {
     float3 hw;  // half widths
     int ref;
     float s10;
+    int first = -1;  // first sorted particle of the group (walk statistics)
 };
 
 __device__ __forceinline__ GroupBox group_box(float3 p, bool active, int ref, float s10) {

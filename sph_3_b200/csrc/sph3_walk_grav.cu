@@ -247,13 +247,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GAr
         if (lane == 0) wm.stack[0] = cl.root;
         __syncwarp();
         int nleaf = 0, nnode = 0;
+        unsigned long long visits = 0;
+        int guard = 0;
         // each node is popped at most once; the bound only trips on a corrupted tree
-        for (int guard = 0; top > 0; ++guard) {
+        for (; top > 0; ++guard) {
             if (guard > A.cap) {
                 if (lane == 0) set_status(A.status, SPH3_STATUS_STACK_OVERFLOW);
                 break;
             }
             const int p = pop_width(top, A.stack_cap, A.max_depth);
+            visits += p;
             int node = -1;
             if (lane < p) node = wm.stack[top - 1 - lane];
             __syncwarp();
@@ -297,6 +300,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GAr
         __syncwarp();
         if (nnode > 0) flush_nodes(nnode);
         if (nleaf > 0) flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
+        if (lane == 0) {  // walk statistics
+            atomicAdd(&A.counters[kCntVisitsGravity], visits);
+            atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
+        }
         if (active) {
             A.acc_g[i] = A.G * (double)ax;
             A.acc_g[A.n + i] = A.G * (double)ay;
@@ -322,9 +329,10 @@ static void allow_smem_g(const void *kern) {
 
 template <typename R, bool QUAD>
 static void launch_grav_t(const GArgs &A, State &S, const Params &P, cudaStream_t st) {
-    const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<R>)) * kWalkWarps;
+    const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<R>)) * P.walk_warps;
     allow_smem_g((const void *)k_gravity<R, QUAD>);
-    k_gravity<R, QUAD><<<S.walk_blocks, kWalkWarps * 32, sm, st>>>(A);
+    // persistent grid: 32 warps' worth of blocks per SM
+    k_gravity<R, QUAD><<<S.num_sms * (32 / P.walk_warps), P.walk_warps * 32, sm, st>>>(A);
 }
 
 void launch_gravity(State &S, const Params &P, cudaStream_t st) {

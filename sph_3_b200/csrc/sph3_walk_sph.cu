@@ -50,6 +50,7 @@ struct WalkArgs {
     int *work;
     unsigned *status;
     unsigned long long *counters;
+    int visit_slot;  // counter that accumulates this pass's node visits
 };
 
 // division in the pass precision: the FP32 path uses the approximate
@@ -77,12 +78,15 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
     const float margin = 1.0f + 4e-5f;
     // every node is popped at most once per walk; the bound only trips on a
     // corrupted tree, which then raises a status bit instead of spinning
-    for (int guard = 0; top > 0; ++guard) {
+    unsigned long long visits = 0;
+    int guard = 0;
+    for (; top > 0; ++guard) {
         if (guard > a.node_cap) {
             if (lane == 0) set_status(a.status, SPH3_STATUS_STACK_OVERFLOW);
             break;
         }
         const int p = pop_width(top, a.stack_cap, a.max_depth);
+        visits += p;
         int node = -1;
         if (lane < p) node = wm.stack[top - 1 - lane];
         __syncwarp();
@@ -121,6 +125,13 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
     }
     __syncwarp();
     if (nleaf > 0) flush(nleaf);
+    if (lane == 0) {  // walk statistics: node visits per pass, longest walk (and where)
+        atomicAdd(&a.counters[a.visit_slot], visits);
+        atomicMax(&a.counters[kCntWalkMaxIter], (unsigned long long)guard);
+        atomicMax(&a.counters[kCntWalkMaxWhere],
+                  ((unsigned long long)guard << 40) | ((unsigned long long)a.visit_slot << 32) |
+                      (unsigned long long)(unsigned)gb.first);
+    }
 }
 
 // ------------------------------------------------------------ group setup
@@ -209,6 +220,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HA
         const Cloud &cl = a.clouds[gi.cloud];
         const int64_t ncl = cl.end - cl.begin;
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        gb.first = gi.first;
         R tx, ty, tz;
         if (sizeof(R) == 8) {
             tx = (R)a.pos[gi.i];
@@ -404,6 +416,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_boot_h(Boot
         const int64_t ncl = cl.end - cl.begin;
         const int need = (int)std::min<int64_t>((int64_t)A.k, ncl - 1) + 1;
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        gb.first = gi.first;
         const double tx = a.pos[gi.i], ty = a.pos[a.n + gi.i], tz = a.pos[2 * a.n + gi.i];
         // phase 1: grow a common radius until every target has `need` particles within it
         double Rg = 2.0 * (double)fmaxf(gb.hw.x, fmaxf(gb.hw.y, gb.hw.z)) + (double)gi.s10;
@@ -514,6 +527,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
     for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        gb.first = gi.first;
         R tx, ty, tz, th, tvx = 0, tvy = 0, tvz = 0;
         if (sizeof(R) == 8) {
             tx = (R)a.pos[gi.i]; ty = (R)a.pos[a.n + gi.i]; tz = (R)a.pos[2 * a.n + gi.i];
@@ -707,6 +721,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
     for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
+        gb.first = gi.first;
         const int i = gi.i;
         R tx, ty, tz, tvx, tvy, tvz, th, trho, tpr, tc, tf;
         if (sizeof(R) == 8) {
@@ -956,13 +971,16 @@ static WalkArgs walk_args(State &S, const Params &P, int slot) {
     a.work = S.work + slot;
     a.status = S.status;
     a.counters = S.counters;
+    // node-visit counters: boot h / h search / density / hydro / neighbours
+    static const int kVisitSlot[5] = {kCntVisitsH, kCntVisitsH, kCntVisitsDensity, kCntVisitsHydro, kCntVisitsH};
+    a.visit_slot = kVisitSlot[slot];
     return a;
 }
 
 // dynamic shared memory of a walk block whose tile entries are E (double buffered)
 template <typename E>
 static size_t walk_smem(const Params &P) {
-    return warp_mem_bytes(P.stack_cap, sizeof(E) * 64) * kWalkWarps;
+    return warp_mem_bytes(P.stack_cap, sizeof(E) * 64) * P.walk_warps;
 }
 
 static void allow_smem(const void *kern) {
@@ -977,7 +995,8 @@ template <typename Args>
 static void run_walk(void (*kern)(Args), const Args &args, size_t smem, State &S, cudaStream_t st, int slot) {
     allow_smem((const void *)kern);
     cudaMemsetAsync(S.work + slot, 0, sizeof(int), st);
-    kern<<<S.walk_blocks, kWalkWarps * 32, smem, st>>>(args);
+    // persistent grid: 32 warps' worth of blocks per SM
+    kern<<<S.num_sms * (32 / S.walk_warps), S.walk_warps * 32, smem, st>>>(args);
 }
 
 void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
@@ -1112,10 +1131,10 @@ int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev,
     A.cursor = nullptr;
     const size_t sm = walk_smem<V4<double>>(P);
     allow_smem((const void *)k_neighbours);
-    int blocks = (int)std::min<int64_t>((nrows + kWalkWarps - 1) / kWalkWarps, (int64_t)S.num_sms * 8);
+    int blocks = (int)std::min<int64_t>((nrows + S.walk_warps - 1) / S.walk_warps, (int64_t)S.num_sms * 8);
     // pass 0: counts into offsets[0..nrows)
     A.pass = 0;
-    k_neighbours<<<blocks, kWalkWarps * 32, sm, st>>>(A);
+    k_neighbours<<<blocks, S.walk_warps * 32, sm, st>>>(A);
     // exclusive scan on the host (few rows)
     std::vector<int64_t> hv(nrows + 1);
     cudaMemcpyAsync(hv.data(), offsets_dev, sizeof(int64_t) * nrows, cudaMemcpyDeviceToHost, st);
@@ -1133,7 +1152,7 @@ int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev,
     cudaMemsetAsync(cursor, 0, sizeof(int) * nrows, st);
     A.cursor = cursor;
     A.pass = 1;
-    k_neighbours<<<blocks, kWalkWarps * 32, sm, st>>>(A);
+    k_neighbours<<<blocks, S.walk_warps * 32, sm, st>>>(A);
     cudaFreeAsync(cursor, st);
     cudaStreamSynchronize(st);
     return 0;
