@@ -219,7 +219,11 @@ def run_ours(args, rank, world, local_rank):
     kphase = max(3, min(args.steps, 8))
     ctx.step(DT, kphase)
     ph = {k: v / kphase for k, v in ctx.phase_times().items()}
-    cnt = {k: v / kphase for k, v in ctx.counters().items()}
+    raw = ctx.counters()
+    # tree sizes are set by the last build and the walk maxima are maxima, not sums
+    cnt = {k: (v if k in ("tree_nodes", "walk_max_iter") else v / kphase) for k, v in raw.items()
+           if k != "walk_max_where"}
+    cnt["mean_group_size"] = n / max(cnt.get("grav_groups", 0), 1)
     ctx.set_config(ctx.config.replace(timing=False))
 
     # ---- e2e through host buffers (pinned), C ABI per step

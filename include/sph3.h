@@ -244,7 +244,9 @@ int sph3_morton_order(sph3_ctx *ctx, int64_t *order, uint64_t *keys);
  * the density pass, [3] of the hydro pass, [4] h-search candidate pairs,
  * [5] h passes, [6] tree nodes (of the last build), [7] tree leaves,
  * [8..11] tree nodes visited by the h-search / density / hydro / gravity
- * walks, [12] the longest single walk (loop iterations), [13..15] reserved.
+ * walks, [12] the longest single walk (loop iterations), [13] where it
+ * happened (iterations << 40 | walk kind << 32 | first particle), [14]
+ * particle groups walked by the gravity pass, [15] reserved.
  * Clears them if `clear`. */
 int sph3_counters(sph3_ctx *ctx, int64_t out[16], int clear);
 

@@ -236,7 +236,7 @@ class Context:
               "counters")
         keys = ["grav_node", "grav_part", "density_pairs", "hydro_pairs", "h_pairs", "h_passes",
                 "tree_nodes", "tree_leaves", "visits_h", "visits_density", "visits_hydro", "visits_gravity",
-                "walk_max_iter"]
+                "walk_max_iter", "walk_max_where", "grav_groups"]
         return dict(zip(keys, out.tolist()))
 
     def phase_times(self, clear=False):

@@ -41,10 +41,11 @@ constexpr int kWalkMinBlocks = 1;
 constexpr int kLeafQ = 96;        // queued leaves per warp before a flush
 constexpr int kNodeQ = 64;        // queued multipole nodes per warp (gravity)
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kBoxChunk = 32768;  // particles per root-cube reduction block
+constexpr int kBoxChunk = 4096;  // particles per root-cube reduction block
 
 // device counters (sph3_counters): 0..7 as documented in sph3.h, then walk
 // statistics
+constexpr int kRsOffsetThreads = 1024;  // threads of the one-block radix offset scan
 constexpr int kNumCounters = 16;
 constexpr int kCntVisitsH = 8;         // nodes popped by the h-search walks
 constexpr int kCntVisitsDensity = 9;   // ... density walks
@@ -52,6 +53,7 @@ constexpr int kCntVisitsHydro = 10;    // ... hydro walks
 constexpr int kCntVisitsGravity = 11;  // ... gravity walks
 constexpr int kCntWalkMaxIter = 12;    // longest single walk (loop iterations)
 constexpr int kCntWalkMaxWhere = 13;   // iterations << 40 | visit slot << 32 | first particle of that walk
+constexpr int kCntGravGroups = 14;     // groups walked by the gravity pass
 
 // ------------------------------------------------------------ per cloud
 struct Cloud {
@@ -86,6 +88,7 @@ struct Tree {
     int *depth_begin;   // [max_depth + 2] node id where each depth starts
     int *nchild_tmp;    // [cap] scan input
     int *scan_tmp;      // [cap] scan output
+    int *bounds;        // [8][n + ncloud + 64] octant starts of one depth's nodes
     int *total;         // [4] scratch counters
 };
 

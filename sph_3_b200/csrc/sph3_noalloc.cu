@@ -36,7 +36,7 @@ __global__ void k_keys(const Cloud *clouds, int ncloud, const double *pos, int64
                        uint64_t *key, uint32_t *perm);
 __global__ void __launch_bounds__(256) k_rs_hist(const uint64_t *key, int64_t n, int shift, uint32_t *hist,
                                                  int nblocks);
-__global__ void __launch_bounds__(256) k_rs_offsets(uint32_t *hist, int nblocks);
+__global__ void __launch_bounds__(kRsOffsetThreads) k_rs_offsets(uint32_t *hist, int nblocks);
 __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t *key_in, const uint32_t *val_in,
                                                     uint64_t *key_out, uint32_t *val_out, int64_t n, int shift,
                                                     const uint32_t *hist, int nblocks);
@@ -159,7 +159,7 @@ extern "C" int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t ma
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
         k_rs_hist<<<nb, 256, 0, st>>>(kin, n, shift, hist, nb);
-        k_rs_offsets<<<1, 256, 0, st>>>(hist, nb);
+        k_rs_offsets<<<1, kRsOffsetThreads, 0, st>>>(hist, nb);
         k_rs_scatter<<<nb, 256, 0, st>>>(kin, vin, kout, vout, n, shift, hist, nb);
         uint64_t *tk = kin;
         kin = kout;

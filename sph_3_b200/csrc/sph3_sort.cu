@@ -181,37 +181,70 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t *key, int
     hist[blockIdx.x * 256 + threadIdx.x] = h[threadIdx.x];  // block-major table
 }
 
-// Offsets from the block-major table: thread d scans digit d's column over
-// the blocks (coalesced row loads), then the digit totals are scanned; the
-// digit bases land in hist[nblocks * 256 + d].
-__global__ void __launch_bounds__(256) k_rs_offsets(uint32_t *hist, int nblocks) {
+// Exclusive prefix of the block-major digit histogram, in place: hist[b][d]
+// becomes the number of keys with digit d in blocks before b, and
+// hist[nblocks][d] the number of keys with a smaller digit.  One block of
+// kRsOffsetThreads threads: 256 digits x kOffQ block ranges; each range is
+// summed with kOffU independent loads in flight, the ranges and digits are
+// combined in shared memory, and a second pass over the (L2-resident) table
+// writes the prefixes.
+constexpr int kOffQ = kRsOffsetThreads / 256;
+constexpr int kOffU = 16;
+
+__global__ void __launch_bounds__(kRsOffsetThreads) k_rs_offsets(uint32_t *hist, int nblocks) {
+    __shared__ uint32_t part[kOffQ][256];
     __shared__ uint32_t tot[256];
-    const int d = threadIdx.x;
-    uint32_t run = 0;
-    int b = 0;
-    for (; b + 4 <= nblocks; b += 4) {
-        const uint32_t v0 = hist[(b + 0) * 256 + d], v1 = hist[(b + 1) * 256 + d];
-        const uint32_t v2 = hist[(b + 2) * 256 + d], v3 = hist[(b + 3) * 256 + d];
-        hist[(b + 0) * 256 + d] = run;
-        hist[(b + 1) * 256 + d] = run + v0;
-        hist[(b + 2) * 256 + d] = run + v0 + v1;
-        hist[(b + 3) * 256 + d] = run + v0 + v1 + v2;
-        run += v0 + v1 + v2 + v3;
+    const int d = threadIdx.x & 255, q = threadIdx.x >> 8;
+    const int per = (nblocks + kOffQ - 1) / kOffQ;
+    const int b0 = min(nblocks, q * per), b1 = min(nblocks, b0 + per);
+    uint32_t s = 0;
+    int b = b0;
+    for (; b + kOffU <= b1; b += kOffU) {
+        uint32_t v[kOffU];
+#pragma unroll
+        for (int k = 0; k < kOffU; ++k) v[k] = hist[(size_t)(b + k) * 256 + d];
+#pragma unroll
+        for (int k = 0; k < kOffU; ++k) s += v[k];
     }
-    for (; b < nblocks; ++b) {
-        const uint32_t v = hist[b * 256 + d];
-        hist[b * 256 + d] = run;
+    for (; b < b1; ++b) s += hist[(size_t)b * 256 + d];
+    part[q][d] = s;
+    __syncthreads();
+    if (q == 0) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int k = 0; k < kOffQ; ++k) {
+            const uint32_t t = part[k][d];
+            part[k][d] = run;
+            run += t;
+        }
+        tot[d] = run;
+    }
+    __syncthreads();
+    const uint32_t own = tot[d];
+    for (int o = 1; o < 256; o <<= 1) {
+        const uint32_t v = (q == 0 && d >= o) ? tot[d - o] : 0u;
+        __syncthreads();
+        if (q == 0) tot[d] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[q][d];
+    b = b0;
+    for (; b + kOffU <= b1; b += kOffU) {
+        uint32_t v[kOffU];
+#pragma unroll
+        for (int k = 0; k < kOffU; ++k) v[k] = hist[(size_t)(b + k) * 256 + d];
+#pragma unroll
+        for (int k = 0; k < kOffU; ++k) {
+            hist[(size_t)(b + k) * 256 + d] = run;
+            run += v[k];
+        }
+    }
+    for (; b < b1; ++b) {
+        const uint32_t v = hist[(size_t)b * 256 + d];
+        hist[(size_t)b * 256 + d] = run;
         run += v;
     }
-    tot[d] = run;
-    __syncthreads();
-    for (int o = 1; o < 256; o <<= 1) {
-        const uint32_t v = d >= o ? tot[d - o] : 0u;
-        __syncthreads();
-        tot[d] += v;
-        __syncthreads();
-    }
-    hist[nblocks * 256 + d] = tot[d] - run;  // exclusive digit base
+    if (q == 0) hist[(size_t)nblocks * 256 + d] = tot[d] - own;  // exclusive digit base
 }
 
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
@@ -278,7 +311,7 @@ void launch_radix_sort(State &S, cudaStream_t st) {
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
         k_rs_hist<<<nb, kRsThreads, 0, st>>>(kin, S.n, shift, S.sort_hist, nb);
-        k_rs_offsets<<<1, 256, 0, st>>>(S.sort_hist, nb);
+        k_rs_offsets<<<1, kRsOffsetThreads, 0, st>>>(S.sort_hist, nb);
         k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kin, vin, kout, vout, S.n, shift, S.sort_hist, nb);
         uint64_t *tk = kin;
         kin = kout;

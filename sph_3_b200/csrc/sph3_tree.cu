@@ -5,13 +5,15 @@
 // keys share a common prefix; its level is the deepest level whose cell holds
 // the whole run.  A node with more than leaf_size particles (and level below
 // max_level) is split on the next 3-bit digit into its 2..8 non-empty
-// sub-runs, found by binary search (digits are non-decreasing inside a run).
+// sub-runs (digits are non-decreasing inside a run, so each digit's start is
+// one boundary: a warp per node finds the 8 starts once and keeps them).
 // Single-child chains never appear, so nodes < 2 * particles.  Children of a
 // node are stored contiguously and each depth is compacted with an exclusive
 // scan, so the layout, and every sum over it, is deterministic.
 // Compared with the reference's pointer octree (bh_tree_iteration_v2.h:149-450:
 // one block, atomicCAS locks, a DFS sort that spins on its parent) there are
 // no locks and no waits.
+#include <algorithm>
 #include <cfloat>
 
 #include "sph3_internal.cuh"
@@ -40,34 +42,57 @@ __global__ void k_tree_roots(Tree T, Cloud *clouds, int ncloud, const uint64_t *
     cl.root = c;
 }
 
-// number of children of each node of depth d (0 for a leaf)
+// Children of each node of depth d: one warp per node finds where each
+// 3-bit digit of the next level starts inside the node's sorted key run and
+// stores the 8 starts (-1 for an empty octant) in T.bounds; nchild_tmp gets
+// the number of non-empty octants (0 for a leaf).  Small runs are scanned
+// with coalesced loads (a digit starts where it differs from the previous
+// key's); large runs binary-search the 7 digit boundaries, one per lane.
+constexpr int kTreeScanMax = 1024;  // runs up to this size are scanned linearly
+
 __global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
-    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        int2 r = T.range[i];
-        int lvl = T.child[i].y >> 8;
-        int nch = 0;
-        if (r.y > leaf_size && lvl < max_level) {
-            const int shift = 3 * (max_level - lvl - 1);
-            int lo = r.x;
-            const int e = r.x + r.y;
-            int prev_digit = -1;
-            // walk the distinct digits by successive binary searches
-            while (lo < e) {
-                int dg = (int)((key[lo] >> shift) & 7u);
-                if (dg != prev_digit) ++nch;
-                prev_digit = dg;
-                // first index with digit > dg
-                int a = lo, b = e;
-                while (a < b) {
-                    int mid = (a + b) >> 1;
-                    if ((int)((key[mid] >> shift) & 7u) <= dg) a = mid + 1;
-                    else b = mid;
-                }
-                lo = a;
-            }
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int i = beg + warp; i < end; i += nwarp) {
+        const int2 r = T.range[i];
+        const int lvl = T.child[i].y >> 8;
+        int *bnd = T.bounds + 8 * (size_t)(i - beg);
+        if (!(r.y > leaf_size && lvl < max_level)) {
+            if (lane == 0) T.nchild_tmp[i - beg] = 0;
+            continue;
         }
-        T.nchild_tmp[i - beg] = nch;
+        const int shift = 3 * (max_level - lvl - 1);
+        const int s = r.x, e = r.x + r.y;
+        if (lane < 8) bnd[lane] = -1;
+        __syncwarp();
+        if (r.y <= kTreeScanMax) {
+            for (int b = s; b < e; b += 32) {
+                const int k = b + lane;
+                int dg = -1, prev = -1;
+                if (k < e) {
+                    dg = (int)((key[k] >> shift) & 7u);
+                    prev = k > s ? (int)((key[k - 1] >> shift) & 7u) : -1;
+                }
+                if (k < e && dg != prev) bnd[dg] = k;  // each digit starts once
+            }
+        } else if (lane < 8) {
+            // first index with digit >= lane (digits are non-decreasing)
+            int a = s, b = e;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if ((int)((key[mid] >> shift) & 7u) < lane) a = mid + 1;
+                else b = mid;
+            }
+            const int nxt = __shfl_down_sync(0xffu, a, 1, 8);
+            const int stop = lane == 7 ? e : nxt;
+            bnd[lane] = a < stop ? a : -1;
+        }
+        __syncwarp();
+        const int v = lane < 8 ? bnd[lane] : -1;
+        const int nch = __popc(__ballot_sync(kFull, v >= 0));
+        if (lane == 0) T.nchild_tmp[i - beg] = nch;
     }
 }
 
@@ -128,24 +153,23 @@ __global__ void k_tree_emit(Tree T, const uint64_t *key, int d, int leaf_size, i
         }
         const int cf = end + T.scan_tmp[i - beg];
         T.child[i] = make_int2(cf, nch | (lvl << 8));
-        int2 r = T.range[i];
-        const int shift = 3 * (max_level - lvl - 1);
-        int lo = r.x, c = 0;
+        const int2 r = T.range[i];
         const int e = r.x + r.y;
-        while (lo < e && c < nch) {
-            int dg = (int)((key[lo] >> shift) & 7u);
-            int a = lo, b = e;
-            while (a < b) {
-                int mid = (a + b) >> 1;
-                if ((int)((key[mid] >> shift) & 7u) <= dg) a = mid + 1;
-                else b = mid;
-            }
-            const int cnt = a - lo;
-            const int cl = common_level(key[lo], key[a - 1], max_level);
-            T.range[cf + c] = make_int2(lo, cnt);
+        const int4 *bq = reinterpret_cast<const int4 *>(T.bounds + 8 * (size_t)(i - beg));
+        const int4 b0 = bq[0], b1 = bq[1];
+        const int st[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        int c = 0;
+#pragma unroll
+        for (int dg = 0; dg < 8; ++dg) {
+            if (st[dg] < 0) continue;
+            int stop = e;
+#pragma unroll
+            for (int q = 7; q > dg; --q)
+                if (st[q] >= 0) stop = st[q];
+            const int cl = common_level(key[st[dg]], key[stop - 1], max_level);
+            T.range[cf + c] = make_int2(st[dg], stop - st[dg]);
             T.child[cf + c] = make_int2(-1, cl << 8);
             ++c;
-            lo = a;
         }
     }
 }

@@ -192,6 +192,56 @@ __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq
     }
 }
 
+// As flush_leaves, with the tile layout left to the caller:
+// store(buf, slot, entry, have) writes slot `slot` (0..31) of buffer `buf`
+// (0 or 1) and is called for every slot, with have = false (write padding)
+// where no candidate is left; interact(buf, ne) runs the targets against the
+// first ne entries of buffer buf.  Padded slots let the interaction run
+// whole pairs of entries without bounds checks.
+template <class E, class Load, class Store, class Interact>
+__device__ __forceinline__ void flush_leaves_st(const int2 *range, const int *leafq, int nleaf, int *lfirst,
+                                                int *lpre, Load &load, Store &store, Interact &interact) {
+    const int lane = lane_id();
+    for (int base = 0; base < nleaf; base += 32) {
+        int cnt = 0, fst = 0;
+        if (base + lane < nleaf) {
+            int2 r = range[leafq[base + lane]];
+            fst = r.x;
+            cnt = r.y;
+        }
+        const int incl = warp_incl_scan(cnt);
+        const int tot = __shfl_sync(kFull, incl, 31);
+        __syncwarp();
+        lfirst[lane] = fst;
+        lpre[lane] = incl - cnt;
+        __syncwarp();
+        const int nl = min(32, nleaf - base);
+        auto fetch = [&](int c0, E &out) -> bool {
+            const int t = c0 + lane;
+            if (t >= tot) return false;
+            int lo = 0, hi = nl - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (lpre[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            out = load(lfirst[lo] + (t - lpre[lo]));
+            return true;
+        };
+        E cur{};
+        bool have = fetch(0, cur);
+        int buf = 0;
+        for (int c0 = 0; c0 < tot; c0 += 32) {
+            store(buf, lane, cur, have);
+            __syncwarp();
+            have = c0 + 32 < tot ? fetch(c0 + 32, cur) : false;
+            interact(buf, min(32, tot - c0));
+            buf ^= 1;
+        }
+        __syncwarp();
+    }
+}
+
 // As flush_leaves, but load(j, keep) also says whether candidate j can reach
 // the group at all (tested once per candidate by the lane that loads it);
 // kept candidates are compacted so that every interact() call but the last

@@ -106,61 +106,109 @@ __device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R eps
     ph -= mj * pk;
 }
 
-template <typename R, bool QUAD>
-__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GArgs A) {
+// The walk of one group, shared by both precisions.  Pops up to 32 nodes per
+// iteration, accepts a node as a multipole when the group's bbox lies outside
+// both its opening radius and its softening reach, queues accepted nodes
+// (nodeq) and opened leaves (wm.leafq), and hands full queues to
+// flush_nodes(count) / flush_leaves(count).  Returns the iteration count.
+template <class FlushNodes, class FlushLeaves>
+__device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int *nodeq, const Cloud &cl, int ref,
+                                         const GroupBox &gb, float eps_g, FlushNodes &flush_nodes,
+                                         FlushLeaves &flush_leaves_fn, unsigned long long &visits) {
+    const int lane = lane_id();
+    int top = 1;
+    if (lane == 0) wm.stack[0] = cl.root;
+    __syncwarp();
+    int nleaf = 0, nnode = 0;
+    int guard = 0;
+    // each node is popped at most once; the bound only trips on a corrupted tree
+    for (; top > 0; ++guard) {
+        if (guard > A.cap) {
+            if (lane == 0) set_status(A.status, SPH3_STATUS_STACK_OVERFLOW);
+            break;
+        }
+        const int p = pop_width(top, A.stack_cap, A.max_depth);
+        visits += p;
+        int node = -1;
+        if (lane < p) node = wm.stack[top - 1 - lane];
+        __syncwarp();
+        top -= p;
+        bool take_leaf = false, take_node = false;
+        int nch = 0, cf = 0;
+        if (node >= 0 && A.range[node].y > 0) {
+            const float4 mo = A.mono[node];
+            const float3 c = rel_to(A.com_c[node], ref, cl.s10);
+            const float d2 = point_gap2(gb, c);
+            const float rs = mo.z + eps_g;
+            if (d2 > mo.y * mo.y && d2 > rs * rs) {
+                take_node = true;
+            } else {
+                const int2 ch = A.child[node];
+                const int k = ch.y & 255;
+                if (k == 0) take_leaf = true;
+                else {
+                    nch = k;
+                    cf = ch.x;
+                }
+            }
+        }
+        const unsigned nb = __ballot_sync(kFull, take_node);
+        if (take_node) nodeq[nnode + __popc(nb & lanemask_lt())] = node;
+        nnode += __popc(nb);
+        const unsigned lb = __ballot_sync(kFull, take_leaf);
+        if (take_leaf) wm.leafq[nleaf + __popc(lb & lanemask_lt())] = node;
+        nleaf += __popc(lb);
+        top = push_children(wm.stack, top, A.stack_cap, nch, cf, A.status);
+        __syncwarp();
+        if (nnode > kNodeQ - 32) {
+            flush_nodes(nnode);
+            nnode = 0;
+        }
+        if (nleaf > kLeafQ - 32) {
+            flush_leaves_fn(nleaf);
+            nleaf = 0;
+        }
+    }
+    __syncwarp();
+    if (nnode > 0) flush_nodes(nnode);
+    if (nleaf > 0) flush_leaves_fn(nleaf);
+    return guard;
+}
+
+// FP64 path: one target per lane, AoS tiles of the FP64 masters.
+template <bool QUAD>
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64(GArgs A) {
+    using R = double;
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTile<R>));
     GTile<R> &tile = *reinterpret_cast<GTile<R> *>(wm.tile);
     const int lane = lane_id();
-    unsigned long long n_node = 0, n_part = 0;
+    unsigned long long n_node = 0, n_part = 0, n_grp = 0;
     for (int g = next_group(A.work, A.status); g < *A.ngroups_dev; g = next_group(A.work, A.status)) {
         const int2 gr = A.groups[g];
         const Cloud &cl = A.clouds[A.group_cloud[g]];
         const int ref = __float_as_int(A.pk_pos[gr.x].w);
+        ++n_grp;
         const bool active = lane < gr.y;
         const int i = gr.x + (active ? lane : 0);
         const float3 prel = rel_to(A.pk_pos[i], ref, cl.s10);
         GroupBox gb = group_box(prel, active, ref, cl.s10);
-        R tx, ty, tz, te;
-        if (sizeof(R) == 8) {
-            tx = (R)A.pos[i]; ty = (R)A.pos[A.n + i]; tz = (R)A.pos[2 * A.n + i];
-            te = (R)A.eps[i];
-        } else {
-            tx = (R)prel.x; ty = (R)prel.y; tz = (R)prel.z;
-            te = (R)A.pk_hme[i].z;
-        }
+        const R tx = A.pos[i], ty = A.pos[A.n + i], tz = A.pos[2 * A.n + i], te = A.eps[i];
         const float eps_g = warp_max(active ? (float)te : 0.f);
         R ax = 0, ay = 0, az = 0, ph = 0;
 
-        // ---- multipole list: double-buffered chunks of 32 nodes
         auto load_node = [&](int nd) {
             GN<R> en;
-            if (sizeof(R) == 8) {
-                en.a.x = (R)A.tcom[nd];
-                en.a.y = (R)A.tcom[A.cap + nd];
-                en.a.z = (R)A.tcom[2 * A.cap + nd];
-                en.a.w = (R)A.tmass[nd];
-                if (QUAD) {
-                    en.b.x = (R)A.tquad[nd];
-                    en.b.y = (R)A.tquad[A.cap + nd];
-                    en.b.z = (R)A.tquad[2 * A.cap + nd];
-                    en.b.w = (R)A.tquad[3 * A.cap + nd];
-                    en.qyz = (R)A.tquad[4 * A.cap + nd];
-                }
-            } else {
-                const float3 c = rel_to(A.com_c[nd], ref, cl.s10);
-                en.a.x = (R)c.x;
-                en.a.y = (R)c.y;
-                en.a.z = (R)c.z;
-                en.a.w = (R)A.mono[nd].x;
-                if (QUAD) {
-                    const float4 q = A.quad4[nd];
-                    en.b.x = (R)q.x;
-                    en.b.y = (R)q.y;
-                    en.b.z = (R)q.z;
-                    en.b.w = (R)q.w;
-                    en.qyz = (R)A.quad1[nd];
-                }
+            en.a.x = A.tcom[nd];
+            en.a.y = A.tcom[A.cap + nd];
+            en.a.z = A.tcom[2 * A.cap + nd];
+            en.a.w = A.tmass[nd];
+            if (QUAD) {
+                en.b.x = A.tquad[nd];
+                en.b.y = A.tquad[A.cap + nd];
+                en.b.z = A.tquad[2 * A.cap + nd];
+                en.b.w = A.tquad[3 * A.cap + nd];
+                en.qyz = A.tquad[4 * A.cap + nd];
             }
             return en;
         };
@@ -211,24 +259,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GAr
             }
             __syncwarp();
         };
-        // ---- opened leaves: particle-particle terms
         auto load_part = [&](int j) {
             GP<R> en;
-            if (sizeof(R) == 8) {
-                en.p.x = (R)A.pos[j];
-                en.p.y = (R)A.pos[A.n + j];
-                en.p.z = (R)A.pos[2 * A.n + j];
-                en.p.w = (R)A.m[j];
-                en.e = (R)A.eps[j];
-            } else {
-                const float3 p = rel_to(A.pk_pos[j], ref, cl.s10);
-                const float4 hm = A.pk_hme[j];
-                en.p.x = (R)p.x;
-                en.p.y = (R)p.y;
-                en.p.z = (R)p.z;
-                en.p.w = (R)hm.y;
-                en.e = (R)hm.z;
-            }
+            en.p.x = A.pos[j];
+            en.p.y = A.pos[A.n + j];
+            en.p.z = A.pos[2 * A.n + j];
+            en.p.w = A.m[j];
+            en.e = A.eps[j];
             return en;
         };
         auto part_interact = [&](const GP<R> *t, int ne) {
@@ -241,74 +278,20 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GAr
                 if (r2 > (R)0) spline_force<R>(r2, dx, dy, dz, p4.w, (R)0.5 * (te + t[e].e), ax, ay, az, ph);
             }
         };
-
-        // ---- walk
-        int top = 1;
-        if (lane == 0) wm.stack[0] = cl.root;
-        __syncwarp();
-        int nleaf = 0, nnode = 0;
+        auto flush_leaves_fn = [&](int nl) {
+            flush_leaves(A.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
+        };
         unsigned long long visits = 0;
-        int guard = 0;
-        // each node is popped at most once; the bound only trips on a corrupted tree
-        for (; top > 0; ++guard) {
-            if (guard > A.cap) {
-                if (lane == 0) set_status(A.status, SPH3_STATUS_STACK_OVERFLOW);
-                break;
-            }
-            const int p = pop_width(top, A.stack_cap, A.max_depth);
-            visits += p;
-            int node = -1;
-            if (lane < p) node = wm.stack[top - 1 - lane];
-            __syncwarp();
-            top -= p;
-            bool take_leaf = false, take_node = false;
-            int nch = 0, cf = 0;
-            if (node >= 0 && A.range[node].y > 0) {
-                const float4 mo = A.mono[node];
-                const float3 c = rel_to(A.com_c[node], ref, cl.s10);
-                const float d2 = point_gap2(gb, c);
-                const float rs = mo.z + eps_g;
-                if (d2 > mo.y * mo.y && d2 > rs * rs) {
-                    take_node = true;
-                } else {
-                    const int2 ch = A.child[node];
-                    const int k = ch.y & 255;
-                    if (k == 0) take_leaf = true;
-                    else {
-                        nch = k;
-                        cf = ch.x;
-                    }
-                }
-            }
-            const unsigned nb = __ballot_sync(kFull, take_node);
-            if (take_node) tile.nodeq[nnode + __popc(nb & lanemask_lt())] = node;
-            nnode += __popc(nb);
-            const unsigned lb = __ballot_sync(kFull, take_leaf);
-            if (take_leaf) wm.leafq[nleaf + __popc(lb & lanemask_lt())] = node;
-            nleaf += __popc(lb);
-            top = push_children(wm.stack, top, A.stack_cap, nch, cf, A.status);
-            __syncwarp();
-            if (nnode > kNodeQ - 32) {
-                flush_nodes(nnode);
-                nnode = 0;
-            }
-            if (nleaf > kLeafQ - 32) {
-                flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
-                nleaf = 0;
-            }
-        }
-        __syncwarp();
-        if (nnode > 0) flush_nodes(nnode);
-        if (nleaf > 0) flush_leaves(A.range, wm.leafq, nleaf, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
+        const int guard = grav_walk(A, wm, tile.nodeq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn, visits);
         if (lane == 0) {  // walk statistics
             atomicAdd(&A.counters[kCntVisitsGravity], visits);
             atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
         }
         if (active) {
-            A.acc_g[i] = A.G * (double)ax;
-            A.acc_g[A.n + i] = A.G * (double)ay;
-            A.acc_g[2 * A.n + i] = A.G * (double)az;
-            A.phi[i] = A.G * (double)ph;
+            A.acc_g[i] = A.G * ax;
+            A.acc_g[A.n + i] = A.G * ay;
+            A.acc_g[2 * A.n + i] = A.G * az;
+            A.phi[i] = A.G * ph;
         }
     }
     n_node = warp_sum(n_node);
@@ -316,6 +299,268 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity(GAr
     if (lane == 0) {
         atomicAdd(&A.counters[0], n_node);
         atomicAdd(&A.counters[1], n_part);
+        atomicAdd(&A.counters[kCntGravGroups], n_grp);
+    }
+}
+
+// ------------------------------------------------------------ FP32 path
+// Mixed path with Blackwell's packed FP32 pipe (FFMA2 / FADD2 / FMUL2): each
+// lane runs its target against two tile entries per instruction, so the
+// issue slots per interaction halve.  Tiles are stored as pairs: one 128-bit
+// shared load yields {x0, x1, y0, y1}, i.e. two ready packed operands.
+// Every tile slot is written (padding: zero mass at 1e18, which contributes
+// exactly zero), so whole pairs run without bounds checks.
+//
+// Signs: with d = source - target the monopole pulls along +d.  Quadrupoles
+// are staged negated (Qn = -Q); with w = d.Qn.d the acceleration is
+//   a += (M r^-3 - 2.5 w r^-7) d + (Qn d) r^-5
+// and the potential is -P with P = M r^-1 - 0.5 w r^-5, the same terms as
+// the FP64 path written for the other sign of d.
+//
+// Small groups split the warp: a group of <= 16 (<= 8) targets runs 2 (4)
+// lanes per target, each lane over every 2nd (4th) entry pair, and the
+// copies are summed with shuffles, so fewer lanes idle.
+struct GTileF {
+    float4 na[2][16], nb[2][16], nc[2][16], nd[2][16], ne[2][16];  // node pairs, two buffers
+    float4 pa[2][16], pb[2][16];                                    // particle pairs
+    float2 pe[2][16];
+    int nodeq[kNodeQ];
+};
+
+struct NodeF {
+    float x, y, z, m, qxx, qxy, qxz, qyy, qyz;
+};
+
+struct PartF {
+    float x, y, z, m, e;
+};
+
+constexpr float kPadFar = 1e18f;
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ void put2(float4 &dst, int h, float a, float b) {
+    float *p = reinterpret_cast<float *>(&dst);
+    p[h] = a;
+    p[2 + h] = b;
+}
+
+// the reference's softened kernel inside its support (r < 2 eps), scalar;
+// r2 = 0 (a particle and itself, or coincident particles) contributes nothing
+__device__ __forceinline__ void spline_near(float r2, float r, float e, float &fk, float &pk) {
+    if (r >= 2.f * e) return;
+    if (!(r2 > 0.f)) {
+        fk = 0.f;
+        pk = 0.f;
+        return;
+    }
+    const float ie = 1.f / e;
+    const float q = r * ie;
+    const float q2 = q * q, q3 = q2 * q;
+    if (q <= 1.f) {
+        fk = ie * ie * ie * (4.f / 3.f - 6.f / 5.f * q2 + 0.5f * q3);
+        pk = -2.f * ie * (1.f / 3.f * q2 - 3.f / 20.f * q2 * q2 + 1.f / 20.f * q2 * q3) + 7.f / 5.f * ie;
+    } else {
+        const float rinv = 1.f / r;
+        const float q4 = q2 * q2;
+        fk = rinv * rinv * rinv * (-1.f / 15.f + 8.f / 3.f * q3 - 3.f * q4 + 6.f / 5.f * q4 * q - 1.f / 6.f * q3 * q3);
+        pk = -1.f / 15.f * rinv - ie * (4.f / 3.f * q2 - q3 + 3.f / 10.f * q4 - 1.f / 30.f * q4 * q) + 8.f / 5.f * ie;
+    }
+}
+
+template <bool QUAD>
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f32(GArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTileF));
+    GTileF &tile = *reinterpret_cast<GTileF *>(wm.tile);
+    const int lane = lane_id();
+    unsigned long long n_node = 0, n_part = 0, n_grp = 0;
+    for (int g = next_group(A.work, A.status); g < *A.ngroups_dev; g = next_group(A.work, A.status)) {
+        const int2 gr = A.groups[g];
+        const Cloud &cl = A.clouds[A.group_cloud[g]];
+        const int ref = __float_as_int(A.pk_pos[gr.x].w);
+        ++n_grp;
+        const int split = gr.y <= 8 ? 4 : (gr.y <= 16 ? 2 : 1);
+        const int gw = 32 / split;  // lanes per copy of the group
+        const int slot = lane & (gw - 1), cp = lane / gw;
+        const bool active = slot < gr.y;
+        const bool lead = active && cp == 0;
+        const int i = gr.x + (active ? slot : 0);
+        const float3 prel = rel_to(A.pk_pos[i], ref, cl.s10);
+        GroupBox gb = group_box(prel, active, ref, cl.s10);
+        const float te = A.pk_hme[i].z;
+        const float eps_g = warp_max(active ? te : 0.f);
+        const float2 ntx = f2(-prel.x), nty = f2(-prel.y), ntz = f2(-prel.z), hte = f2(0.5f * te);
+        float2 ax = f2(0.f), ay = f2(0.f), az = f2(0.f), pp = f2(0.f);
+
+        // ---- accepted multipoles
+        auto load_node = [&](int nd) {
+            NodeF en;
+            const float3 c = rel_to(A.com_c[nd], ref, cl.s10);
+            en.x = c.x;
+            en.y = c.y;
+            en.z = c.z;
+            en.m = A.mono[nd].x;
+            if (QUAD) {
+                const float4 q = A.quad4[nd];
+                en.qxx = q.x;
+                en.qxy = q.y;
+                en.qxz = q.z;
+                en.qyy = q.w;
+                en.qyz = A.quad1[nd];
+            }
+            return en;
+        };
+        auto store_node = [&](int buf, int s, const NodeF &e, bool have) {
+            const int p = s >> 1, h = s & 1;
+            put2(tile.na[buf][p], h, have ? e.x : kPadFar, have ? e.y : kPadFar);
+            put2(tile.nb[buf][p], h, have ? e.z : kPadFar, have ? e.m : 0.f);
+            if (QUAD) {
+                put2(tile.nc[buf][p], h, have ? -e.qxx : 0.f, have ? -e.qxy : 0.f);
+                put2(tile.nd[buf][p], h, have ? -e.qxz : 0.f, have ? -e.qyy : 0.f);
+                put2(tile.ne[buf][p], h, have ? -e.qyz : 0.f, have ? e.qxx + e.qyy : 0.f);  // -qzz
+            }
+        };
+        auto node_interact = [&](int buf, int ne) {
+            if (lead) n_node += ne;
+            const int np = (ne + 1) >> 1;
+            for (int pb = 0; pb < np; pb += split) {
+                const int p = pb + cp;  // < 16; pairs past np are padding
+                const float4 a4 = tile.na[buf][p], b4 = tile.nb[buf][p];
+                const float2 dx = __fadd2_rn(lo2(a4), ntx), dy = __fadd2_rn(hi2(a4), nty),
+                             dz = __fadd2_rn(lo2(b4), ntz);
+                const float2 M = hi2(b4);
+                float2 r2 = __fmul2_rn(dx, dx);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                const float2 rinv2 = __fmul2_rn(rinv, rinv);
+                const float2 rinv3 = __fmul2_rn(rinv2, rinv);
+                float2 s = __fmul2_rn(M, rinv3);
+                pp = __ffma2_rn(M, rinv, pp);
+                if (QUAD) {
+                    const float4 c4 = tile.nc[buf][p], d4 = tile.nd[buf][p], e4 = tile.ne[buf][p];
+                    float2 qx = __fmul2_rn(lo2(c4), dx);  // Qn d
+                    qx = __ffma2_rn(hi2(c4), dy, qx);
+                    qx = __ffma2_rn(lo2(d4), dz, qx);
+                    float2 qy = __fmul2_rn(hi2(c4), dx);
+                    qy = __ffma2_rn(hi2(d4), dy, qy);
+                    qy = __ffma2_rn(lo2(e4), dz, qy);
+                    float2 qz = __fmul2_rn(lo2(d4), dx);
+                    qz = __ffma2_rn(lo2(e4), dy, qz);
+                    qz = __ffma2_rn(hi2(e4), dz, qz);
+                    float2 w = __fmul2_rn(dx, qx);  // d.Qn.d
+                    w = __ffma2_rn(dy, qy, w);
+                    w = __ffma2_rn(dz, qz, w);
+                    const float2 rinv5 = __fmul2_rn(rinv3, rinv2);
+                    const float2 rinv7 = __fmul2_rn(rinv5, rinv2);
+                    s = __ffma2_rn(__fmul2_rn(w, f2(-2.5f)), rinv7, s);
+                    pp = __ffma2_rn(__fmul2_rn(w, f2(-0.5f)), rinv5, pp);
+                    ax = __ffma2_rn(qx, rinv5, ax);
+                    ay = __ffma2_rn(qy, rinv5, ay);
+                    az = __ffma2_rn(qz, rinv5, az);
+                }
+                ax = __ffma2_rn(s, dx, ax);
+                ay = __ffma2_rn(s, dy, ay);
+                az = __ffma2_rn(s, dz, az);
+            }
+        };
+        auto flush_nodes = [&](int nq) {
+            NodeF cur{};
+            bool have = lane < nq;
+            if (have) cur = load_node(tile.nodeq[lane]);
+            int buf = 0;
+            for (int base = 0; base < nq; base += 32) {
+                store_node(buf, lane, cur, have);
+                __syncwarp();
+                have = base + 32 + lane < nq;
+                if (have) cur = load_node(tile.nodeq[base + 32 + lane]);
+                node_interact(buf, min(32, nq - base));
+                buf ^= 1;
+            }
+            __syncwarp();
+        };
+
+        // ---- opened leaves: particle-particle terms
+        auto load_part = [&](int j) {
+            PartF en;
+            const float3 p = rel_to(A.pk_pos[j], ref, cl.s10);
+            const float4 hm = A.pk_hme[j];
+            en.x = p.x;
+            en.y = p.y;
+            en.z = p.z;
+            en.m = hm.y;
+            en.e = hm.z;
+            return en;
+        };
+        auto store_part = [&](int buf, int s, const PartF &e, bool have) {
+            const int p = s >> 1, h = s & 1;
+            put2(tile.pa[buf][p], h, have ? e.x : kPadFar, have ? e.y : kPadFar);
+            put2(tile.pb[buf][p], h, have ? e.z : kPadFar, have ? e.m : 0.f);
+            reinterpret_cast<float *>(&tile.pe[buf][p])[h] = have ? e.e : 1.f;
+        };
+        auto part_interact = [&](int buf, int ne) {
+            if (lead) n_part += ne;
+            const int np = (ne + 1) >> 1;
+            for (int pb = 0; pb < np; pb += split) {
+                const int p = pb + cp;
+                const float4 a4 = tile.pa[buf][p], b4 = tile.pb[buf][p];
+                const float2 e2 = tile.pe[buf][p];
+                const float2 dx = __fadd2_rn(lo2(a4), ntx), dy = __fadd2_rn(hi2(a4), nty),
+                             dz = __fadd2_rn(lo2(b4), ntz);
+                const float2 m = hi2(b4);
+                float2 r2 = __fmul2_rn(dx, dx);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                const float2 r = __fmul2_rn(r2, rinv);
+                const float2 eij = __ffma2_rn(e2, f2(0.5f), hte);
+                float2 fk = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
+                float2 pk = rinv;
+                // NaN-safe: r2 = 0 gives r = NaN, which lands in the near branch
+                const bool near = active && (!(r.x >= 2.f * eij.x) || !(r.y >= 2.f * eij.y));
+                if (__any_sync(kFull, near)) {
+                    spline_near(r2.x, r.x, eij.x, fk.x, pk.x);
+                    spline_near(r2.y, r.y, eij.y, fk.y, pk.y);
+                }
+                const float2 mf = __fmul2_rn(m, fk);
+                ax = __ffma2_rn(mf, dx, ax);
+                ay = __ffma2_rn(mf, dy, ay);
+                az = __ffma2_rn(mf, dz, az);
+                pp = __ffma2_rn(m, pk, pp);
+            }
+        };
+        auto flush_leaves_fn = [&](int nl) {
+            flush_leaves_st<PartF>(A.range, wm.leafq, nl, wm.lfirst, wm.lpre, load_part, store_part,
+                                   part_interact);
+        };
+        unsigned long long visits = 0;
+        const int guard = grav_walk(A, wm, tile.nodeq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn, visits);
+        if (lane == 0) {  // walk statistics
+            atomicAdd(&A.counters[kCntVisitsGravity], visits);
+            atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
+        }
+        float fx = ax.x + ax.y, fy = ay.x + ay.y, fz = az.x + az.y, P = pp.x + pp.y;
+        for (int off = gw; off < 32; off <<= 1) {
+            fx += __shfl_xor_sync(kFull, fx, off);
+            fy += __shfl_xor_sync(kFull, fy, off);
+            fz += __shfl_xor_sync(kFull, fz, off);
+            P += __shfl_xor_sync(kFull, P, off);
+        }
+        if (lead) {
+            A.acc_g[i] = A.G * (double)fx;
+            A.acc_g[A.n + i] = A.G * (double)fy;
+            A.acc_g[2 * A.n + i] = A.G * (double)fz;
+            A.phi[i] = -A.G * (double)P;
+        }
+    }
+    n_node = warp_sum(n_node);
+    n_part = warp_sum(n_part);
+    if (lane == 0) {
+        atomicAdd(&A.counters[0], n_node);
+        atomicAdd(&A.counters[1], n_part);
+        atomicAdd(&A.counters[kCntGravGroups], n_grp);
     }
 }
 
@@ -327,12 +572,19 @@ static void allow_smem_g(const void *kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-template <typename R, bool QUAD>
+template <bool QUAD>
 static void launch_grav_t(const GArgs &A, State &S, const Params &P, cudaStream_t st) {
-    const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<R>)) * P.walk_warps;
-    allow_smem_g((const void *)k_gravity<R, QUAD>);
     // persistent grid: 32 warps' worth of blocks per SM
-    k_gravity<R, QUAD><<<S.num_sms * (32 / P.walk_warps), P.walk_warps * 32, sm, st>>>(A);
+    const int blocks = S.num_sms * (32 / P.walk_warps), threads = P.walk_warps * 32;
+    if (P.precision == SPH3_PREC_FP64) {
+        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<double>)) * P.walk_warps;
+        allow_smem_g((const void *)k_gravity_f64<QUAD>);
+        k_gravity_f64<QUAD><<<blocks, threads, sm, st>>>(A);
+    } else {
+        const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTileF)) * P.walk_warps;
+        allow_smem_g((const void *)k_gravity_f32<QUAD>);
+        k_gravity_f32<QUAD><<<blocks, threads, sm, st>>>(A);
+    }
 }
 
 void launch_gravity(State &S, const Params &P, cudaStream_t st) {
@@ -368,13 +620,8 @@ void launch_gravity(State &S, const Params &P, cudaStream_t st) {
     A.status = S.status;
     A.counters = S.counters;
     cudaMemsetAsync(A.work, 0, sizeof(int), st);
-    if (P.precision == SPH3_PREC_FP64) {
-        if (P.quadrupole) launch_grav_t<double, true>(A, S, P, st);
-        else launch_grav_t<double, false>(A, S, P, st);
-    } else {
-        if (P.quadrupole) launch_grav_t<float, true>(A, S, P, st);
-        else launch_grav_t<float, false>(A, S, P, st);
-    }
+    if (P.quadrupole) launch_grav_t<true>(A, S, P, st);
+    else launch_grav_t<false>(A, S, P, st);
 }
 
 // ------------------------------------------------------------ FP64 direct sum
