@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--leaf", type=int, default=0)
+    p.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                   help="override a Config field of the timed context (repeatable), e.g. --set stack_cap=1024")
     return p.parse_args()
 
 
@@ -170,6 +172,10 @@ def run_ours(args, rank, world, local_rank):
         cfg = Config(precision=prec, timing=timing)
         if args.leaf:
             cfg = cfg.replace(leaf_size=args.leaf)
+        for kv in args.set:
+            k, v = kv.split("=", 1)
+            cur = getattr(cfg, k)
+            cfg = cfg.replace(**{k: type(cur)(v) if not isinstance(cur, bool) else v.lower() in ("1", "true")})
         ctx = Context(cfg, device=local_rank)
         ctx.set_particles(ic["pos"], ic["m"], vel=ic["vel"], u=ic["u"], eps=eps)
         ctx.first_step(DT)
@@ -206,6 +212,7 @@ def run_ours(args, rank, world, local_rank):
     clocks.start()
     ms = timed(ctx, args.steps, args.warmup)
     ck = clocks.stop()
+    kernels_per_step = ctx.kernels_per_step()
     e_end = ctx.energy()
     status = ctx.status_names()
     ctx.counters(clear=True)
@@ -332,7 +339,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": "Evrard collapse N=%d, N_ngb=64, theta=0.5, eps=0.01, dt=1e-3, one full "
                                "KDK step per update" % n, "n_per_gpu": n, "parallelism": "replicas",
                    "l2": "working set ~0.5 GB per GPU > 126 MB L2 (no flush needed)",
-                   "cuda_graph": True},
+                   "cuda_graph": True, "overrides": list(args.set)},
         "fp64": fp64,
         "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
         "energy_drift_timed_region": drift,
@@ -342,7 +349,8 @@ def run_ours(args, rank, world, local_rank):
         "kernels": kernels,
         "counters_per_step": cnt,
         "clocks": ck,
-        "gpu_launches": None,
+        "gpu_launches": kernels_per_step * args.steps if kernels_per_step > 0 else None,
+        "gpu_launches_per_step": kernels_per_step,
         "cpu_baseline": cpu,
     }
     return line

@@ -137,7 +137,7 @@ typedef struct sph3_config {
     int32_t h_max_iter;  /* cap on h iterations (SPH3_STATUS_H_NOT_CONVERGED past it) */
     int32_t n_boot;      /* k of the bootstrap h (reference: 50, 0-based sorted index) */
     int32_t leaf_size;   /* octree leaf capacity (1..64) */
-    int32_t stack_cap;   /* walk-stack entries per warp (default 2048; >= 7 (max_level + 2) + 32, <= 4096).
+    int32_t stack_cap;   /* walk-stack entries per warp (default 1024; >= 7 (max_level + 2) + 32, <= 4096).
                           * Wide pops need room: once the stack nears its capacity the walk pops one
                           * node per iteration, which is exact but slow. */
     int32_t max_level;   /* octree levels (3 key bits each), 4..21 */
@@ -254,6 +254,12 @@ int sph3_counters(sph3_ctx *ctx, int64_t out[16], int clear);
  * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,
  * [5] density, [6] gravity, [7] hydro, [8] kick+u+energy.  Clears if `clear`. */
 int sph3_phase_times(sph3_ctx *ctx, double out[9], int clear);
+
+/* Kernel launches one sph3_step makes once its CUDA graph is captured (the
+ * kernel nodes of the graph; memsets are not counted), or -1 before the
+ * first graph capture.  No reference counterpart: it backs the launch count
+ * that benchmarks report. */
+int sph3_kernels_per_step(sph3_ctx *ctx, int64_t *out);
 
 /* Morton sort that allocates no device memory -- it has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc: code running inside a

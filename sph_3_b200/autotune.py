@@ -27,7 +27,7 @@ from typing import Dict, Iterable, Optional, Tuple
 DEFAULT_GRID = {
     "leaf_size": (8, 12, 16, 24, 32),
     "walk_warps": (2, 4, 8),
-    "stack_cap": (256, 512),
+    "stack_cap": (768, 1024, 2048),
 }
 
 

@@ -45,7 +45,7 @@ class Config:
     h_max_iter: int = 64
     n_boot: int = 50
     leaf_size: int = 16
-    stack_cap: int = 2048
+    stack_cap: int = 1024
     max_level: int = 16
     gravity: bool = True
     quadrupole: bool = True
@@ -238,6 +238,12 @@ class Context:
                 "tree_nodes", "tree_leaves", "visits_h", "visits_density", "visits_hydro", "visits_gravity",
                 "walk_max_iter", "walk_max_where", "grav_groups"]
         return dict(zip(keys, out.tolist()))
+
+    def kernels_per_step(self):
+        """Kernel launches per step of the captured step graph (-1 before capture)."""
+        v = ctypes.c_int64()
+        check(self.lib.sph3_kernels_per_step(self._ptr, ctypes.byref(v)), "kernels_per_step")
+        return int(v.value)
 
     def phase_times(self, clear=False):
         out = np.zeros(9)

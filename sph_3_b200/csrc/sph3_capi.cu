@@ -47,6 +47,7 @@ struct sph3_ctx {
     // graphs (one per carried-block parity)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt[2] = {0, 0};
+    int64_t graph_kernels[2] = {0, 0};  // kernel nodes of each captured step graph
     int warm_steps = 0;
     // timing
     cudaEvent_t ev[12] = {};
@@ -56,6 +57,20 @@ struct sph3_ctx {
 namespace {
 
 int cuda_err(cudaError_t e) { return e == cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA; }
+
+// number of kernel launches recorded in a captured graph
+int64_t count_kernel_nodes(cudaGraph_t g) {
+    size_t nn = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess || nn == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (cudaGraphGetNodes(g, nodes.data(), &nn) != cudaSuccess) return 0;
+    int64_t k = 0;
+    for (size_t i = 0; i < nn; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
 
 #define CK(x)                                            \
     do {                                                 \
@@ -536,7 +551,7 @@ void sph3_default_config(sph3_config *cfg) {
     cfg->h_max_iter = 64;
     cfg->n_boot = 50;
     cfg->leaf_size = 16;
-    cfg->stack_cap = 2048;
+    cfg->stack_cap = 1024;
     cfg->max_level = 16;
     cfg->gravity = 1;
     cfg->quadrupole = 1;
@@ -955,6 +970,7 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
             enqueue_step(c, dt, st);
             cudaError_t e = cudaStreamEndCapture(st, &g);
             if (e != cudaSuccess) return SPH3_ERR_CUDA;
+            c->graph_kernels[pq] = count_kernel_nodes(g);
             e = cudaGraphInstantiate(&c->graph[pq], g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return SPH3_ERR_CUDA;
@@ -968,6 +984,13 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
         point_carried(c);
         c->inv_valid = false;
     }
+    return SPH3_OK;
+}
+
+int sph3_kernels_per_step(sph3_ctx *c, int64_t *out) {
+    if (!c || !out) return SPH3_ERR_INVALID_ARG;
+    const int64_t k = c->graph_kernels[c->cur];
+    *out = k > 0 ? k : -1;
     return SPH3_OK;
 }
 
