@@ -147,6 +147,11 @@ def cpu_baseline(ic, target_s=12.0):
 
 
 # ------------------------------------------------------------ GPU arm
+# DRAM bytes per particle of one gravity launch, from the ncu capture
+# summarised in profiles/k_gravity_f32_evrard262k.md (12.62 MB at N=262144)
+GRAV_DRAM_BYTES_PER_PARTICLE = 12.62e6 / 262144
+
+
 def make_ic(n, seed):
     from sph_3_b200.ic import evrard
     return evrard(n, seed=seed)
@@ -298,8 +303,12 @@ def run_ours(args, rank, world, local_rank):
     dom = max(ph, key=lambda k: ph[k])
     if dom == "gravity":
         ach = g_flops / (ph["gravity"] / 1e3) / 1e12
-        roof = {"kernel": "k_gravity<float>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": None,
+        roof = {"kernel": "k_gravity_f32<QUAD>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                "traffic": GRAV_DRAM_BYTES_PER_PARTICLE * n,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=262144 launch "
+                                  "(12.62 MB), scaled per particle to this N "
+                                  "(profiles/k_gravity_f32_evrard262k.md)",
                 "peak_source": "nominal FP32 issue rate 148 SM x 128 lanes x 2 at the sampled median SM "
                                "clock (%.0f MHz); MEASURED_PEAKS.json has no CUDA-core FP32 figure" % sm_mhz,
                 "work": "%.3g node + %.3g particle interactions per launch" % (cnt.get("grav_node", 0),

@@ -59,17 +59,20 @@ __global__ void __launch_bounds__(256) k_box_partial(const int4 *items, const do
 __global__ void k_cloud_boxes(Cloud *clouds, const int *item_begin, const double *part, int max_level,
                               int periodic, double Lx, double Ly, double Lz) {
     Cloud &cl = clouds[blockIdx.x];
-    if (threadIdx.x == 0) {
-        double lo[3], hi[3];
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = DBL_MAX;
-            hi[d] = -DBL_MAX;
-            for (int it = item_begin[blockIdx.x]; it < item_begin[blockIdx.x + 1]; ++it) {
-                lo[d] = fmin(lo[d], part[it * 6 + d]);
-                hi[d] = fmax(hi[d], part[it * 6 + 3 + d]);
-            }
-            if (lo[d] > hi[d]) lo[d] = hi[d] = 0.0;  // empty cloud
+    // one warp: lanes stride over the cloud's items, then a warp reduction
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = DBL_MAX;
+        hi[d] = -DBL_MAX;
+        for (int it = item_begin[blockIdx.x] + (int)threadIdx.x; it < item_begin[blockIdx.x + 1]; it += 32) {
+            lo[d] = fmin(lo[d], part[it * 6 + d]);
+            hi[d] = fmax(hi[d], part[it * 6 + 3 + d]);
         }
+        lo[d] = warp_min(lo[d]);
+        hi[d] = warp_max(hi[d]);
+        if (lo[d] > hi[d]) lo[d] = hi[d] = 0.0;  // empty cloud
+    }
+    if (threadIdx.x == 0) {
         double size;
         double org[3];
         if (periodic) {
