@@ -89,6 +89,9 @@ extern "C" {
 #define SPH3_VISC_MG83 1    /* getAcc_sph_mpiXXX / get_dU_mpiXXXX (libsx.py:236-246) */
 #define SPH3_VISC_BALSARA 2 /* getAcc_sph_shear / get_dU_shear (shear.py:193-215) */
 
+#define SPH3_MAC_BH 0        /* Barnes-Hut: accept a node when d(com, group box) > s / theta */
+#define SPH3_MAC_BH_OFFSET 1 /* ... when d > s / theta + the offset of the com from the node's box centre */
+
 #define SPH3_ORDER_SERIAL 0 /* du/dt with the half-step v, before the 2nd kick (sph_serial.py) */
 #define SPH3_ORDER_MPI4 1   /* du/dt with the full-step v, after the 2nd kick (sph_mpi4_v4.py) */
 
@@ -146,7 +149,14 @@ typedef struct sph3_config {
     int32_t use_graph;   /* 1: sph3_step replays a captured CUDA graph */
     int32_t timing;      /* 1: record per-phase CUDA events (no graph) */
     int32_t walk_warps;  /* warps per walk block: 1, 2, 4 (default) or 8; each warp walks one group of <= 32 particles */
-    int32_t reserved_i[4];
+    int32_t list_cap;    /* mixed precision: neighbour-list slots per particle that the density walk keeps
+                          * for the hydro pass (default 128; 0 = the hydro pass walks the tree).  The lists
+                          * hold exactly the pairs inside the support (|r| <= h_i + h_j); a particle with
+                          * more neighbours than list_cap is handled by a walk.  4 * list_cap bytes per
+                          * particle; a multiple of 8 in 0..1024. */
+    int32_t mac;         /* multipole acceptance: SPH3_MAC_BH (d > s/theta, the default) or
+                          * SPH3_MAC_BH_OFFSET (d > s/theta + |com - box centre|, more conservative) */
+    int32_t reserved_i[2];
     double gamma;        /* adiabatic index (5/3) */
     double alpha;        /* artificial viscosity alpha (1) */
     double beta;         /* beta of the MG83 form (2) */

@@ -11,7 +11,8 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libsph3.so")
+# SPH3_LIB selects another build of the library (e.g. side-by-side variants)
+LIB_PATH = os.environ.get("SPH3_LIB") or os.path.join(HERE, "lib", "libsph3.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "sph3.h")
 
 
@@ -57,7 +58,9 @@ class Config(ctypes.Structure):
         ("use_graph", ctypes.c_int32),
         ("timing", ctypes.c_int32),
         ("walk_warps", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 4),
+        ("list_cap", ctypes.c_int32),
+        ("mac", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 2),
         ("gamma", ctypes.c_double),
         ("alpha", ctypes.c_double),
         ("beta", ctypes.c_double),

@@ -31,6 +31,7 @@ _PREC = {"mixed": C["SPH3_PREC_MIXED"], "fp64": C["SPH3_PREC_FP64"]}
 _HMODE = {"newton": C["SPH3_H_NEWTON"], "refstep": C["SPH3_H_REFSTEP"]}
 _VISC = {"signal": C["SPH3_VISC_SIGNAL"], "mg83": C["SPH3_VISC_MG83"], "balsara": C["SPH3_VISC_BALSARA"]}
 _ORDER = {"serial": C["SPH3_ORDER_SERIAL"], "mpi4": C["SPH3_ORDER_MPI4"]}
+_MAC = {"bh": C["SPH3_MAC_BH"], "bh_offset": C["SPH3_MAC_BH_OFFSET"]}
 
 
 @dataclass
@@ -52,6 +53,8 @@ class Config:
     use_graph: bool = True
     timing: bool = False
     walk_warps: int = 4            # warps per walk block (1, 2, 4, 8)
+    list_cap: int = 128            # mixed: neighbour-list slots per particle for the hydro pass (0: walk)
+    mac: str = "bh"                # multipole acceptance: "bh" (d > s/theta) | "bh_offset" (+ com offset)
     gamma: float = 5.0 / 3.0
     alpha: float = 1.0
     beta: float = 2.0
@@ -67,8 +70,9 @@ class Config:
         c.h_mode = _HMODE[self.h_mode]
         c.visc = _VISC[self.visc]
         c.step_order = _ORDER[self.step_order]
+        c.mac = _MAC[self.mac]
         for name in ("n_ngb", "n_ngb_tol", "h_max_iter", "n_boot", "leaf_size", "stack_cap", "max_level",
-                     "walk_warps"):
+                     "walk_warps", "list_cap"):
             setattr(c, name, int(getattr(self, name)))
         for name in ("gravity", "quadrupole", "use_graph", "timing"):
             setattr(c, name, 1 if getattr(self, name) else 0)

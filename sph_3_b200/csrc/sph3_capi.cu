@@ -130,6 +130,8 @@ void params_from(const sph3_config &cfg, Params &P) {
     P.gravity = cfg.gravity;
     P.quadrupole = cfg.quadrupole;
     P.walk_warps = cfg.walk_warps;
+    P.list_cap = cfg.precision == SPH3_PREC_MIXED ? cfg.list_cap : 0;
+    P.mac = cfg.mac;
     P.gamma = cfg.gamma;
     P.alpha = cfg.alpha;
     P.beta = cfg.beta;
@@ -156,6 +158,8 @@ int validate(const sph3_config *c) {
     if (c->walk_warps != 1 && c->walk_warps != 2 && c->walk_warps != 4 && c->walk_warps != 8)
         return SPH3_ERR_INVALID_ARG;
     if (c->max_level < 4 || c->max_level > 21) return SPH3_ERR_INVALID_ARG;
+    if (c->list_cap < 0 || c->list_cap > 1024 || c->list_cap % 8) return SPH3_ERR_INVALID_ARG;
+    if (c->mac != SPH3_MAC_BH && c->mac != SPH3_MAC_BH_OFFSET) return SPH3_ERR_INVALID_ARG;
     if (c->stack_cap < 7 * (c->max_level + 2) + 32 || c->stack_cap > 4096) return SPH3_ERR_INVALID_ARG;
     if (!(c->theta >= 0.0) || !(c->eps > 0.0) || !(c->gamma >= 1.0)) return SPH3_ERR_INVALID_ARG;
     for (int d = 0; d < 3; ++d)
@@ -171,7 +175,7 @@ void free_buffers(sph3_ctx *c) {
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.tree.bounds, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.tree.scan_tmp, S.tree.bounds, S.list, S.nlist, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
                     S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -184,6 +188,9 @@ void free_buffers(sph3_ctx *c) {
     S.perm = S.perm_alt = nullptr;
     S.pk_pos = S.pk_hme = S.pk_vel = S.pk_thm = nullptr;
     S.sort_hist = nullptr;
+    S.list = S.nlist = nullptr;
+    S.list_cap = 0;
+    S.list_valid = false;
     S.tree = Tree{};
     S.groups = nullptr;
     S.group_cloud = nullptr;
@@ -208,6 +215,24 @@ void drop_graphs(sph3_ctx *c) {
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
     return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+}
+
+// neighbour lists of the mixed path: list_cap slots per particle (particle-major,
+// slot k of particle i at i * list_cap + k) and the count per particle
+int ensure_lists(sph3_ctx *c, int64_t nn) {
+    State &S = c->S;
+    const int want = c->P.list_cap;
+    S.list_valid = false;
+    if (want == S.list_cap && (want == 0 || S.list)) return SPH3_OK;
+    if (S.list) cudaFree(S.list);
+    if (S.nlist) cudaFree(S.nlist);
+    S.list = S.nlist = nullptr;
+    S.list_cap = 0;
+    if (want == 0) return SPH3_OK;
+    CK(dalloc(&S.list, (size_t)want * nn));
+    CK(dalloc(&S.nlist, nn));
+    S.list_cap = want;
+    return SPH3_OK;
 }
 
 int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
@@ -277,7 +302,7 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     c->cur = 0;
     point_carried(c);
     point_fixed(c);
-    return SPH3_OK;
+    return ensure_lists(c, nn);
 }
 
 cudaStream_t pick(sph3_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
@@ -556,6 +581,8 @@ void sph3_default_config(sph3_config *cfg) {
     cfg->gravity = 1;
     cfg->quadrupole = 1;
     cfg->walk_warps = 4;
+    cfg->list_cap = 128;
+    cfg->mac = SPH3_MAC_BH;
     cfg->use_graph = 1;
     cfg->timing = 0;
     cfg->gamma = 5.0 / 3.0;
@@ -656,7 +683,8 @@ int sph3_set_config(sph3_ctx *c, const sph3_config *cfg) {
     int rc = validate(cfg);
     if (rc) return rc;
     const bool relevel = cfg->max_level != c->cfg.max_level || cfg->leaf_size != c->cfg.leaf_size ||
-                         cfg->theta != c->cfg.theta || cfg->quadrupole != c->cfg.quadrupole;
+                         cfg->theta != c->cfg.theta || cfg->quadrupole != c->cfg.quadrupole ||
+                         cfg->mac != c->cfg.mac;
     if (cfg->max_level != c->cfg.max_level && c->have) {
         int cb = 0;
         while ((1ll << cb) < (int64_t)c->S.ncloud) ++cb;
@@ -666,6 +694,11 @@ int sph3_set_config(sph3_ctx *c, const sph3_config *cfg) {
     params_from(*cfg, c->P);
     c->S.walk_warps = cfg->walk_warps;
     drop_graphs(c);
+    if (c->cap_n > 0) {
+        cudaSetDevice(c->device);
+        rc = ensure_lists(c, std::max<int64_t>(c->cap_n, 1));
+        if (rc) return rc;
+    }
     if (relevel && c->have) {
         cudaSetDevice(c->device);
         c->S.max_level = cfg->max_level;
@@ -809,11 +842,17 @@ int sph3_set_field(sph3_ctx *c, int field, const double *src, int on_device, voi
             // re-sorted lazily: by the next pass that needs the tree, or by
             // the next step, which sorts anyway
             c->order_dirty = true;
+            c->S.list_valid = false;
             break;
         case SPH3_FIELD_VEL: c->pack_dirty |= kPackVel; break;
         case SPH3_FIELD_MASS:
         case SPH3_FIELD_EPS: c->pack_dirty |= kPackHme; c->tree_dirty = true; break;
-        case SPH3_FIELD_H: c->pack_dirty |= kPackHme; c->h_dirty_tree = true; c->bal_dirty = true; break;
+        case SPH3_FIELD_H:
+            c->pack_dirty |= kPackHme;
+            c->h_dirty_tree = true;
+            c->bal_dirty = true;
+            c->S.list_valid = false;
+            break;
         case SPH3_FIELD_RHO:
         case SPH3_FIELD_P: c->pack_dirty |= kPackThm; break;
         case SPH3_FIELD_C:

@@ -136,12 +136,19 @@ struct State {
     int num_sms = 0;
     int walk_blocks = 0;
     int walk_warps = 4;  // warps per walk block (the config's walk_warps)
+    // neighbour lists kept by the mixed density walk for the hydro pass
+    int *list = nullptr;   // [n][list_cap], slot k of particle i at i * list_cap + k
+    int *nlist = nullptr;  // [n] neighbours found (may exceed list_cap: then the hydro pass walks)
+    int list_cap = 0;
+    bool list_valid = false;  // host flag: lists match the current order, positions and h
 };
 
 struct Params {
     int precision, h_mode, visc, step_order, n_ngb, n_ngb_tol, h_max_iter, n_boot;
     int leaf_size, stack_cap, max_level, gravity, quadrupole;
     int walk_warps;  // warps per walk block (1, 2, 4 or 8)
+    int list_cap;    // neighbour-list slots (0: the hydro pass walks)
+    int mac;         // SPH3_MAC_*
     double gamma, alpha, beta, eta, G, theta, eps;
     double box[3];
     int periodic;

@@ -182,6 +182,7 @@ struct MomArgs {
     const uint64_t *key;
     int max_level;
     double inv_theta;  // 1/theta (inf for theta = 0)
+    int mac_offset;    // add the com offset to the opening radius
 };
 
 __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
@@ -289,9 +290,12 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         const double bmax = sqrt(ex * ex + ey * ey + ez * ez);
         const double side = 2.0 * fmax(hx, fmax(hy, hz));
         const double delta = sqrt((cx - bcx) * (cx - bcx) + (cy - bcy) * (cy - bcy) + (cz - bcz) * (cz - bcz));
-        // s/d < theta with the offset of the centre of mass (d > s/theta + delta);
-        // theta = 0 never accepts a node (exact sum)
-        double r_open = isinf(a.inv_theta) ? (double)FLT_MAX : side * a.inv_theta + delta;
+        // s/d < theta (d > s/theta), optionally plus the offset of the centre of
+        // mass from the box centre (d > s/theta + delta); theta = 0 never
+        // accepts a node (exact sum).  The walks also require d > r_soft
+        // (bmax + eps), so an accepted node's particles always lie outside the
+        // group's box, whatever theta.
+        double r_open = isinf(a.inv_theta) ? (double)FLT_MAX : side * a.inv_theta + (a.mac_offset ? delta : 0.0);
         r_open = fmin(r_open * (1.0 + 1e-5) + pad, (double)FLT_MAX);
         const double r_soft = fmin((bmax + em) * (1.0 + 1e-5) + pad, (double)FLT_MAX);
         T.mono[i] = make_float4((float)M, (float)r_open, (float)r_soft, 0.f);
@@ -462,6 +466,7 @@ void launch_groups(State &S, cudaStream_t st) {
 }
 
 void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
+    S.list_valid = false;  // a new order invalidates the neighbour lists
     if (S.ncloud == 0) return;
     Tree &T = S.tree;
     const int maxd = S.max_level + 1;  // depths 0..max_level
@@ -476,6 +481,7 @@ void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
     a.pos = S.pos; a.m = S.m; a.h = S.h; a.eps = S.eps; a.n = S.n;
     a.clouds = S.clouds; a.key = S.key; a.max_level = S.max_level;
     a.inv_theta = P.theta > 0 ? 1.0 / P.theta : __builtin_inf();
+    a.mac_offset = P.mac == SPH3_MAC_BH_OFFSET;
     for (int d = maxd; d >= 0; --d) k_tree_moments<<<blocks, 128, 0, st>>>(T, a, d, P.quadrupole);
     k_tree_totals<<<blocks, 256, 0, st>>>(T, maxd + 1, S.counters);
     launch_groups(S, st);

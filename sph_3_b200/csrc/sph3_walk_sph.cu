@@ -507,20 +507,43 @@ struct DArgs {
     float4 *pk_thm;
     double gamma;
     int keep_rho;
+    // neighbour lists for the hydro pass (null: none kept)
+    int *list, *nlist;
+    int list_cap;
 };
 
-// tile entry: p = {x, y, z, h}, q = {m, vx, vy, vz}
-template <typename R>
+// tile entry: p = {x, y, z, h}, q = {m, vx, vy, vz}, and the sorted source
+// index j for the neighbour lists: in the unused q.y without div/curl (no
+// velocities staged), in a field of its own with them
+template <typename R, bool DC>
 struct DE {
     V4<R> p, q;
+    int j;
+    __device__ void set_j(int v) { j = v; }
+    __device__ int get_j() const { return j; }
 };
+
+template <typename R>
+struct DE<R, false> {
+    V4<R> p, q;
+    __device__ void set_j(int v) { q.y = sizeof(R) == 4 ? (R)__int_as_float(v) : (R)v; }
+    __device__ int get_j() const { return sizeof(R) == 4 ? __float_as_int((float)q.y) : (int)q.y; }
+};
+
+// Neighbour lists are written particle-major (row i holds list_cap slots,
+// list_cap a multiple of 8): each lane stages its pairs in shared memory and
+// writes them 8 at a time (two 16-byte stores, one full 32-byte sector).
+constexpr int kListChunk = 8;
+constexpr size_t kListStageBytes = sizeof(int) * kListChunk * 32;
 
 template <typename R, bool DC>
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
-    using E = DE<R>;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
+    using E = DE<R, DC>;
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64 + kListStageBytes);
+    // neighbour-list staging: slot x of lane l at stage[x * 32 + l] (conflict-free)
+    int *stage = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(wm.tile) + sizeof(E) * 64);
     E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     unsigned long long pairs = 0;
@@ -540,6 +563,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
         }
         const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
         R rho = 0, sdiv = 0, cx = 0, cy = 0, cz = 0;
+        int nkept = 0;  // in-support pairs found (kept in the list while < list_cap)
         const Images ims = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic);
         for (int im = 0; im < 27; ++im) {
             float3 s;
@@ -559,6 +583,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
                     if (DC) { const float4 v = A.pk_vel[j]; en.q.y = (R)v.x; en.q.z = (R)v.y; en.q.w = (R)v.z; }
                     f = make_float3((float)en.p.x, (float)en.p.y, (float)en.p.z);
                 }
+                en.set_j(j);
                 keep = reaches(gb, f, hmax_g + (float)en.p.w);
                 return en;
             };
@@ -590,6 +615,20 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
                     const int e = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const E en = t[e];
+                    if (A.list) {  // keep the pair for the hydro pass
+                        if (nkept < A.list_cap) {
+                            const int x = nkept & (kListChunk - 1);
+                            stage[x * 32 + lane] = en.get_j();
+                            if (x == kListChunk - 1) {
+                                int4 *dst = reinterpret_cast<int4 *>(A.list + (size_t)gi.i * A.list_cap +
+                                                                     (nkept - x));
+                                dst[0] = make_int4(stage[lane], stage[32 + lane], stage[64 + lane], stage[96 + lane]);
+                                dst[1] = make_int4(stage[128 + lane], stage[160 + lane], stage[192 + lane],
+                                                   stage[224 + lane]);
+                            }
+                        }
+                        ++nkept;
+                    }
                     if (sizeof(R) == 8) {
                         // reference order: dx = x_i - x_j, q = |r| / hbar
                         const double dx = __dsub_rn((double)tx, (double)en.p.x);
@@ -660,6 +699,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
         }
         if (gi.active) {
             const int i = gi.i;
+            if (A.list) {
+                A.nlist[i] = nkept;
+                const int kept = min(nkept, A.list_cap);
+                const int base = kept & ~(kListChunk - 1);
+                for (int x = 0; x < kept - base; ++x) A.list[(size_t)i * A.list_cap + base + x] = stage[x * 32 + lane];
+            }
             double r, P, c;
             if (A.keep_rho) {  // div/curl only: divide by the caller's rho
                 r = A.rho[i];
@@ -700,6 +745,10 @@ struct YArgs {
     const double *h, *m, *vel, *rho, *P, *c, *bal;
     double *acc_sph, *dudt;
     double alpha, beta, eta;
+    // only_overflow: walk only for particles whose neighbour list overflowed
+    const int *nlist;
+    int list_cap;
+    int only_overflow;
 };
 
 // tile entry: p = {x, y, z, h}, v = {vx, vy, vz, m}, t = {rho, P/rho^2, c, f}
@@ -720,6 +769,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
     const R alpha = (R)A.alpha, beta = (R)A.beta, eta2 = (R)(A.eta * A.eta);
     for (int g = next_group(a.work, a.status); g < *a.ngroups_dev; g = next_group(a.work, a.status)) {
         GroupInfo gi = group_info(a, g);
+        const bool mine = !A.only_overflow || (gi.active && A.nlist[gi.i] > A.list_cap);
+        if (A.only_overflow && !__any_sync(kFull, mine)) continue;
         GroupBox gb = group_box(gi.prel, gi.active, gi.ref, gi.s10);
         gb.first = gi.first;
         const int i = gi.i;
@@ -855,7 +906,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
-        if (gi.active) {
+        if (gi.active && mine) {
             if (ACC) {
                 A.acc_sph[i] = (double)ax;
                 A.acc_sph[a.n + i] = (double)ay;
@@ -866,6 +917,114 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
     }
     pairs = warp_sum(pairs);
     if (lane == 0) atomicAdd(&a.counters[3], pairs);
+}
+
+// ============================================================ hydro over lists
+// Mixed path: the hydro pass over the neighbour lists kept by the density
+// walk, one thread per particle.  The lists hold exactly the in-support pairs
+// (|r| <= h_i + h_j in FP32, the same test as the walks' first pass) in the
+// order the density walk met them, so this is the walk's pair loop without
+// the walk: no tree traversal, no candidate tests.  Pair terms are the
+// reference's (sph_code/libsx.py:117-165 acceleration, :364-417 du/dt; MG83
+// :236-246; Balsara sph_code/shear.py:193-215) in FP32 on positions relative
+// to the target's level-10 cell.  Periodic boxes use the minimum image (a
+// unique image within the support: 2h < L/2 is checked by the h search).
+// Particles whose list overflowed are skipped here and walked instead.
+struct LArgs {
+    const int *list, *nlist;
+    int list_cap;
+    const float4 *pk_pos, *pk_hme, *pk_vel, *pk_thm;
+    const uint64_t *key;
+    int cloud_shift;
+    const Cloud *clouds;
+    int64_t n;
+    int periodic;
+    float box[3];
+    double *acc_sph, *dudt;
+    float alpha, beta, eta2;
+    unsigned long long *counters;
+};
+
+__device__ __forceinline__ float min_image(float d, float L) {
+    if (L > 0.f) d -= L * rintf(d * (1.0f / L));
+    return d;
+}
+
+template <int VISC, bool ACC, bool DU>
+__global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
+    unsigned long long pairs = 0;
+    const float alpha = A.alpha, beta = A.beta, eta2 = A.eta2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int cnt = A.nlist[i];
+        if (cnt > A.list_cap) continue;  // walked instead
+        const float s10 = A.clouds[(int)(A.key[i] >> A.cloud_shift)].s10;
+        const float4 pi = A.pk_pos[i];
+        const int ref = __float_as_int(pi.w);
+        const float3 t = rel_to(pi, ref, s10);
+        const float th = A.pk_hme[i].x;
+        const float4 tv = A.pk_vel[i];
+        const float4 tt = A.pk_thm[i];  // {rho, P/rho^2, c, f}
+        float ax = 0.f, ay = 0.f, az = 0.f, du = 0.f;
+        const int *row = A.list + (size_t)i * A.list_cap;
+        for (int k = 0; k < cnt; ++k) {
+            const int j = row[k];
+            const float3 p = rel_to(A.pk_pos[j], ref, s10);
+            const float hj = A.pk_hme[j].x, mj = A.pk_hme[j].y;
+            const float4 sv = A.pk_vel[j];
+            const float4 st = A.pk_thm[j];
+            float dx = t.x - p.x, dy = t.y - p.y, dz = t.z - p.z;
+            if (A.periodic) {
+                dx = min_image(dx, A.box[0]);
+                dy = min_image(dy, A.box[1]);
+                dz = min_image(dz, A.box[2]);
+            }
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const float hs = th + hj;
+            const float rr = sqrtf(d2);
+            const float hij = 0.5f * hs;
+            const float q = rr * __fdividef(1.0f, hij);
+            const float ih = __fdividef(1.0f, hij);
+            const float ih5 = ih * ih * ih * ih * ih;
+            float nW;
+            if (q <= 1.f) nW = kSigF * ih5 * (-3.f + 2.25f * q);
+            else {
+                const float tq = 2.f - q;
+                nW = __fdividef((float)(-0.75 * kSig) * ih5 * tq * tq, q + 1e-20f);
+            }
+            const float gx = nW * dx, gy = nW * dy, gz = nW * dz;
+            const float vx = tv.x - sv.x, vy = tv.y - sv.y, vz = tv.z - sv.z;
+            const float vr = vx * dx + vy * dy + vz * dz;
+            const float rhoij = 0.5f * (tt.x + st.x);
+            float PI = 0.f;
+            if (VISC == SPH3_VISC_MG83) {
+                const float cij = 0.5f * (tt.z + st.z);
+                const float mu = __fdividef(hij * vr, rr * rr + hij * hij * eta2);
+                if (vr <= 0.f) PI = __fdividef(-alpha * cij * mu + beta * mu * mu, rhoij);
+            } else {
+                const float w = __fdividef(vr, rr + 1e-5f);
+                const float vsig = tt.z + st.z - 3.f * w;
+                if (vr <= 0.f) PI = __fdividef(-0.5f * alpha * vsig * w, rhoij);
+                if (VISC == SPH3_VISC_BALSARA) PI = 0.5f * (tt.w + st.w) * PI;
+            }
+            if (ACC) {
+                const float pt = mj * (tt.y + st.y + PI);
+                ax -= pt * gx;
+                ay -= pt * gy;
+                az -= pt * gz;
+            }
+            if (DU) du += mj * (tt.y + 0.5f * PI) * (vx * gx + vy * gy + vz * gz);
+        }
+        pairs += (unsigned long long)cnt;
+        if (ACC) {
+            A.acc_sph[i] = (double)ax;
+            A.acc_sph[A.n + i] = (double)ay;
+            A.acc_sph[2 * A.n + i] = (double)az;
+        }
+        if (DU) A.dudt[i] = (double)du;
+    }
+    pairs = warp_sum(pairs);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&A.counters[3], pairs);
 }
 
 // ============================================================ neighbours
@@ -983,6 +1142,12 @@ static size_t walk_smem(const Params &P) {
     return warp_mem_bytes(P.stack_cap, sizeof(E) * 64) * P.walk_warps;
 }
 
+// as walk_smem, with `extra` bytes per warp after the tile
+template <typename E>
+static size_t walk_smem_x(const Params &P, size_t extra) {
+    return warp_mem_bytes(P.stack_cap, sizeof(E) * 64 + extra) * P.walk_warps;
+}
+
 static void allow_smem(const void *kern) {
     static std::mutex mu;
     static std::set<const void *> done;
@@ -1000,6 +1165,7 @@ static void run_walk(void (*kern)(Args), const Args &args, size_t smem, State &S
 }
 
 void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
+    S.list_valid = false;
     if (S.n == 0) return;
     BootArgs A;
     A.w = walk_args(S, P, 0);
@@ -1010,6 +1176,7 @@ void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
 }
 
 void launch_h_search(State &S, const Params &P, cudaStream_t st) {
+    S.list_valid = false;  // new h: the supports change
     if (S.n == 0) return;
     HArgs A;
     A.w = walk_args(S, P, 1);
@@ -1042,12 +1209,16 @@ void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bo
     A.rho = S.rho; A.P = S.P; A.c = S.c; A.divV = S.divV; A.curlV = S.curlV; A.bal = S.bal;
     A.pk_thm = S.pk_thm;
     A.gamma = P.gamma;
+    A.list = S.list_cap > 0 ? S.list : nullptr;
+    A.nlist = S.nlist;
+    A.list_cap = S.list_cap;
+    S.list_valid = A.list != nullptr;
     if (P.precision == SPH3_PREC_FP64) {
-        if (divcurl) run_walk(k_density<double, true>, A, walk_smem<DE<double>>(P), S, st, 2);
-        else run_walk(k_density<double, false>, A, walk_smem<DE<double>>(P), S, st, 2);
+        if (divcurl) run_walk(k_density<double, true>, A, walk_smem_x<DE<double, true>>(P, kListStageBytes), S, st, 2);
+        else run_walk(k_density<double, false>, A, walk_smem_x<DE<double, false>>(P, kListStageBytes), S, st, 2);
     } else {
-        if (divcurl) run_walk(k_density<float, true>, A, walk_smem<DE<float>>(P), S, st, 2);
-        else run_walk(k_density<float, false>, A, walk_smem<DE<float>>(P), S, st, 2);
+        if (divcurl) run_walk(k_density<float, true>, A, walk_smem_x<DE<float, true>>(P, kListStageBytes), S, st, 2);
+        else run_walk(k_density<float, false>, A, walk_smem_x<DE<float, false>>(P, kListStageBytes), S, st, 2);
     }
 }
 
@@ -1059,6 +1230,13 @@ static void hydro_dispatch(const YArgs &A, bool acc, bool du, const Params &P, S
     else run_walk(k_hydro<R, V, false, true>, A, sm, S, st, 3);
 }
 
+template <int V>
+static void list_dispatch(const LArgs &L, bool acc, bool du, int blocks, cudaStream_t st) {
+    if (acc && du) k_hydro_list<V, true, true><<<blocks, 256, 0, st>>>(L);
+    else if (acc) k_hydro_list<V, true, false><<<blocks, 256, 0, st>>>(L);
+    else k_hydro_list<V, false, true><<<blocks, 256, 0, st>>>(L);
+}
+
 void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cudaStream_t st) {
     if (S.n == 0 || (!want_acc && !want_dudt)) return;
     YArgs A;
@@ -1067,6 +1245,27 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
     A.h = S.h; A.m = S.m; A.vel = S.vel; A.rho = S.rho; A.P = S.P; A.c = S.c; A.bal = S.bal;
     A.acc_sph = S.acc_sph; A.dudt = S.dudt;
     A.alpha = P.alpha; A.beta = P.beta; A.eta = P.eta;
+    A.nlist = S.nlist;
+    A.list_cap = S.list_cap;
+    A.only_overflow = 0;
+    if (P.precision != SPH3_PREC_FP64 && S.list_valid) {
+        // the list pass, then a walk for the particles whose lists overflowed
+        LArgs L;
+        L.list = S.list; L.nlist = S.nlist; L.list_cap = S.list_cap;
+        L.pk_pos = S.pk_pos; L.pk_hme = S.pk_hme; L.pk_vel = S.pk_vel; L.pk_thm = S.pk_thm;
+        L.key = S.key; L.cloud_shift = 3 * S.max_level; L.clouds = S.clouds;
+        L.n = S.n;
+        L.periodic = P.periodic;
+        for (int d = 0; d < 3; ++d) L.box[d] = (float)P.box[d];
+        L.acc_sph = S.acc_sph; L.dudt = S.dudt;
+        L.alpha = (float)P.alpha; L.beta = (float)P.beta; L.eta2 = (float)(P.eta * P.eta);
+        L.counters = S.counters;
+        const int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 16);
+        if (P.visc == SPH3_VISC_MG83) list_dispatch<SPH3_VISC_MG83>(L, want_acc, want_dudt, blocks, st);
+        else if (P.visc == SPH3_VISC_BALSARA) list_dispatch<SPH3_VISC_BALSARA>(L, want_acc, want_dudt, blocks, st);
+        else list_dispatch<SPH3_VISC_SIGNAL>(L, want_acc, want_dudt, blocks, st);
+        A.only_overflow = 1;
+    }
     if (P.precision == SPH3_PREC_FP64) {
         if (P.visc == SPH3_VISC_MG83) hydro_dispatch<double, SPH3_VISC_MG83>(A, want_acc, want_dudt, P, S, st);
         else if (P.visc == SPH3_VISC_BALSARA) hydro_dispatch<double, SPH3_VISC_BALSARA>(A, want_acc, want_dudt, P, S, st);
