@@ -301,6 +301,14 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         T.mono[i] = make_float4((float)M, (float)r_open, (float)r_soft, 0.f);
         T.quad4[i] = make_float4((float)Q[0], (float)Q[1], (float)Q[2], (float)Q[3]);
         T.quad1[i] = (float)Q[4];
+        // walk records: everything one node test needs in one contiguous
+        // record, so a walk step is a single round trip to L2
+        const int chy = r.y > 0 ? ch.y : -1;  // -1: empty node, never taken
+        T.gw[2 * i] = T.com_c[i];
+        T.gw[2 * i + 1] = make_float4((float)r_open, (float)r_soft, __int_as_float(ch.x), __int_as_float(chy));
+        T.sw[3 * i] = T.box_c[i];
+        T.sw[3 * i + 1] = T.box_h[i];
+        T.sw[3 * i + 2] = make_float4(__int_as_float(ch.x), __int_as_float(chy), 0.f, 0.f);
     }
 }
 
@@ -330,6 +338,7 @@ __global__ void k_tree_refit_h(Tree T, const double *h, int d) {
         }
         T.hmax[i] = hm;
         T.box_h[i].w = (float)(hm * (1.0 + 1e-6));
+        T.sw[3 * i + 1].w = (float)(hm * (1.0 + 1e-6));
     }
 }
 

@@ -29,6 +29,7 @@ struct GArgs {
     const int2 *child;
     const float4 *com_c;
     const float4 *mono;
+    const float4 *gw;  // walk records
     const float4 *quad4;
     const float *quad1;
     const double *tcom;   // FP64 node com [3][cap]
@@ -135,20 +136,22 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
         top -= p;
         bool take_leaf = false, take_node = false;
         int nch = 0, cf = 0;
-        if (node >= 0 && A.range[node].y > 0) {
-            const float4 mo = A.mono[node];
-            const float3 c = rel_to(A.com_c[node], ref, cl.s10);
-            const float d2 = point_gap2(gb, c);
-            const float rs = mo.z + eps_g;
-            if (d2 > mo.y * mo.y && d2 > rs * rs) {
-                take_node = true;
-            } else {
-                const int2 ch = A.child[node];
-                const int k = ch.y & 255;
-                if (k == 0) take_leaf = true;
-                else {
-                    nch = k;
-                    cf = ch.x;
+        if (node >= 0) {
+            const float4 w0 = A.gw[2 * node], w1 = A.gw[2 * node + 1];  // one record, one round trip
+            const int chy = __float_as_int(w1.w);
+            if (chy >= 0) {
+                const float3 c = rel_to(w0, ref, cl.s10);
+                const float d2 = point_gap2(gb, c);
+                const float rs = w1.y + eps_g;
+                if (d2 > w1.x * w1.x && d2 > rs * rs) {
+                    take_node = true;
+                } else {
+                    const int k = chy & 255;
+                    if (k == 0) take_leaf = true;
+                    else {
+                        nch = k;
+                        cf = __float_as_int(w1.z);
+                    }
                 }
             }
         }
@@ -598,6 +601,7 @@ void launch_gravity(State &S, const Params &P, cudaStream_t st) {
     A.child = S.tree.child;
     A.com_c = S.tree.com_c;
     A.mono = S.tree.mono;
+    A.gw = S.tree.gw;
     A.quad4 = S.tree.quad4;
     A.quad1 = S.tree.quad1;
     A.tcom = S.tree.com;

@@ -39,6 +39,7 @@ struct WalkArgs {
     const int2 *child;
     const float4 *box_c;
     const float4 *box_h;
+    const float4 *sw;  // walk records [node][3]
     const float4 *pk_pos;
     const double *pos;
     int64_t n;
@@ -94,22 +95,22 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
         bool take = false;
         int nch = 0, cf = 0;
         if (node >= 0) {
-            const float4 bc = a.box_c[node];
-            const float4 bh = a.box_h[node];
+            // one record per node: box, half widths + hmax, children (one round trip)
+            const float4 bc = a.sw[3 * node], bh = a.sw[3 * node + 1], w2 = a.sw[3 * node + 2];
+            const int chy = __float_as_int(w2.y);
             float3 c = rel_to(bc, gb.ref, gb.s10);
             c.x += shift.x;
             c.y += shift.y;
             c.z += shift.z;
             const float reach = (Rg + (node_h ? bh.w : 0.f)) * margin;
             const float g2 = box_gap2(gb, c, make_float3(bh.x, bh.y, bh.z));
-            if (g2 <= reach * reach) {
-                const int2 ch = a.child[node];
-                const int k = ch.y & 255;
+            if (chy >= 0 && g2 <= reach * reach) {
+                const int k = chy & 255;
                 if (k == 0) {
-                    take = a.range[node].y > 0;
+                    take = true;
                 } else {
                     nch = k;
-                    cf = ch.x;
+                    cf = __float_as_int(w2.x);
                 }
             }
         }
@@ -1119,6 +1120,7 @@ static WalkArgs walk_args(State &S, const Params &P, int slot) {
     a.child = S.tree.child;
     a.box_c = S.tree.box_c;
     a.box_h = S.tree.box_h;
+    a.sw = S.tree.sw;
     a.pk_pos = S.pk_pos;
     a.pos = S.pos;
     a.n = S.n;
