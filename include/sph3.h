@@ -140,7 +140,7 @@ typedef struct sph3_config {
     int32_t h_max_iter;  /* cap on h iterations (SPH3_STATUS_H_NOT_CONVERGED past it) */
     int32_t n_boot;      /* k of the bootstrap h (reference: 50, 0-based sorted index) */
     int32_t leaf_size;   /* octree leaf capacity (1..64) */
-    int32_t stack_cap;   /* walk-stack entries per warp (default 1024; >= 7 (max_level + 2) + 32, <= 4096).
+    int32_t stack_cap;   /* walk-stack entries per warp (default 768; >= 7 (max_level + 2) + 32, <= 4096).
                           * Wide pops need room: once the stack nears its capacity the walk pops one
                           * node per iteration, which is exact but slow. */
     int32_t max_level;   /* octree levels (3 key bits each), 4..21 */

@@ -46,7 +46,7 @@ class Config:
     h_max_iter: int = 64
     n_boot: int = 50
     leaf_size: int = 16
-    stack_cap: int = 1024
+    stack_cap: int = 768
     max_level: int = 16
     gravity: bool = True
     quadrupole: bool = True

@@ -578,7 +578,7 @@ void sph3_default_config(sph3_config *cfg) {
     cfg->h_max_iter = 64;
     cfg->n_boot = 50;
     cfg->leaf_size = 16;
-    cfg->stack_cap = 1024;
+    cfg->stack_cap = 768;
     cfg->max_level = 16;
     cfg->gravity = 1;
     cfg->quadrupole = 1;

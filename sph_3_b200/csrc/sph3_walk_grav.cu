@@ -372,8 +372,11 @@ __device__ __forceinline__ void spline_near(float r2, float r, float e, float &f
     }
 }
 
+// 24 resident warps per SM (at most 85 registers): the walk part is latency-bound
+constexpr int kGravMinWarpsPerSM = 24;
+
 template <bool QUAD>
-__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f32(GArgs A) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWarps) k_gravity_f32(GArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTileF));
     GTileF &tile = *reinterpret_cast<GTileF *>(wm.tile);

@@ -206,7 +206,7 @@ constexpr int kHK = 16;  // thresholds per pass in the reference-step mode
 constexpr double kNewtonDelta = 0.08;
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HArgs A) {
+__device__ __forceinline__ void h_search_body(const HArgs &A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = V4<R>;
@@ -392,6 +392,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HA
         atomicAdd(&a.counters[5], passes);
     }
 }
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HArgs A) {
+    h_search_body<R, MODE>(A);
+}
+
+// The mixed Newton search (the per-step path) capped at 102 registers: 20
+// resident warps per SM instead of 16 (its walk is latency-bound).
+__global__ void __maxnreg__(102) k_h_search_f32_newton(HArgs A) { h_search_body<float, SPH3_H_NEWTON>(A); }
 
 // ============================================================ bootstrap h
 // h = 0.5 * (k-th smallest distance, self included), the reference's
@@ -1197,7 +1206,7 @@ void launch_h_search(State &S, const Params &P, cudaStream_t st) {
         if (P.h_mode == SPH3_H_REFSTEP)
             run_walk(k_h_search<float, SPH3_H_REFSTEP>, A, walk_smem<V4<float>>(P), S, st, 1);
         else
-            run_walk(k_h_search<float, SPH3_H_NEWTON>, A, walk_smem<V4<float>>(P), S, st, 1);
+            run_walk(k_h_search_f32_newton, A, walk_smem<V4<float>>(P), S, st, 1);
     }
 }
 
