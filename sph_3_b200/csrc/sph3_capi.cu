@@ -175,7 +175,7 @@ void free_buffers(sph3_ctx *c) {
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.tree.bounds, S.tree.gw, S.tree.sw, S.list, S.nlist, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.tree.scan_tmp, S.tree.bounds, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
                     S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -189,6 +189,7 @@ void free_buffers(sph3_ctx *c) {
     S.pk_pos = S.pk_hme = S.pk_vel = S.pk_thm = nullptr;
     S.sort_hist = nullptr;
     S.list = S.nlist = nullptr;
+    S.hrec = nullptr;
     S.list_cap = 0;
     S.list_valid = false;
     S.tree = Tree{};
@@ -226,11 +227,14 @@ int ensure_lists(sph3_ctx *c, int64_t nn) {
     if (want == S.list_cap && (want == 0 || S.list)) return SPH3_OK;
     if (S.list) cudaFree(S.list);
     if (S.nlist) cudaFree(S.nlist);
+    if (S.hrec) cudaFree(S.hrec);
     S.list = S.nlist = nullptr;
+    S.hrec = nullptr;
     S.list_cap = 0;
     if (want == 0) return SPH3_OK;
     CK(dalloc(&S.list, (size_t)want * nn));
     CK(dalloc(&S.nlist, nn));
+    CK(dalloc(&S.hrec, 3 * (size_t)nn));
     S.list_cap = want;
     return SPH3_OK;
 }

@@ -144,6 +144,7 @@ struct State {
     int *nlist = nullptr;  // [n] neighbours found (may exceed list_cap: then the hydro pass walks)
     int list_cap = 0;
     bool list_valid = false;  // host flag: lists match the current order, positions and h
+    float4 *hrec = nullptr;   // [n][3] hydro source records {pk_pos}, {vx, vy, vz, m}, {rho, P/rho^2, c, h}
 };
 
 struct Params {

@@ -944,6 +944,7 @@ struct LArgs {
     const int *list, *nlist;
     int list_cap;
     const float4 *pk_pos, *pk_hme, *pk_vel, *pk_thm;
+    float4 *hrec;  // [n][3] source records, packed by k_pack_hrec
     const uint64_t *key;
     int cloud_shift;
     const Cloud *clouds;
@@ -954,6 +955,18 @@ struct LArgs {
     float alpha, beta, eta2;
     unsigned long long *counters;
 };
+
+// one 48-byte record per source: everything a hydro pair reads from it, in
+// two 32-byte sectors instead of four (pk_pos, pk_hme, pk_vel, pk_thm)
+__global__ void k_pack_hrec(LArgs A) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 hm = A.pk_hme[i], v = A.pk_vel[i], t = A.pk_thm[i];
+        A.hrec[3 * i] = A.pk_pos[i];
+        A.hrec[3 * i + 1] = make_float4(v.x, v.y, v.z, hm.y);
+        A.hrec[3 * i + 2] = make_float4(t.x, t.y, t.z, hm.x);
+    }
+}
 
 __device__ __forceinline__ float min_image(float d, float L) {
     if (L > 0.f) d -= L * rintf(d * (1.0f / L));
@@ -969,20 +982,32 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
         const int cnt = A.nlist[i];
         if (cnt > A.list_cap) continue;  // walked instead
         const float s10 = A.clouds[(int)(A.key[i] >> A.cloud_shift)].s10;
-        const float4 pi = A.pk_pos[i];
+        const float4 pi = A.hrec[3 * i], tv = A.hrec[3 * i + 1], tt = A.hrec[3 * i + 2];  // tt = {rho, P/rho^2, c, h}
         const int ref = __float_as_int(pi.w);
         const float3 t = rel_to(pi, ref, s10);
-        const float th = A.pk_hme[i].x;
-        const float4 tv = A.pk_vel[i];
-        const float4 tt = A.pk_thm[i];  // {rho, P/rho^2, c, f}
+        const float th = tt.w;
+        const float tf = VISC == SPH3_VISC_BALSARA ? A.pk_thm[i].w : 0.f;
         float ax = 0.f, ay = 0.f, az = 0.f, du = 0.f;
         const int *row = A.list + (size_t)i * A.list_cap;
+        // software pipeline: the next source's record is in flight while this pair runs
+        int jn = cnt > 0 ? row[0] : 0;
+        float4 q0, q1, q2;
+        if (cnt > 0) {
+            q0 = A.hrec[3 * jn];
+            q1 = A.hrec[3 * jn + 1];
+            q2 = A.hrec[3 * jn + 2];
+        }
         for (int k = 0; k < cnt; ++k) {
-            const int j = row[k];
-            const float3 p = rel_to(A.pk_pos[j], ref, s10);
-            const float hj = A.pk_hme[j].x, mj = A.pk_hme[j].y;
-            const float4 sv = A.pk_vel[j];
-            const float4 st = A.pk_thm[j];
+            const float4 r0 = q0, r1 = q1, r2 = q2;  // {pos}, {vx, vy, vz, m}, {rho, P/rho^2, c, h}
+            const int j = jn;
+            if (k + 1 < cnt) {
+                jn = row[k + 1];
+                q0 = A.hrec[3 * jn];
+                q1 = A.hrec[3 * jn + 1];
+                q2 = A.hrec[3 * jn + 2];
+            }
+            const float3 p = rel_to(r0, ref, s10);
+            const float hj = r2.w, mj = r1.w;
             float dx = t.x - p.x, dy = t.y - p.y, dz = t.z - p.z;
             if (A.periodic) {
                 dx = min_image(dx, A.box[0]);
@@ -1003,22 +1028,22 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
                 nW = __fdividef((float)(-0.75 * kSig) * ih5 * tq * tq, q + 1e-20f);
             }
             const float gx = nW * dx, gy = nW * dy, gz = nW * dz;
-            const float vx = tv.x - sv.x, vy = tv.y - sv.y, vz = tv.z - sv.z;
+            const float vx = tv.x - r1.x, vy = tv.y - r1.y, vz = tv.z - r1.z;
             const float vr = vx * dx + vy * dy + vz * dz;
-            const float rhoij = 0.5f * (tt.x + st.x);
+            const float rhoij = 0.5f * (tt.x + r2.x);
             float PI = 0.f;
             if (VISC == SPH3_VISC_MG83) {
-                const float cij = 0.5f * (tt.z + st.z);
+                const float cij = 0.5f * (tt.z + r2.z);
                 const float mu = __fdividef(hij * vr, rr * rr + hij * hij * eta2);
                 if (vr <= 0.f) PI = __fdividef(-alpha * cij * mu + beta * mu * mu, rhoij);
             } else {
                 const float w = __fdividef(vr, rr + 1e-5f);
-                const float vsig = tt.z + st.z - 3.f * w;
+                const float vsig = tt.z + r2.z - 3.f * w;
                 if (vr <= 0.f) PI = __fdividef(-0.5f * alpha * vsig * w, rhoij);
-                if (VISC == SPH3_VISC_BALSARA) PI = 0.5f * (tt.w + st.w) * PI;
+                if (VISC == SPH3_VISC_BALSARA) PI = 0.5f * (tf + A.pk_thm[j].w) * PI;
             }
             if (ACC) {
-                const float pt = mj * (tt.y + st.y + PI);
+                const float pt = mj * (tt.y + r2.y + PI);
                 ax -= pt * gx;
                 ay -= pt * gy;
                 az -= pt * gz;
@@ -1271,7 +1296,9 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
         L.acc_sph = S.acc_sph; L.dudt = S.dudt;
         L.alpha = (float)P.alpha; L.beta = (float)P.beta; L.eta2 = (float)(P.eta * P.eta);
         L.counters = S.counters;
+        L.hrec = S.hrec;
         const int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 16);
+        k_pack_hrec<<<blocks, 256, 0, st>>>(L);
         if (P.visc == SPH3_VISC_MG83) list_dispatch<SPH3_VISC_MG83>(L, want_acc, want_dudt, blocks, st);
         else if (P.visc == SPH3_VISC_BALSARA) list_dispatch<SPH3_VISC_BALSARA>(L, want_acc, want_dudt, blocks, st);
         else list_dispatch<SPH3_VISC_SIGNAL>(L, want_acc, want_dudt, blocks, st);
