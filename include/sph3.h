@@ -127,7 +127,10 @@ extern "C" {
 #define SPH3_FIELD_NNGB 17     /* 1, neighbour count N(r < 2h) of the last h search */
 #define SPH3_FIELD_BALSARA 18  /* 1 */
 #define SPH3_FIELD_U_PREV 19   /* 1 */
-#define SPH3_NUM_FIELDS 20
+#define SPH3_FIELD_VSIG 20     /* 1, max signal velocity c_i + c_j - 3 w_ij over the last hydro pass's pairs */
+#define SPH3_FIELD_DT 21       /* 1, per-particle time step of the last sph3_timestep */
+#define SPH3_FIELD_DHDT 22     /* 1, h divV / 3 of the last sph3_timestep */
+#define SPH3_NUM_FIELDS 23
 
 /* ---------------------------------------------------------------- config */
 typedef struct sph3_config {
@@ -264,6 +267,20 @@ int sph3_counters(sph3_ctx *ctx, int64_t out[16], int clear);
  * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,
  * [5] density, [6] gravity, [7] hydro, [8] kick+u+energy.  Clears if `clear`. */
 int sph3_phase_times(sph3_ctx *ctx, double out[9], int clear);
+
+/* Per-particle time step, the reference's dt_array_indiv_dt
+ * (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:1189-1262;
+ * present but switched off in its driver, hfvGpuSphBHtree_newCool_v8_KH.cu:1540):
+ *   dt_i = min(C h/max_j vsig_ij, C h/(h|divV| + max(c,|v|)(1 + 0.6 alpha)),
+ *              sqrt(h/|a_g|), sqrt(h/|a|), 0.4 sqrt(eps/|a|), 0.4 eps/|v|),
+ * vsig_ij = c_i + c_j - 3 (v_ij . r_ij)/(|r_ij| + 1e-5), in FP64, into the
+ * SPH3_FIELD_DT field (and h divV / 3 into SPH3_FIELD_DHDT); *dt_min gets the
+ * minimum over all particles.  all_pairs = 1 takes max_j over every particle
+ * of the system, as the reference does (O(N^2)); 0 takes it over the pairs of
+ * the last hydro pass (|r_ij| <= h_i + h_j), which that pass recorded in
+ * SPH3_FIELD_VSIG.  Uses the accelerations of the last step or compute call;
+ * div v is recomputed at the current positions and velocities. */
+int sph3_timestep(sph3_ctx *ctx, double c_cfl, int all_pairs, double *dt_min, void *stream);
 
 /* Kernel launches one sph3_step makes once its CUDA graph is captured (the
  * kernel nodes of the graph; memsets are not counted), or -1 before the

@@ -80,6 +80,7 @@ def _load():
         "orc_grav_sym": [I, P, P, D, P, P],
         "orc_pe": [I, P, P, D, P],
         "orc_ke": [I, P, P],
+        "orc_timestep": [I, P, P, P, P, P, P, P, P, D, D, C, P, I, P, P],
         "orc_set_threads": [C],
         "orc_num_threads": [],
     }
@@ -352,3 +353,15 @@ def getKE(v, m):
 
 
 from .step import serial_first_step, serial_step  # noqa: E402,F401
+
+def timestep_rows(pos, v, acc_tot, acc_g, h, c, divV, eps, c_cfl, alpha, neighbours=False, rows=None):
+    """Per-particle dt and dh/dt of dt_array_indiv_dt (see orc_timestep)."""
+    pos = _f64(pos, (-1, 3)); n = pos.shape[0]
+    v = _f64(v, (-1, 3)); at = _f64(acc_tot, (-1, 3)); ag = _f64(acc_g, (-1, 3))
+    h = _f64(h); c = _f64(c); dv = _f64(divV)
+    eps = np.broadcast_to(_f64(eps), (n,)).copy() if np.ndim(eps) == 0 else _f64(eps)
+    r = _rows(n, rows)
+    dt = np.zeros(r.shape[0]); dh = np.zeros(r.shape[0])
+    _load().orc_timestep(n, _ptr(pos), _ptr(v), _ptr(at), _ptr(ag), _ptr(h), _ptr(c), _ptr(dv), _ptr(eps),
+                         float(c_cfl), float(alpha), 1 if neighbours else 0, _ptr(r), r.shape[0], _ptr(dt), _ptr(dh))
+    return dt, dh

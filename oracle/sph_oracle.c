@@ -489,3 +489,58 @@ double orc_ke(int64_t n, const double *v, const double *m) {
         KE += 0.5 * m[i] * (ipow(v[3 * i + 0], 2) + ipow(v[3 * i + 1], 2) + ipow(v[3 * i + 2], 2));
     return KE;
 }
+
+/* Per-particle time step, restating dt_array_indiv_dt
+ * (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:
+ * 1189-1262) in FP64:
+ *   vsig_ij  = c_i + c_j - 3 w_ij,  w_ij = (v_ij . r_ij) / (|r_ij| + 1e-5)
+ *   dt_hyd   = C h_i / max_j vsig_ij            (max starts at 0)
+ *   dt_cour  = C h_i / (h_i |divV_i| + max(c_i, |v_i|) (1 + 0.6 alpha))
+ *   dt_G1    = 0.4 sqrt(eps_i / |a_tot,i|),  dt_G2 = 0.4 eps_i / |v_i|
+ *   dt_f     = sqrt(h_i / |a_g,i|),          dt_kin = sqrt(h_i / |a_tot,i|)
+ *   dt_i     = min of the six;  dh/dt_i = h_i divV_i / 3.
+ * The reference takes the signal-velocity maximum over every particle
+ * (neighbours = 0); neighbours = 1 restricts it to |r_ij| <= h_i + h_j (the
+ * support of the hydro pairs, as in the criterion's source, Springel 2005
+ * eq. 16).  j = i contributes c_i + c_i (w = 0), as in the reference loop. */
+void orc_timestep(int64_t n, const double *pos, const double *v, const double *acc_tot,
+                  const double *acc_g, const double *h, const double *c, const double *divV,
+                  const double *eps, double c_cfl, double alpha, int neighbours,
+                  const int64_t *rows, int64_t nrows, double *dt, double *dhdt) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        const int64_t i = rows[r];
+        double vmax = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            const double dx = pos[3 * i + 0] - pos[3 * j + 0];
+            const double dy = pos[3 * i + 1] - pos[3 * j + 1];
+            const double dz = pos[3 * i + 2] - pos[3 * j + 2];
+            const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            if (neighbours && !(rr <= h[i] + h[j])) continue;
+            const double vx = v[3 * i + 0] - v[3 * j + 0];
+            const double vy = v[3 * i + 1] - v[3 * j + 1];
+            const double vz = v[3 * i + 2] - v[3 * j + 2];
+            const double w = (vx * dx + vy * dy + vz * dz) / (rr + 1e-5);
+            const double s = c[i] + c[j] - 3.0 * w;
+            if (s > vmax) vmax = s;
+        }
+        const double ag = sqrt(acc_g[3 * i] * acc_g[3 * i] + acc_g[3 * i + 1] * acc_g[3 * i + 1] +
+                               acc_g[3 * i + 2] * acc_g[3 * i + 2]);
+        const double at = sqrt(acc_tot[3 * i] * acc_tot[3 * i] + acc_tot[3 * i + 1] * acc_tot[3 * i + 1] +
+                               acc_tot[3 * i + 2] * acc_tot[3 * i + 2]);
+        const double av = sqrt(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+        const double d[6] = {
+            c_cfl * h[i] / vmax,
+            c_cfl * h[i] / (h[i] * fabs(divV[i]) + fmax(c[i], av) * (1.0 + 0.6 * alpha)),
+            sqrt(h[i] / ag),
+            sqrt(h[i] / at),
+            0.4 * sqrt(eps[i] / at),
+            0.4 * eps[i] / av,
+        };
+        double m = d[0];
+        for (int k = 0; k < 6; ++k)
+            if (d[k] <= m) m = d[k];
+        dt[r] = m;
+        dhdt[r] = 1.0 / 3.0 * h[i] * divV[i];
+    }
+}

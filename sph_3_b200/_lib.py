@@ -103,6 +103,7 @@ SIGNATURES = {
     "sph3_counters": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_phase_times": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_kernels_per_step": (ctypes.c_int, [P, P]),
+    "sph3_timestep": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_int, P, P]),
     "sph3_morton_sort_noalloc": (ctypes.c_int, [P, I64, I32, P, P, P]),
 }
 

@@ -21,7 +21,8 @@ FIELDS = {
     "acc_sph": (C["SPH3_FIELD_ACC_SPH"], 3), "dudt": (C["SPH3_FIELD_DUDT"], 1),
     "dudt_prev": (C["SPH3_FIELD_DUDT_PREV"], 1), "phi": (C["SPH3_FIELD_PHI"], 1),
     "nngb": (C["SPH3_FIELD_NNGB"], 1), "balsara": (C["SPH3_FIELD_BALSARA"], 1),
-    "u_prev": (C["SPH3_FIELD_U_PREV"], 1),
+    "u_prev": (C["SPH3_FIELD_U_PREV"], 1), "vsig": (C["SPH3_FIELD_VSIG"], 1),
+    "dt": (C["SPH3_FIELD_DT"], 1), "dhdt": (C["SPH3_FIELD_DHDT"], 1),
 }
 
 DO = {k[len("SPH3_DO_"):].lower(): v for k, v in C.items() if k.startswith("SPH3_DO_")}
@@ -242,6 +243,14 @@ class Context:
                 "tree_nodes", "tree_leaves", "visits_h", "visits_density", "visits_hydro", "visits_gravity",
                 "walk_max_iter", "walk_max_where", "grav_groups"]
         return dict(zip(keys, out.tolist()))
+
+    def timestep(self, c_cfl=0.25, all_pairs=False):
+        """Per-particle time steps of the reference's criterion (see sph3_timestep in
+        include/sph3.h); returns (dt per particle in the caller's order, min dt)."""
+        v = ctypes.c_double()
+        check(self.lib.sph3_timestep(self._ptr, float(c_cfl), 1 if all_pairs else 0, ctypes.byref(v), None),
+              "timestep")
+        return self.get_field("dt"), float(v.value)
 
     def kernels_per_step(self):
         """Kernel launches per step of the captured step graph (-1 before capture)."""

@@ -81,7 +81,7 @@ int64_t count_kernel_nodes(cudaGraph_t g) {
 int check_launch() { return cuda_err(cudaGetLastError()); }
 
 constexpr int kCarried = 12;  // pos(3) vel(3) u u_prev dudt_prev m h eps
-constexpr int kFixed = 17;    // acc(3) acc_g(3) acc_sph(3) dudt rho P c divV curlV bal phi
+constexpr int kFixed = 20;    // acc(3) acc_g(3) acc_sph(3) dudt rho P c divV curlV bal phi vsig dt dhdt
 
 void point_carried(sph3_ctx *c) {
     State &S = c->S;
@@ -113,6 +113,9 @@ void point_fixed(sph3_ctx *c) {
     S.curlV = b + 14 * n;
     S.bal = b + 15 * n;
     S.phi = b + 16 * n;
+    S.vsig = b + 17 * n;
+    S.dt = b + 18 * n;
+    S.dhdt = b + 19 * n;
 }
 
 void params_from(const sph3_config &cfg, Params &P) {
@@ -384,6 +387,9 @@ double *field_ptr(sph3_ctx *c, int f, int *ncomp) {
         case SPH3_FIELD_PHI: return S.phi;
         case SPH3_FIELD_BALSARA: return S.bal;
         case SPH3_FIELD_U_PREV: return S.u_prev;
+        case SPH3_FIELD_VSIG: return S.vsig;
+        case SPH3_FIELD_DT: return S.dt;
+        case SPH3_FIELD_DHDT: return S.dhdt;
         default: return nullptr;
     }
 }
@@ -1029,6 +1035,29 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
         point_carried(c);
         c->inv_valid = false;
     }
+    return SPH3_OK;
+}
+
+int sph3_timestep(sph3_ctx *c, double c_cfl, int all_pairs, double *dt_min, void *stream) {
+    if (!c || !dt_min || !(c_cfl > 0.0)) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    State &S = c->S;
+    if (S.n == 0) {
+        *dt_min = INFINITY;
+        return SPH3_OK;
+    }
+    int rc = sync_packs(c, st);
+    if (rc) return rc;
+    // div v at the current positions and velocities (rho, P, c kept)
+    launch_density(S, c->P, true, st, true);
+    c->bal_dirty = false;
+    launch_timestep(S, c->P, c_cfl, all_pairs != 0, c->staging, st);
+    rc = check_launch();
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(dt_min, c->staging, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     return SPH3_OK;
 }
 

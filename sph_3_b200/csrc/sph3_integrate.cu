@@ -8,6 +8,9 @@
 //   a_sph; a = a_g + a_sph; v += a dt/2          -> k_kick_update (second_kick)
 // The MPI driver (sph_code/sph_mpi4_v4.py:380-427) kicks first and computes
 // du/dt with the full-step v; both orders are available.
+#include <algorithm>
+#include <cmath>
+
 #include "sph3_internal.cuh"
 
 namespace sph3 {
@@ -164,6 +167,108 @@ void launch_energy(State &S, const Params &P, cudaStream_t st) {
     }
     k_energy_part<<<kEnergyBlocks, 256, 0, st>>>(S.n, S.vel, S.m, S.u, S.phi, S.energy_part);
     k_energy_final<<<1, 32, 0, st>>>(S.energy_part, kEnergyBlocks, S.energy);
+}
+
+// ------------------------------------------------------------ time step
+// Per-particle time-step estimate of the reference's dt_array_indiv_dt
+// (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:
+// 1189-1262), in FP64: dt_i = min(dt_hyd, dt_cour, dt_f, dt_kin, dt_G1, dt_G2)
+// with dt_hyd = C h / max_j vsig_ij, dt_cour = C h / (h |divV| + max(c, |v|)
+// (1 + 0.6 alpha)), dt_f = sqrt(h / |a_g|), dt_kin = sqrt(h / |a|),
+// dt_G1 = 0.4 sqrt(eps / |a|), dt_G2 = 0.4 eps / |v|; dh/dt = h divV / 3.
+
+// signal-velocity maximum over every particle of the same system (the
+// reference's all-pairs loop): one block per target row, FP64
+__global__ void __launch_bounds__(256) k_vsig_all(const Cloud *clouds, int ncloud, const double *pos,
+                                                  const double *vel, const double *c, int64_t n,
+                                                  double *vsig) {
+    __shared__ double red[8];
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        int lo = 0, hi = ncloud - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (clouds[mid].begin <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const Cloud &cl = clouds[lo];
+        const double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i];
+        const double vxi = vel[i], vyi = vel[n + i], vzi = vel[2 * n + i], ci = c[i];
+        double m = 0.0;
+        for (int64_t j = cl.begin + threadIdx.x; j < cl.end; j += blockDim.x) {
+            const double dx = xi - pos[j], dy = yi - pos[n + j], dz = zi - pos[2 * n + j];
+            const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const double vr = (vxi - vel[j]) * dx + (vyi - vel[n + j]) * dy + (vzi - vel[2 * n + j]) * dz;
+            const double sig = ci + c[j] - 3.0 * (vr / (rr + 1e-5));
+            m = fmax(m, sig);
+        }
+        m = warp_max(m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmax(t, red[w]);
+            vsig[i] = t;
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kDtBlocks = 296;
+
+__global__ void __launch_bounds__(256) k_timestep(int64_t n, const double *vel, const double *acc,
+                                                  const double *acc_g, const double *h, const double *c,
+                                                  const double *divV, const double *eps, const double *vsig,
+                                                  double c_cfl, double alpha, double *dt, double *dhdt,
+                                                  double *part) {
+    double lmin = INFINITY;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ag = sqrt(acc_g[i] * acc_g[i] + acc_g[n + i] * acc_g[n + i] + acc_g[2 * n + i] * acc_g[2 * n + i]);
+        const double at = sqrt(acc[i] * acc[i] + acc[n + i] * acc[n + i] + acc[2 * n + i] * acc[2 * n + i]);
+        const double av = sqrt(vel[i] * vel[i] + vel[n + i] * vel[n + i] + vel[2 * n + i] * vel[2 * n + i]);
+        const double hi = h[i], ci = c[i], ei = eps[i];
+        const double d[6] = {c_cfl * hi / vsig[i],
+                             c_cfl * hi / (hi * fabs(divV[i]) + fmax(ci, av) * (1.0 + 0.6 * alpha)),
+                             sqrt(hi / ag),
+                             sqrt(hi / at),
+                             0.4 * sqrt(ei / at),
+                             0.4 * ei / av};
+        double m = d[0];
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (d[k] <= m) m = d[k];
+        dt[i] = m;
+        dhdt[i] = 1.0 / 3.0 * hi * divV[i];
+        lmin = fmin(lmin, m);
+    }
+    __shared__ double red[8];
+    lmin = warp_min(lmin);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lmin;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = INFINITY;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmin(t, red[w]);
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_min_final(const double *part, int nb, double *out) {
+    if (threadIdx.x == 0) {
+        double t = INFINITY;
+        for (int b = 0; b < nb; ++b) t = fmin(t, part[b]);
+        *out = t;
+    }
+}
+
+void launch_timestep(State &S, const Params &P, double c_cfl, bool all_pairs, double *dt_min_dev,
+                     cudaStream_t st) {
+    if (S.n == 0) return;
+    if (all_pairs) {
+        const int blocks = (int)std::min<int64_t>(S.n, (int64_t)S.num_sms * 16);
+        k_vsig_all<<<blocks, 256, 0, st>>>(S.clouds, S.ncloud, S.pos, S.vel, S.c, S.n, S.vsig);
+    }
+    k_timestep<<<kDtBlocks, 256, 0, st>>>(S.n, S.vel, S.acc, S.acc_g, S.h, S.c, S.divV, S.eps, S.vsig, c_cfl,
+                                          P.alpha, S.dt, S.dhdt, S.energy_part);
+    k_min_final<<<1, 32, 0, st>>>(S.energy_part, kDtBlocks, dt_min_dev);
 }
 
 // non-finite velocity, mass, u or h -> SPH3_STATUS_NAN_INPUT (positions are

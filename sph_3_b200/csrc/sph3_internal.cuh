@@ -115,6 +115,7 @@ struct State {
     double *u = nullptr, *u_prev = nullptr, *dudt = nullptr, *dudt_prev = nullptr;
     double *m = nullptr, *h = nullptr, *eps = nullptr, *rho = nullptr, *P = nullptr, *c = nullptr;
     double *divV = nullptr, *curlV = nullptr, *bal = nullptr, *phi = nullptr;
+    double *vsig = nullptr, *dt = nullptr, *dhdt = nullptr;  // signal velocity, time-step estimate
     int *nngb = nullptr;
     int64_t *orig = nullptr;
     // keys / sort
@@ -299,6 +300,8 @@ void launch_first_u(State &S, const Params &P, double dt, cudaStream_t st);
 void launch_sum_acc(State &S, cudaStream_t st);
 void launch_energy(State &S, const Params &P, cudaStream_t st);
 void launch_check_finite(State &S, cudaStream_t st);
+void launch_timestep(State &S, const Params &P, double c_cfl, bool all_pairs, double *dt_min_dev,
+                     cudaStream_t st);
 
 // pack selectors for launch_pack
 constexpr unsigned kPackPos = 1, kPackHme = 2, kPackVel = 4, kPackThm = 8;

@@ -754,6 +754,7 @@ struct YArgs {
     const float4 *pk_hme, *pk_vel, *pk_thm;
     const double *h, *m, *vel, *rho, *P, *c, *bal;
     double *acc_sph, *dudt;
+    double *vsig;  // max signal velocity over the pairs (written with the acceleration)
     double alpha, beta, eta;
     // only_overflow: walk only for particles whose neighbour list overflowed
     const int *nlist;
@@ -800,7 +801,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
             trho = (R)t.x; tpr = (R)t.y; tc = (R)t.z; tf = (R)t.w;
         }
         const float hmax_g = warp_max(gi.active ? (float)th : 0.f);
-        R ax = 0, ay = 0, az = 0, du = 0;
+        R ax = 0, ay = 0, az = 0, du = 0, vmax = 0;
         const Images ims = group_images(gb, hmax_g + a.box_h[gi.root].w, a.box, a.periodic);
         for (int im = 0; im < 27; ++im) {
             float3 s;
@@ -891,16 +892,19 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
                     const R vr = vx * dx + vy * dy + vz * dz;
                     const R rhoij = (R)0.5 * (trho + en.t.x);
                     R PI = 0;
+                    R vsig;  // signal velocity (time-step estimate)
                     if (VISC == SPH3_VISC_MG83) {
                         const R cij = (R)0.5 * (tc + en.t.z);
                         const R mu = fdiv(hij * vr, rr * rr + hij * hij * eta2);
                         if (vr <= (R)0) PI = fdiv(-alpha * cij * mu + beta * mu * mu, rhoij);
+                        if (ACC) vsig = tc + en.t.z - (R)3 * fdiv(vr, rr + (R)1e-5);
                     } else {
                         const R w = fdiv(vr, rr + (R)1e-5);
-                        const R vsig = tc + en.t.z - (R)3 * w;
+                        vsig = tc + en.t.z - (R)3 * w;
                         if (vr <= (R)0) PI = fdiv((R)-0.5 * alpha * vsig * w, rhoij);
                         if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + en.t.w) * PI;
                     }
+                    if (ACC && vsig > vmax) vmax = vsig;
                     const R mj = en.v.w;
                     if (ACC) {
                         const R pt = mj * (tpr + en.t.y + PI);
@@ -921,6 +925,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
                 A.acc_sph[i] = (double)ax;
                 A.acc_sph[a.n + i] = (double)ay;
                 A.acc_sph[2 * a.n + i] = (double)az;
+                A.vsig[i] = (double)vmax;
             }
             if (DU) A.dudt[i] = (double)du;
         }
@@ -951,7 +956,7 @@ struct LArgs {
     int64_t n;
     int periodic;
     float box[3];
-    double *acc_sph, *dudt;
+    double *acc_sph, *dudt, *vsig;
     float alpha, beta, eta2;
     unsigned long long *counters;
 };
@@ -987,7 +992,7 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
         const float3 t = rel_to(pi, ref, s10);
         const float th = tt.w;
         const float tf = VISC == SPH3_VISC_BALSARA ? A.pk_thm[i].w : 0.f;
-        float ax = 0.f, ay = 0.f, az = 0.f, du = 0.f;
+        float ax = 0.f, ay = 0.f, az = 0.f, du = 0.f, vmax = 0.f;
         const int *row = A.list + (size_t)i * A.list_cap;
         // software pipeline: the next source's record is in flight while this pair runs
         int jn = cnt > 0 ? row[0] : 0;
@@ -1032,16 +1037,19 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
             const float vr = vx * dx + vy * dy + vz * dz;
             const float rhoij = 0.5f * (tt.x + r2.x);
             float PI = 0.f;
+            float vsig;  // signal velocity (time-step estimate)
             if (VISC == SPH3_VISC_MG83) {
                 const float cij = 0.5f * (tt.z + r2.z);
                 const float mu = __fdividef(hij * vr, rr * rr + hij * hij * eta2);
                 if (vr <= 0.f) PI = __fdividef(-alpha * cij * mu + beta * mu * mu, rhoij);
+                if (ACC) vsig = tt.z + r2.z - 3.f * __fdividef(vr, rr + 1e-5f);
             } else {
                 const float w = __fdividef(vr, rr + 1e-5f);
-                const float vsig = tt.z + r2.z - 3.f * w;
+                vsig = tt.z + r2.z - 3.f * w;
                 if (vr <= 0.f) PI = __fdividef(-0.5f * alpha * vsig * w, rhoij);
                 if (VISC == SPH3_VISC_BALSARA) PI = 0.5f * (tf + A.pk_thm[j].w) * PI;
             }
+            if (ACC) vmax = fmaxf(vmax, vsig);
             if (ACC) {
                 const float pt = mj * (tt.y + r2.y + PI);
                 ax -= pt * gx;
@@ -1055,6 +1063,7 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
             A.acc_sph[i] = (double)ax;
             A.acc_sph[A.n + i] = (double)ay;
             A.acc_sph[2 * A.n + i] = (double)az;
+            A.vsig[i] = (double)vmax;
         }
         if (DU) A.dudt[i] = (double)du;
     }
@@ -1279,7 +1288,7 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
     A.w = walk_args(S, P, 3);
     A.pk_hme = S.pk_hme; A.pk_vel = S.pk_vel; A.pk_thm = S.pk_thm;
     A.h = S.h; A.m = S.m; A.vel = S.vel; A.rho = S.rho; A.P = S.P; A.c = S.c; A.bal = S.bal;
-    A.acc_sph = S.acc_sph; A.dudt = S.dudt;
+    A.acc_sph = S.acc_sph; A.dudt = S.dudt; A.vsig = S.vsig;
     A.alpha = P.alpha; A.beta = P.beta; A.eta = P.eta;
     A.nlist = S.nlist;
     A.list_cap = S.list_cap;
@@ -1293,7 +1302,7 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
         L.n = S.n;
         L.periodic = P.periodic;
         for (int d = 0; d < 3; ++d) L.box[d] = (float)P.box[d];
-        L.acc_sph = S.acc_sph; L.dudt = S.dudt;
+        L.acc_sph = S.acc_sph; L.dudt = S.dudt; L.vsig = S.vsig;
         L.alpha = (float)P.alpha; L.beta = (float)P.beta; L.eta2 = (float)(P.eta * P.eta);
         L.counters = S.counters;
         L.hrec = S.hrec;
