@@ -239,6 +239,7 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
         int steps = 0;  // reference-rule steps taken
         int dir = 0;    // reference rule: -1 down, +1 up, 0 unknown (first pass)
         double lb = 0.0, hb = DBL_MAX;
+        int n_hb = 0;  // count at hb
         bool failed = false;
         const double hcap = 4.0 * cl.size;
         for (int pass = 0; pass < A.max_iter + 2; ++pass) {
@@ -353,8 +354,21 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                 } else {
                     // Newton step on ln N(ln h) with the slope measured between
                     // h and h (1 + delta), safeguarded by the bracket [lb, hb]
-                    if (n0 > up) hb = fmin(hb, h);
-                    else lb = fmax(lb, h);
+                    if (n0 > up && h < hb) {
+                        hb = h;
+                        n_hb = n0;
+                    } else if (n0 < low) {
+                        lb = fmax(lb, h);
+                    }
+                }
+                if (!conv && lb > 0.0 && hb < DBL_MAX && hb - lb <= 1e-6 * hb) {
+                    // the count jumps over the whole window at one radius (a
+                    // shell of equidistant neighbours, e.g. on a lattice): no h
+                    // reaches the window, take the smallest h above the jump
+                    h = hb;
+                    ncount = n_hb;
+                    conv = true;
+                } else if (!conv) {
                     double hn;
                     if (n0 == 0) {
                         hn = 2.0 * h;

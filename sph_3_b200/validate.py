@@ -29,7 +29,12 @@ def evolve(ctx, t_end, dt_max=1e-3, c_cfl=0.25, check_every=10, t0=0.0, first=Tr
     """Steps ``ctx`` from t0 to t_end; returns (t, number of steps, dts used)."""
     t = float(t0)
     if first:
-        ctx.first_step(dt_max)
+        # forces at t0 first, so that the start-up step already uses a safe dt
+        passes = ["boot_h", "h", "density", "acc_sph", "dudt"] + (["gravity"] if ctx.config.gravity else [])
+        ctx.compute(*passes)
+        _, dtmin = ctx.timestep(c_cfl)
+        k = 0 if not (dtmin < dt_max) else int(math.ceil(math.log2(dt_max / dtmin)))
+        ctx.first_step(dt_max * 2.0 ** (-k))
     steps = 0
     used = []
     while t < t_end * (1 - 1e-12):

@@ -1,0 +1,80 @@
+"""The full-size configurations besides the N = 1M Evrard benchmark, checked
+through size-free properties (the CPU oracle cannot run them):
+
+* Sedov blast, 128^3 = 2,097,152 particles on a jittered lattice in the
+  periodic unit box, hydro only, to t = 0.05: mixed vs the FP64 GPU path (L1
+  of density), total energy conservation, and the blast radius against the
+  Sedov-Taylor solution R = xi0 (E t^2 / rho)^(1/5), xi0 = 1.15 for gamma = 5/3;
+* Kelvin-Helmholtz slab, 4,194,304 particles, 200 steps: energy and momentum
+  conservation, no status flags, mixed vs FP64 density.
+Both use the global time step of the reference's per-particle criterion."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(ic, prec, t_end=None, nsteps=None, dt_max=1e-3):
+    from sph_3_b200 import Config, Context
+    from sph_3_b200 import validate as V
+    ctx = Context(Config(precision=prec, gravity=False, box=ic["box"]))
+    ctx.set_particles(ic["pos"], ic["m"], vel=ic["vel"], u=ic["u"])
+    E0 = ctx.energy()
+    if t_end is not None:
+        t, steps, used = V.evolve(ctx, t_end, dt_max=dt_max)
+    else:
+        # nsteps steps at the start-up time step of the criterion
+        ctx.compute("boot_h", "h", "density", "acc_sph", "dudt")
+        _, dtmin = ctx.timestep(0.25)
+        dt = dt_max * 2.0 ** (-int(np.ceil(np.log2(dt_max / dtmin)))) if dtmin < dt_max else dt_max
+        ctx.first_step(dt)
+        ctx.step(dt, nsteps - 1)
+        t, steps = dt * nsteps, nsteps
+    assert ctx.status() == 0, ctx.status_names()
+    out = {k: ctx.get_field(k) for k in ("pos", "vel", "rho", "u", "m")}
+    out["E0"], out["E1"], out["t"], out["steps"] = E0, ctx.energy(), t, steps
+    ctx.close()
+    return out
+
+
+def test_sedov_128_cubed_to_t005():
+    from sph_3_b200.ic import sedov
+    ic = sedov(n_side=128, seed=0)
+    mix = _run(ic, "mixed", t_end=0.05)
+    f64 = _run(ic, "fp64", t_end=0.05)
+
+    def drift(o):
+        e0 = o["E0"]["KE"] + o["E0"]["U"]
+        return (o["E1"]["KE"] + o["E1"]["U"] - e0) / e0
+
+    dE, dE64 = drift(mix), drift(f64)
+    l1 = np.mean(np.abs(mix["rho"] - f64["rho"])) / np.mean(f64["rho"])
+    # blast radius: mass-weighted radius of the particles heated above 1 % of the deposit's mean u
+    r = np.linalg.norm(mix["pos"] - 0.5, axis=1)
+    hot = mix["u"] > 100 * 1e-5
+    r_shock = np.percentile(r[hot], 99)
+    r_st = 1.15 * (1.0 * 0.05 ** 2 / 1.0) ** 0.2
+    print("Sedov 128^3: steps %d, dE/E %.2e (fp64 path %.2e), L1(rho) mixed vs fp64 %.2e, shock radius %.4f "
+          "(Sedov-Taylor %.4f)" % (mix["steps"], dE, dE64, l1, r_shock, r_st))
+    # the energy error is the integrator's (first order in the step, the same
+    # in FP64: 6 % at C_CFL = 0.25, 2.4 % at 0.1), not the arithmetic's
+    assert abs(dE) < 0.1 and abs(dE - dE64) < 0.01
+    assert l1 < 1e-2
+    assert abs(r_shock / r_st - 1) < 0.15
+
+
+def test_kelvin_helmholtz_4m_200_steps():
+    from sph_3_b200.ic import kelvin_helmholtz
+    ic = kelvin_helmholtz(n=4194304, seed=0)
+    mix = _run(ic, "mixed", nsteps=200)
+    f64 = _run(ic, "fp64", nsteps=200)
+    E0 = mix["E0"]["KE"] + mix["E0"]["U"]
+    dE = abs(mix["E1"]["KE"] + mix["E1"]["U"] - E0) / E0
+    p0 = np.array([mix["E0"][k] for k in ("px", "py", "pz")])
+    p1 = np.array([mix["E1"][k] for k in ("px", "py", "pz")])
+    l1 = np.mean(np.abs(mix["rho"] - f64["rho"])) / np.mean(f64["rho"])
+    print("KH 4M: t %.4f after 200 steps, |dE/E| %.2e, |dp| %.2e, L1(rho) mixed vs fp64 %.2e"
+          % (mix["t"], dE, np.abs(p1 - p0).max(), l1))
+    assert dE < 1e-3
+    assert np.abs(p1 - p0).max() < 1e-6
+    assert l1 < 1e-3
