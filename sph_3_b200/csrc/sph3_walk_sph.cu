@@ -692,11 +692,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
                         const float hs = (float)th + (float)en.p.w;  // = 2 hbar
                         {
                             const float ih = __fdividef(2.0f, hs);
-                            const float q = sqrtf(d2) * ih;
+                            // |r| as d2 * rsqrt(d2) (0 for the self pair), and both
+                            // branches of the kernel evaluated and selected: no
+                            // divergence inside the warp
+                            const float q = (d2 > 0.f ? d2 * rsqrtf(d2) : 0.f) * ih;
                             const float ih3 = ih * ih * ih;
-                            float W;
-                            if (q <= 1.0f) W = kSigF * ih3 * fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
-                            else { const float tq = 2.0f - q; W = kSigF * ih3 * 0.25f * tq * tq * tq; }
+                            const float tq = 2.0f - q;
+                            const float w_in = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
+                            const float w_out = 0.25f * tq * tq * tq;
+                            const float W = kSigF * ih3 * (q <= 1.0f ? w_in : w_out);
                             rho = fmaf((float)en.q.x, W, (float)rho);
                             if (DC) {
                                 float nW;
