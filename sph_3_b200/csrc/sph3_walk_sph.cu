@@ -559,15 +559,20 @@ struct DE<R, false> {
 // writes them 8 at a time (two 16-byte stores, one full 32-byte sector).
 constexpr int kListChunk = 8;
 constexpr size_t kListStageBytes = sizeof(int) * kListChunk * 32;
+// task list of the balanced density pass: one (target lane, tile entry) pair
+// per in-support candidate of a tile, at most 32 x 32
+constexpr size_t kTaskBytes = sizeof(unsigned short) * 32 * 32;
+constexpr size_t kDensityExtraBytes = kListStageBytes + kTaskBytes;
 
 template <typename R, bool DC>
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = DE<R, DC>;
-    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64 + kListStageBytes);
+    WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64 + kDensityExtraBytes);
     // neighbour-list staging: slot x of lane l at stage[x * 32 + l] (conflict-free)
     int *stage = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(wm.tile) + sizeof(E) * 64);
+    unsigned short *tasks = reinterpret_cast<unsigned short *>(stage + kListChunk * 32);
     E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
     unsigned long long pairs = 0;
@@ -720,8 +725,91 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
                     }
                 }
             };
+            // Mixed path without div/curl: pass 2 balanced over the warp.  The
+            // in-support (target, entry) pairs of the tile become a task list
+            // ordered by target; lane k runs task k of each chunk of 32 (target
+            // values by shuffle), writes the pair into the target's neighbour
+            // list, and the density terms are summed per target with a
+            // segmented warp reduction (fixed order: deterministic).  Lanes no
+            // longer idle while the lane with the most neighbours finishes.
+            auto interact_bal = [&](const E *t, int ne) {
+                if (gi.active) pairs += ne;
+                unsigned mask = 0;
+                if (gi.active) {
+                    for (int e = 0; e < ne; ++e) {
+                        const V4<R> p = t[e].p;
+                        const float dx = (float)tx - (float)p.x;
+                        const float dy = (float)ty - (float)p.y;
+                        const float dz = (float)tz - (float)p.z;
+                        const float hs = (float)th + (float)p.w;
+                        mask |= (unsigned)(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= hs * hs) << e;
+                    }
+                }
+                const int c = __popc(mask);
+                const int incl = warp_incl_scan(c);
+                const int total = __shfl_sync(kFull, incl, 31);
+                const int off = incl - c;
+                {
+                    int o = off;
+                    unsigned mm = mask;
+                    while (mm) {
+                        const int e = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        tasks[o++] = (unsigned short)((lane << 5) | e);
+                    }
+                }
+                __syncwarp();
+                for (int k0 = 0; k0 < total; k0 += 32) {
+                    const int k = k0 + lane;
+                    const bool valid = k < total;
+                    const int task = valid ? (int)tasks[k] : 0;
+                    const int tl = valid ? task >> 5 : 32;  // key: target lane (32 past the end)
+                    const int e = task & 31;
+                    const float qx = __shfl_sync(kFull, (float)tx, tl & 31);
+                    const float qy = __shfl_sync(kFull, (float)ty, tl & 31);
+                    const float qz = __shfl_sync(kFull, (float)tz, tl & 31);
+                    const float qh = __shfl_sync(kFull, (float)th, tl & 31);
+                    const int base = __shfl_sync(kFull, nkept, tl & 31);
+                    const int toff = __shfl_sync(kFull, off, tl & 31);
+                    float v = 0.f;
+                    if (valid) {
+                        const E en = t[e];
+                        if (A.list) {
+                            const int slot = base + (k - toff);
+                            if (slot < A.list_cap) A.list[(size_t)(gi.first + tl) * A.list_cap + slot] = en.get_j();
+                        }
+                        const float dx = qx - (float)en.p.x;
+                        const float dy = qy - (float)en.p.y;
+                        const float dz = qz - (float)en.p.z;
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float ih = __fdividef(2.0f, qh + (float)en.p.w);
+                        const float q = (d2 > 0.f ? d2 * rsqrtf(d2) : 0.f) * ih;
+                        const float ih3 = ih * ih * ih;
+                        const float tq = 2.0f - q;
+                        const float w_in = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
+                        const float w_out = 0.25f * tq * tq * tq;
+                        v = (float)en.q.x * (kSigF * ih3 * (q <= 1.0f ? w_in : w_out));
+                    }
+                    // segmented suffix sums over equal keys (keys are non-decreasing)
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const float ov = __shfl_down_sync(kFull, v, d);
+                        const int ot = __shfl_down_sync(kFull, tl, d);
+                        if (lane + d < 32 && ot == tl) v += ov;
+                    }
+                    // each target takes the sum of its run inside this chunk
+                    const int first_pos = off > k0 ? off - k0 : 0;
+                    const float got = __shfl_sync(kFull, v, first_pos & 31);
+                    if (c > 0 && off < k0 + 32 && off + c > k0) rho += (R)got;
+                }
+                nkept += c;
+                __syncwarp();
+            };
             auto flush = [&](int nl) {
-                flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                if constexpr (sizeof(R) == 4 && !DC)
+                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact_bal);
+                else
+                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
@@ -729,9 +817,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
             const int i = gi.i;
             if (A.list) {
                 A.nlist[i] = nkept;
-                const int kept = min(nkept, A.list_cap);
-                const int base = kept & ~(kListChunk - 1);
-                for (int x = 0; x < kept - base; ++x) A.list[(size_t)i * A.list_cap + base + x] = stage[x * 32 + lane];
+                if constexpr (!(sizeof(R) == 4 && !DC)) {  // the staged path: write the last partial chunk
+                    const int kept = min(nkept, A.list_cap);
+                    const int base = kept & ~(kListChunk - 1);
+                    for (int x = 0; x < kept - base; ++x)
+                        A.list[(size_t)i * A.list_cap + base + x] = stage[x * 32 + lane];
+                }
             }
             double r, P, c;
             if (A.keep_rho) {  // div/curl only: divide by the caller's rho
@@ -1277,11 +1368,11 @@ void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bo
     A.list_cap = S.list_cap;
     S.list_valid = A.list != nullptr;
     if (P.precision == SPH3_PREC_FP64) {
-        if (divcurl) run_walk(k_density<double, true>, A, walk_smem_x<DE<double, true>>(P, kListStageBytes), S, st, 2);
-        else run_walk(k_density<double, false>, A, walk_smem_x<DE<double, false>>(P, kListStageBytes), S, st, 2);
+        if (divcurl) run_walk(k_density<double, true>, A, walk_smem_x<DE<double, true>>(P, kDensityExtraBytes), S, st, 2);
+        else run_walk(k_density<double, false>, A, walk_smem_x<DE<double, false>>(P, kDensityExtraBytes), S, st, 2);
     } else {
-        if (divcurl) run_walk(k_density<float, true>, A, walk_smem_x<DE<float, true>>(P, kListStageBytes), S, st, 2);
-        else run_walk(k_density<float, false>, A, walk_smem_x<DE<float, false>>(P, kListStageBytes), S, st, 2);
+        if (divcurl) run_walk(k_density<float, true>, A, walk_smem_x<DE<float, true>>(P, kDensityExtraBytes), S, st, 2);
+        else run_walk(k_density<float, false>, A, walk_smem_x<DE<float, false>>(P, kDensityExtraBytes), S, st, 2);
     }
 }
 
