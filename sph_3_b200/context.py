@@ -190,12 +190,28 @@ class Context:
         check(self.lib.sph3_set_field(self._ptr, fid, p, on_dev, self._stream(on_dev)), "set_field " + name)
         del keep
 
-    def get_field(self, name, rows=None, device=False):
+    def get_field(self, name, rows=None, device=False, out=None):
         """Field values (caller's order).  rows: (begin, end) slice or None.
-        device=True returns a torch CUDA tensor."""
+        device=True returns a torch CUDA tensor.  out: a C-contiguous float64
+        host array (NumPy, or a torch CPU tensor, e.g. page-locked) of the
+        field's shape to copy into instead of a new array."""
         fid, nc = FIELDS[name]
         b, e = (0, self.n) if rows is None else (int(rows[0]), int(rows[1]))
         shape = (e - b, nc) if nc > 1 else (e - b,)
+        if out is not None:
+            if hasattr(out, "data_ptr"):  # torch CPU tensor
+                ok = (not out.is_cuda and out.is_contiguous() and str(out.dtype) == "torch.float64"
+                      and tuple(out.shape) == shape)
+                ptr = out.data_ptr()
+            else:
+                ok = (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                      and out.shape == shape)
+                ptr = out.ctypes.data if ok else 0
+            if not ok:
+                raise ValueError("get_field out= must be a C-contiguous float64 host array of shape %s" % (shape,))
+            check(self.lib.sph3_get_field(self._ptr, fid, ctypes.c_void_p(ptr), b, e, 0, None),
+                  "get_field " + name)
+            return out
         if device:
             import torch
             out = torch.empty(shape, dtype=torch.float64, device="cuda")

@@ -178,7 +178,7 @@ void free_buffers(sph3_ctx *c) {
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.tree.bounds, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.tree.scan_tmp, S.tree.bounds, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
                     S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -193,6 +193,7 @@ void free_buffers(sph3_ctx *c) {
     S.sort_hist = nullptr;
     S.list = S.nlist = nullptr;
     S.hrec = nullptr;
+    S.ovf = nullptr;
     S.list_cap = 0;
     S.list_valid = false;
     S.tree = Tree{};
@@ -231,13 +232,17 @@ int ensure_lists(sph3_ctx *c, int64_t nn) {
     if (S.list) cudaFree(S.list);
     if (S.nlist) cudaFree(S.nlist);
     if (S.hrec) cudaFree(S.hrec);
+    if (S.ovf) cudaFree(S.ovf);
     S.list = S.nlist = nullptr;
     S.hrec = nullptr;
+    S.ovf = nullptr;
     S.list_cap = 0;
     if (want == 0) return SPH3_OK;
     CK(dalloc(&S.list, (size_t)want * nn));
     CK(dalloc(&S.nlist, nn));
     CK(dalloc(&S.hrec, 3 * (size_t)nn));
+    CK(dalloc(&S.ovf, 1));
+    CK(cudaMemset(S.ovf, 0, sizeof(int)));
     S.list_cap = want;
     return SPH3_OK;
 }

@@ -146,6 +146,7 @@ struct State {
     int list_cap = 0;
     bool list_valid = false;  // host flag: lists match the current order, positions and h
     float4 *hrec = nullptr;   // [n][3] hydro source records {pk_pos}, {vx, vy, vz, m}, {rho, P/rho^2, c, h}
+    int *ovf = nullptr;       // [1] particles whose lists overflowed in the last density pass
 };
 
 struct Params {

@@ -412,9 +412,9 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_h_search(HA
     h_search_body<R, MODE>(A);
 }
 
-// The mixed Newton search (the per-step path) capped at 102 registers: 20
+// The mixed Newton search (the per-step path) capped at 96 registers: 20
 // resident warps per SM instead of 16 (its walk is latency-bound).
-__global__ void __maxnreg__(102) k_h_search_f32_newton(HArgs A) { h_search_body<float, SPH3_H_NEWTON>(A); }
+__global__ void __maxnreg__(96) k_h_search_f32_newton(HArgs A) { h_search_body<float, SPH3_H_NEWTON>(A); }
 
 // ============================================================ bootstrap h
 // h = 0.5 * (k-th smallest distance, self included), the reference's
@@ -534,6 +534,7 @@ struct DArgs {
     // neighbour lists for the hydro pass (null: none kept)
     int *list, *nlist;
     int list_cap;
+    int *ovf;  // particles with more pairs than list_cap
 };
 
 // tile entry: p = {x, y, z, h}, q = {m, vx, vy, vz}, and the sorted source
@@ -565,7 +566,7 @@ constexpr size_t kTaskBytes = sizeof(unsigned short) * 32 * 32;
 constexpr size_t kDensityExtraBytes = kListStageBytes + kTaskBytes;
 
 template <typename R, bool DC>
-__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DArgs A) {
+__device__ __forceinline__ void density_body(const DArgs &A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = DE<R, DC>;
@@ -817,6 +818,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
             const int i = gi.i;
             if (A.list) {
                 A.nlist[i] = nkept;
+                if (nkept > A.list_cap) atomicAdd(A.ovf, 1);
                 if constexpr (!(sizeof(R) == 4 && !DC)) {  // the staged path: write the last partial chunk
                     const int kept = min(nkept, A.list_cap);
                     const int base = kept & ~(kListChunk - 1);
@@ -857,6 +859,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DAr
     if (lane == 0) atomicAdd(&a.counters[2], pairs);
 }
 
+template <typename R, bool DC>
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_density(DArgs A) {
+    density_body<R, DC>(A);
+}
+
+// The mixed density pass of every step capped at 96 registers: 20 resident
+// warps per SM instead of 16.
+__global__ void __maxnreg__(96) k_density_f32(DArgs A) { density_body<float, false>(A); }
+
 // ============================================================ hydro
 struct YArgs {
     WalkArgs w;
@@ -869,6 +880,7 @@ struct YArgs {
     const int *nlist;
     int list_cap;
     int only_overflow;
+    const int *ovf;  // number of overflowed lists (only_overflow: nothing to do when 0)
 };
 
 // tile entry: p = {x, y, z, h}, v = {vx, vy, vz, m}, t = {rho, P/rho^2, c, f}
@@ -882,6 +894,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
     extern __shared__ __align__(16) unsigned char smem[];
     const WalkArgs &a = A.w;
     using E = YE<R>;
+    if (A.only_overflow && *A.ovf == 0) return;  // every list fitted
     WarpMem wm = carve_warp_mem(smem, a.stack_cap, sizeof(E) * 64);
     E *tile = reinterpret_cast<E *>(wm.tile);
     const int lane = lane_id();
@@ -1366,13 +1379,15 @@ void launch_density(State &S, const Params &P, bool divcurl, cudaStream_t st, bo
     A.list = S.list_cap > 0 ? S.list : nullptr;
     A.nlist = S.nlist;
     A.list_cap = S.list_cap;
+    A.ovf = S.ovf;
+    if (A.list) cudaMemsetAsync(S.ovf, 0, sizeof(int), st);
     S.list_valid = A.list != nullptr;
     if (P.precision == SPH3_PREC_FP64) {
         if (divcurl) run_walk(k_density<double, true>, A, walk_smem_x<DE<double, true>>(P, kDensityExtraBytes), S, st, 2);
         else run_walk(k_density<double, false>, A, walk_smem_x<DE<double, false>>(P, kDensityExtraBytes), S, st, 2);
     } else {
         if (divcurl) run_walk(k_density<float, true>, A, walk_smem_x<DE<float, true>>(P, kDensityExtraBytes), S, st, 2);
-        else run_walk(k_density<float, false>, A, walk_smem_x<DE<float, false>>(P, kDensityExtraBytes), S, st, 2);
+        else run_walk(k_density_f32, A, walk_smem_x<DE<float, false>>(P, kDensityExtraBytes), S, st, 2);
     }
 }
 
@@ -1402,6 +1417,7 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
     A.nlist = S.nlist;
     A.list_cap = S.list_cap;
     A.only_overflow = 0;
+    A.ovf = S.ovf;
     if (P.precision != SPH3_PREC_FP64 && S.list_valid) {
         // the list pass, then a walk for the particles whose lists overflowed
         LArgs L;
