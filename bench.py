@@ -148,8 +148,8 @@ def cpu_baseline(ic, target_s=12.0):
 
 # ------------------------------------------------------------ GPU arm
 # DRAM bytes per particle of one gravity launch, from the ncu capture
-# summarised in profiles/k_gravity_f32_evrard262k.md (12.62 MB at N=262144)
-GRAV_DRAM_BYTES_PER_PARTICLE = 12.62e6 / 262144
+# summarised in profiles/k_gravity_f32_evrard262k.md (14.07 MB at N=262144)
+GRAV_DRAM_BYTES_PER_PARTICLE = 14.07e6 / 262144
 
 
 def make_ic(n, seed):
@@ -307,7 +307,7 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "TFLOP/s", "frac": ach / fp32_peak,
                 "traffic": GRAV_DRAM_BYTES_PER_PARTICLE * n,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=262144 launch "
-                                  "(12.62 MB), scaled per particle to this N "
+                                  "(14.07 MB), scaled per particle to this N "
                                   "(profiles/k_gravity_f32_evrard262k.md)",
                 "peak_source": "nominal FP32 issue rate 148 SM x 128 lanes x 2 at the sampled median SM "
                                "clock (%.0f MHz); MEASURED_PEAKS.json has no CUDA-core FP32 figure" % sm_mhz,
