@@ -159,7 +159,10 @@ typedef struct sph3_config {
                           * particle; a multiple of 8 in 0..1024. */
     int32_t mac;         /* multipole acceptance: SPH3_MAC_BH (d > s/theta, the default) or
                           * SPH3_MAC_BH_OFFSET (d > s/theta + |com - box centre|, more conservative) */
-    int32_t reserved_i[2];
+    int32_t eps_from_h;  /* 1: gravitational softening eps = h after every h search, as the reference GPU
+                          * driver's set_eps_of_gas_to_h (Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:584-593);
+                          * 0 (default): eps stays as set (the benchmark fixes eps = 0.01) */
+    int32_t reserved_i[1];
     double gamma;        /* adiabatic index (5/3) */
     double alpha;        /* artificial viscosity alpha (1) */
     double beta;         /* beta of the MG83 form (2) */

@@ -60,7 +60,8 @@ class Config(ctypes.Structure):
         ("walk_warps", ctypes.c_int32),
         ("list_cap", ctypes.c_int32),
         ("mac", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 2),
+        ("eps_from_h", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 1),
         ("gamma", ctypes.c_double),
         ("alpha", ctypes.c_double),
         ("beta", ctypes.c_double),

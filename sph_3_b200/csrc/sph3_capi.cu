@@ -135,6 +135,7 @@ void params_from(const sph3_config &cfg, Params &P) {
     P.walk_warps = cfg.walk_warps;
     P.list_cap = cfg.precision == SPH3_PREC_MIXED ? cfg.list_cap : 0;
     P.mac = cfg.mac;
+    P.eps_from_h = cfg.eps_from_h;
     P.gamma = cfg.gamma;
     P.alpha = cfg.alpha;
     P.beta = cfg.beta;
@@ -163,6 +164,7 @@ int validate(const sph3_config *c) {
     if (c->max_level < 4 || c->max_level > 21) return SPH3_ERR_INVALID_ARG;
     if (c->list_cap < 0 || c->list_cap > 1024 || c->list_cap % 8) return SPH3_ERR_INVALID_ARG;
     if (c->mac != SPH3_MAC_BH && c->mac != SPH3_MAC_BH_OFFSET) return SPH3_ERR_INVALID_ARG;
+    if (c->eps_from_h != 0 && c->eps_from_h != 1) return SPH3_ERR_INVALID_ARG;
     if (c->stack_cap < 7 * (c->max_level + 2) + 32 || c->stack_cap > 4096) return SPH3_ERR_INVALID_ARG;
     if (!(c->theta >= 0.0) || !(c->eps > 0.0) || !(c->gamma >= 1.0)) return SPH3_ERR_INVALID_ARG;
     for (int d = 0; d < 3; ++d)
@@ -485,7 +487,7 @@ int sync_packs(sph3_ctx *c, cudaStream_t st, bool for_step = false) {
         c->h_dirty_tree = false;
     }
     if (c->h_dirty_tree) {
-        launch_tree_refit_h(c->S, st);
+        launch_tree_refit_h(c->S, c->P, st);
         c->h_dirty_tree = false;
     }
     return check_launch();
@@ -528,7 +530,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
     launch_tree_build(S, P, st);
     record(c, 4, st);
     launch_h_search(S, P, st);
-    launch_tree_refit_h(S, st);
+    launch_tree_refit_h(S, P, st);
     record(c, 5, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
     record(c, 6, st);
@@ -970,7 +972,7 @@ int sph3_first_step(sph3_ctx *c, double dt, void *stream) {
     CK(cudaStreamSynchronize(st));
     if (!(h0[0] > 0.0)) launch_boot_h(S, P, st);
     launch_h_search(S, P, st);
-    launch_tree_refit_h(S, st);
+    launch_tree_refit_h(S, P, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
     if (P.gravity) launch_gravity(S, P, st);
     else cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st);

@@ -155,6 +155,7 @@ struct Params {
     int walk_warps;  // warps per walk block (1, 2, 4 or 8)
     int list_cap;    // neighbour-list slots (0: the hydro pass walks)
     int mac;         // SPH3_MAC_*
+    int eps_from_h;  // eps = h after every h search
     double gamma, alpha, beta, eta, G, theta, eps;
     double box[3];
     int periodic;
@@ -279,7 +280,7 @@ void launch_pack(State &S, const Params &P, unsigned which, cudaStream_t st);
 void launch_identity_perm(State &S, cudaStream_t st);
 // tree.cu
 void launch_tree_build(State &S, const Params &P, cudaStream_t st);
-void launch_tree_refit_h(State &S, cudaStream_t st);
+void launch_tree_refit_h(State &S, const Params &P, cudaStream_t st);
 // walk_sph.cu
 void launch_boot_h(State &S, const Params &P, cudaStream_t st);
 void launch_h_search(State &S, const Params &P, cudaStream_t st);

@@ -324,8 +324,13 @@ __global__ void k_tree_totals(Tree T, int max_depth, unsigned long long *counter
 }
 
 // hmax of every node from the current h (after an h search), bottom-up
-__global__ void k_tree_refit_h(Tree T, const double *h, int d) {
+// Node hmax after the h search, bottom-up one depth per launch.  With eps = h
+// (eps_from_h) the softening maximum and the softening reach r_soft = bmax +
+// eps_max follow as well.
+__global__ void k_tree_refit_h(Tree T, const double *h, int d, int refit_eps, const uint64_t *key,
+                               const Cloud *clouds, int max_level) {
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+    const int cap = T.cap;
     for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const int2 r = T.range[i];
         const int2 ch = T.child[i];
@@ -339,13 +344,26 @@ __global__ void k_tree_refit_h(Tree T, const double *h, int d) {
         T.hmax[i] = hm;
         T.box_h[i].w = (float)(hm * (1.0 + 1e-6));
         T.sw[3 * i + 1].w = (float)(hm * (1.0 + 1e-6));
+        if (refit_eps && r.y > 0) {
+            T.epsmax[i] = hm;
+            const Cloud &cl = clouds[(int)(key[r.x] >> (3 * max_level))];
+            const double cx = T.com[i], cy = T.com[cap + i], cz = T.com[2 * cap + i];
+            const double ex = fmax(fabs(T.bmax[i] - cx), fabs(cx - T.bmin[i]));
+            const double ey = fmax(fabs(T.bmax[cap + i] - cy), fabs(cy - T.bmin[cap + i]));
+            const double ez = fmax(fabs(T.bmax[2 * cap + i] - cz), fabs(cz - T.bmin[2 * cap + i]));
+            const double bmax = sqrt(ex * ex + ey * ey + ez * ez);
+            const float r_soft = (float)fmin((bmax + hm) * (1.0 + 1e-5) + 1e-6 * cl.size, (double)FLT_MAX);
+            T.mono[i].z = r_soft;
+            T.gw[2 * i + 1].y = r_soft;
+        }
     }
 }
 
-void launch_tree_refit_h(State &S, cudaStream_t st) {
+void launch_tree_refit_h(State &S, const Params &P, cudaStream_t st) {
     if (S.ncloud == 0) return;
     const int blocks = S.num_sms * 4;
-    for (int d = S.max_level + 1; d >= 0; --d) k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d);
+    for (int d = S.max_level + 1; d >= 0; --d)
+        k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d, P.eps_from_h, S.key, S.clouds, S.max_level);
 }
 
 // ------------------------------------------------------------ walk groups

@@ -1342,6 +1342,14 @@ void launch_boot_h(State &S, const Params &P, cudaStream_t st) {
     run_walk(k_boot_h, A, walk_smem<V4<double>>(P), S, st, 0);
 }
 
+// eps = h (the reference GPU driver's set_eps_of_gas_to_h)
+__global__ void k_eps_from_h(int64_t n, const double *h, double *eps, float4 *pk_hme) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        eps[i] = h[i];
+        pk_hme[i].z = (float)h[i];
+    }
+}
+
 void launch_h_search(State &S, const Params &P, cudaStream_t st) {
     S.list_valid = false;  // new h: the supports change
     if (S.n == 0) return;
@@ -1363,6 +1371,10 @@ void launch_h_search(State &S, const Params &P, cudaStream_t st) {
             run_walk(k_h_search<float, SPH3_H_REFSTEP>, A, walk_smem<V4<float>>(P), S, st, 1);
         else
             run_walk(k_h_search_f32_newton, A, walk_smem<V4<float>>(P), S, st, 1);
+    }
+    if (P.eps_from_h) {
+        const int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8);
+        k_eps_from_h<<<blocks, 256, 0, st>>>(S.n, S.h, S.eps, S.pk_hme);
     }
 }
 
