@@ -349,26 +349,49 @@ __device__ __forceinline__ void put2(float4 &dst, int h, float a, float b) {
     p[2 + h] = b;
 }
 
-// the reference's softened kernel inside its support (r < 2 eps), scalar;
-// r2 = 0 (a particle and itself, or coincident particles) contributes nothing
-__device__ __forceinline__ void spline_near(float r2, float r, float e, float &fk, float &pk) {
-    if (r >= 2.f * e) return;
-    if (!(r2 > 0.f)) {
-        fk = 0.f;
-        pk = 0.f;
-        return;
+// The reference's softened kernel inside its support (r < 2 eps), for both
+// halves of a pair at once: the two polynomial pieces (q <= 1 and q <= 2,
+// written in Horner form) are evaluated packed and selected per half, so
+// lanes never diverge; halves outside the support keep the far values
+// (fk = 1/r^3, pk = 1/r), and r2 = 0 (a particle and itself, or coincident
+// particles) contributes nothing.  Same pieces as the FP64 path's
+// spline_force (sph_code/libsx.py:640-652 force, :609-616 potential).
+__device__ __forceinline__ void spline_near2(float2 r2, float2 r, float2 rinv, float2 e, float2 &fk, float2 &pk) {
+    const float2 ie = make_float2(__fdividef(1.f, e.x), __fdividef(1.f, e.y));
+    const float2 q = __fmul2_rn(r, ie);
+    const float2 q2 = __fmul2_rn(q, q);
+    const float2 q3 = __fmul2_rn(q2, q);
+    const float2 ie3 = __fmul2_rn(__fmul2_rn(ie, ie), ie);
+    // q <= 1: fk = ie^3 (4/3 + q^2 (-6/5 + q/2)), pk = ie (7/5 + q^2 (-2/3 + q^2 (3/10 - q/10)))
+    float2 t = __ffma2_rn(q, f2(0.5f), f2(-1.2f));
+    t = __ffma2_rn(q2, t, f2(4.f / 3.f));
+    const float2 fk1 = __fmul2_rn(ie3, t);
+    float2 u = __ffma2_rn(q, f2(-0.1f), f2(0.3f));
+    u = __ffma2_rn(q2, u, f2(-2.f / 3.f));
+    u = __ffma2_rn(q2, u, f2(1.4f));
+    const float2 pk1 = __fmul2_rn(ie, u);
+    // 1 < q <= 2: fk = r^-3 (-1/15 + q^3 (8/3 + q (-3 + q (6/5 - q/6)))),
+    //             pk = -r^-1/15 + ie (8/5 - q^2 (4/3 + q (-1 + q (3/10 - q/30))))
+    float2 v = __ffma2_rn(q, f2(-1.f / 6.f), f2(1.2f));
+    v = __ffma2_rn(q, v, f2(-3.f));
+    v = __ffma2_rn(q, v, f2(8.f / 3.f));
+    v = __ffma2_rn(q3, v, f2(-1.f / 15.f));
+    const float2 fk2 = __fmul2_rn(fk, v);  // fk holds r^-3 on entry
+    float2 w = __ffma2_rn(q, f2(-1.f / 30.f), f2(0.3f));
+    w = __ffma2_rn(q, w, f2(-1.f));
+    w = __ffma2_rn(q, w, f2(4.f / 3.f));
+    const float2 x = __ffma2_rn(__fmul2_rn(q2, f2(-1.f)), w, f2(1.6f));
+    const float2 pk2 = __ffma2_rn(ie, x, __fmul2_rn(rinv, f2(-1.f / 15.f)));
+    // select per half
+    if (!(r.x >= 2.f * e.x)) {
+        const bool z = !(r2.x > 0.f);
+        fk.x = z ? 0.f : (q.x <= 1.f ? fk1.x : fk2.x);
+        pk.x = z ? 0.f : (q.x <= 1.f ? pk1.x : pk2.x);
     }
-    const float ie = 1.f / e;
-    const float q = r * ie;
-    const float q2 = q * q, q3 = q2 * q;
-    if (q <= 1.f) {
-        fk = ie * ie * ie * (4.f / 3.f - 6.f / 5.f * q2 + 0.5f * q3);
-        pk = -2.f * ie * (1.f / 3.f * q2 - 3.f / 20.f * q2 * q2 + 1.f / 20.f * q2 * q3) + 7.f / 5.f * ie;
-    } else {
-        const float rinv = 1.f / r;
-        const float q4 = q2 * q2;
-        fk = rinv * rinv * rinv * (-1.f / 15.f + 8.f / 3.f * q3 - 3.f * q4 + 6.f / 5.f * q4 * q - 1.f / 6.f * q3 * q3);
-        pk = -1.f / 15.f * rinv - ie * (4.f / 3.f * q2 - q3 + 3.f / 10.f * q4 - 1.f / 30.f * q4 * q) + 8.f / 5.f * ie;
+    if (!(r.y >= 2.f * e.y)) {
+        const bool z = !(r2.y > 0.f);
+        fk.y = z ? 0.f : (q.y <= 1.f ? fk1.y : fk2.y);
+        pk.y = z ? 0.f : (q.y <= 1.f ? pk1.y : pk2.y);
     }
 }
 
@@ -526,10 +549,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
                 float2 pk = rinv;
                 // NaN-safe: r2 = 0 gives r = NaN, which lands in the near branch
                 const bool near = active && (!(r.x >= 2.f * eij.x) || !(r.y >= 2.f * eij.y));
-                if (__any_sync(kFull, near)) {
-                    spline_near(r2.x, r.x, eij.x, fk.x, pk.x);
-                    spline_near(r2.y, r.y, eij.y, fk.y, pk.y);
-                }
+                if (__any_sync(kFull, near)) spline_near2(r2, r, rinv, eij, fk, pk);
                 const float2 mf = __fmul2_rn(m, fk);
                 ax = __ffma2_rn(mf, dx, ax);
                 ay = __ffma2_rn(mf, dy, ay);
