@@ -248,6 +248,17 @@ int sph3_gravity_direct_rows(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, 
  * order: row k's set is idx[offsets[k] .. offsets[k+1]).  offsets has nrows+1
  * entries; at most cap indices are written (SPH3_STATUS_LIST_OVERFLOW past
  * it).  Host buffers. */
+/* The pairs the mixed path's hydro pass runs for the listed rows: the
+ * neighbour lists the last density pass kept (|r_ij| <= h_i + h_j tested in
+ * FP32 on cell-relative positions), as caller's indices in ascending order,
+ * laid out as in sph3_neighbours.  A row with more pairs than list_cap gives
+ * its first list_cap (its hydro terms come from a walk).  SPH3_ERR_STATE when
+ * no valid lists exist (FP64 precision, list_cap = 0, or no density pass since
+ * positions or h changed).  No reference counterpart: it states how the
+ * mixed-precision pair sets differ from the exact ones. */
+int sph3_pair_lists(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *offsets, int64_t *idx,
+                    int64_t cap);
+
 int sph3_neighbours(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *offsets,
                     int64_t *idx, int64_t cap);
 

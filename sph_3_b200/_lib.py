@@ -100,6 +100,7 @@ SIGNATURES = {
     "sph3_status": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_gravity_direct_rows": (ctypes.c_int, [P, P, I64, P, P]),
     "sph3_neighbours": (ctypes.c_int, [P, P, I64, P, P, I64]),
+    "sph3_pair_lists": (ctypes.c_int, [P, P, I64, P, P, I64]),
     "sph3_morton_order": (ctypes.c_int, [P, P, P]),
     "sph3_counters": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_phase_times": (ctypes.c_int, [P, P, ctypes.c_int]),

@@ -302,6 +302,17 @@ class Context:
                                        cap), "neighbours")
         return [idx[off[k]:off[k + 1]].copy() for k in range(rows.size)]
 
+    def pair_lists(self, rows, cap=None):
+        """The mixed path's kept pairs (sph3_pair_lists) of the listed rows, caller indices, ascending."""
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cap = int(cap if cap is not None else max(1, rows.size) * 1024)
+        off = np.zeros(rows.size + 1, dtype=np.int64)
+        idx = np.zeros(max(cap, 1), dtype=np.int64)
+        check(self.lib.sph3_pair_lists(self._ptr, rows.ctypes.data_as(ctypes.c_void_p), rows.size,
+                                       off.ctypes.data_as(ctypes.c_void_p), idx.ctypes.data_as(ctypes.c_void_p),
+                                       cap), "pair_lists")
+        return [idx[off[k]:off[k + 1]].copy() for k in range(rows.size)]
+
     def morton_order(self):
         order = np.zeros(self.n, dtype=np.int64)
         keys = np.zeros(self.n, dtype=np.uint64)

@@ -1177,6 +1177,38 @@ int sph3_neighbours(sph3_ctx *c, const int64_t *rows, int64_t nrows, int64_t *of
     return rc;
 }
 
+int sph3_pair_lists(sph3_ctx *c, const int64_t *rows, int64_t nrows, int64_t *offsets, int64_t *idx, int64_t cap) {
+    if (!c || nrows < 0 || !offsets || (nrows > 0 && !rows) || cap < 0 || (cap > 0 && !idx))
+        return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    offsets[0] = 0;
+    if (nrows == 0) return SPH3_OK;
+    State &S = c->S;
+    if (!S.list_valid || S.list_cap == 0) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    std::vector<int64_t> srt;
+    int rc = rows_to_sorted(c, rows, nrows, srt);
+    if (rc) return rc;
+    std::vector<int64_t> orig(S.n);
+    CK(cudaMemcpyAsync(orig.data(), S.orig, sizeof(int64_t) * S.n, cudaMemcpyDeviceToHost, st));
+    std::vector<int> cnt(nrows), row(S.list_cap);
+    for (int64_t r = 0; r < nrows; ++r)
+        CK(cudaMemcpyAsync(&cnt[r], S.nlist + srt[r], sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int64_t pos = 0;
+    for (int64_t r = 0; r < nrows; ++r) {
+        const int k = std::min(cnt[r], S.list_cap);
+        CK(cudaMemcpy(row.data(), S.list + (size_t)srt[r] * S.list_cap, sizeof(int) * k, cudaMemcpyDeviceToHost));
+        const int64_t b = pos;
+        for (int s = 0; s < k; ++s, ++pos)
+            if (pos < cap) idx[pos] = orig[row[s]];
+        std::sort(idx + std::min(b, cap), idx + std::min(pos, cap));
+        offsets[r + 1] = pos;
+    }
+    return SPH3_OK;
+}
+
 int sph3_morton_order(sph3_ctx *c, int64_t *order, uint64_t *keys) {
     if (!c) return SPH3_ERR_INVALID_ARG;
     if (!c->have) return SPH3_ERR_STATE;
