@@ -417,7 +417,7 @@ def main():
         import torch
         import torch.distributed as td
         torch.cuda.set_device(local_rank)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
     else:

@@ -152,11 +152,13 @@ typedef struct sph3_config {
     int32_t use_graph;   /* 1: sph3_step replays a captured CUDA graph */
     int32_t timing;      /* 1: record per-phase CUDA events (no graph) */
     int32_t walk_warps;  /* warps per walk block: 1, 2, 4 (default) or 8; each warp walks one group of <= 32 particles */
-    int32_t list_cap;    /* mixed precision: neighbour-list slots per particle that the density walk keeps
-                          * for the hydro pass (default 128; 0 = the hydro pass walks the tree).  The lists
-                          * hold exactly the pairs inside the support (|r| <= h_i + h_j); a particle with
-                          * more neighbours than list_cap is handled by a walk.  4 * list_cap bytes per
-                          * particle; a multiple of 8 in 0..1024. */
+    int32_t list_cap;    /* neighbour-list slots per particle that the density walk keeps for the hydro
+                          * pass (default 128; 0 = the hydro pass walks the tree).  The lists hold exactly
+                          * the pairs inside the support (|r| <= h_i + h_j, tested in the precision of the
+                          * path); a particle with more neighbours than list_cap is handled by a walk.  In
+                          * FP64 the list pass runs the walk's arithmetic in the walk's pair order, so its
+                          * results equal the walk's.  4 * list_cap bytes per particle; a multiple of 8 in
+                          * 0..1024. */
     int32_t mac;         /* multipole acceptance: SPH3_MAC_BH (d > s/theta, the default) or
                           * SPH3_MAC_BH_OFFSET (d > s/theta + |com - box centre|, more conservative) */
     int32_t eps_from_h;  /* 1: gravitational softening eps = h after every h search, as the reference GPU

@@ -54,7 +54,7 @@ class Config:
     use_graph: bool = True
     timing: bool = False
     walk_warps: int = 4            # warps per walk block (1, 2, 4, 8)
-    list_cap: int = 128            # mixed: neighbour-list slots per particle for the hydro pass (0: walk)
+    list_cap: int = 128            # neighbour-list slots per particle for the hydro pass (0: walk)
     mac: str = "bh"                # multipole acceptance: "bh" (d > s/theta) | "bh_offset" (+ com offset)
     eps_from_h: bool = False       # softening eps = h after every h search (reference GPU driver option)
     gamma: float = 5.0 / 3.0

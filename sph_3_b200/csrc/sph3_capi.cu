@@ -133,7 +133,7 @@ void params_from(const sph3_config &cfg, Params &P) {
     P.gravity = cfg.gravity;
     P.quadrupole = cfg.quadrupole;
     P.walk_warps = cfg.walk_warps;
-    P.list_cap = cfg.precision == SPH3_PREC_MIXED ? cfg.list_cap : 0;
+    P.list_cap = cfg.list_cap;
     P.mac = cfg.mac;
     P.eps_from_h = cfg.eps_from_h;
     P.gamma = cfg.gamma;

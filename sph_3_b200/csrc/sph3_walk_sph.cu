@@ -889,6 +889,49 @@ struct YE {
     V4<R> p, v, t;
 };
 
+// One hydro pair, after the pair geometry (d = r_i - r_j, |d|, hbar_ij,
+// q = |d| / hbar_ij): the reference's acceleration and du/dt terms
+// (sph_code/libsx.py:117-165, :364-417; MG83 :236-246; Balsara
+// sph_code/shear.py:193-215) and the pair's signal velocity.  sv = {vx, vy,
+// vz, m} and st = {rho, P/rho^2, c, f} of the source.  Shared by the walk and
+// the list passes, so both run the same arithmetic.
+template <typename R, int VISC, bool ACC, bool DU>
+__device__ __forceinline__ void hydro_pair(R dx, R dy, R dz, R rr, R hij, R q, R tvx, R tvy, R tvz, R trho, R tpr,
+                                           R tc, R tf, const V4<R> &sv, const V4<R> &st, R alpha, R beta, R eta2,
+                                           R &ax, R &ay, R &az, R &du, R &vmax) {
+    const R ih = fdiv((R)1, hij);
+    const R ih5 = ih * ih * ih * ih * ih;
+    R nW;
+    if (q <= (R)1) nW = (R)kSig * ih5 * ((R)-3 + (R)2.25 * q);
+    else { const R tq = (R)2 - q; nW = fdiv((R)(-0.75 * kSig) * ih5 * tq * tq, q + (R)1e-20); }
+    const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+    const R vx = tvx - sv.x, vy = tvy - sv.y, vz = tvz - sv.z;
+    const R vr = vx * dx + vy * dy + vz * dz;
+    const R rhoij = (R)0.5 * (trho + st.x);
+    R PI = 0;
+    R vsig;  // signal velocity (time-step estimate)
+    if (VISC == SPH3_VISC_MG83) {
+        const R cij = (R)0.5 * (tc + st.z);
+        const R mu = fdiv(hij * vr, rr * rr + hij * hij * eta2);
+        if (vr <= (R)0) PI = fdiv(-alpha * cij * mu + beta * mu * mu, rhoij);
+        if (ACC) vsig = tc + st.z - (R)3 * fdiv(vr, rr + (R)1e-5);
+    } else {
+        const R w = fdiv(vr, rr + (R)1e-5);
+        vsig = tc + st.z - (R)3 * w;
+        if (vr <= (R)0) PI = fdiv((R)-0.5 * alpha * vsig * w, rhoij);
+        if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + st.w) * PI;
+    }
+    if (ACC && vsig > vmax) vmax = vsig;
+    const R mj = sv.w;
+    if (ACC) {
+        const R pt = mj * (tpr + st.y + PI);
+        ax -= pt * gx;
+        ay -= pt * gy;
+        az -= pt * gz;
+    }
+    if (DU) du += mj * (tpr + (R)0.5 * PI) * (vx * gx + vy * gy + vz * gz);
+}
+
 template <typename R, int VISC, bool ACC, bool DU>
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1004,37 +1047,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
                         q = (R)((float)rr * __fdividef(1.0f, (float)hij));
                     }
                     (void)in;
-                    const R ih = fdiv((R)1, hij);
-                    const R ih5 = ih * ih * ih * ih * ih;
-                    R nW;
-                    if (q <= (R)1) nW = (R)kSig * ih5 * ((R)-3 + (R)2.25 * q);
-                    else { const R tq = (R)2 - q; nW = fdiv((R)(-0.75 * kSig) * ih5 * tq * tq, q + (R)1e-20); }
-                    const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
-                    const R vx = tvx - en.v.x, vy = tvy - en.v.y, vz = tvz - en.v.z;
-                    const R vr = vx * dx + vy * dy + vz * dz;
-                    const R rhoij = (R)0.5 * (trho + en.t.x);
-                    R PI = 0;
-                    R vsig;  // signal velocity (time-step estimate)
-                    if (VISC == SPH3_VISC_MG83) {
-                        const R cij = (R)0.5 * (tc + en.t.z);
-                        const R mu = fdiv(hij * vr, rr * rr + hij * hij * eta2);
-                        if (vr <= (R)0) PI = fdiv(-alpha * cij * mu + beta * mu * mu, rhoij);
-                        if (ACC) vsig = tc + en.t.z - (R)3 * fdiv(vr, rr + (R)1e-5);
-                    } else {
-                        const R w = fdiv(vr, rr + (R)1e-5);
-                        vsig = tc + en.t.z - (R)3 * w;
-                        if (vr <= (R)0) PI = fdiv((R)-0.5 * alpha * vsig * w, rhoij);
-                        if (VISC == SPH3_VISC_BALSARA) PI = (R)0.5 * (tf + en.t.w) * PI;
-                    }
-                    if (ACC && vsig > vmax) vmax = vsig;
-                    const R mj = en.v.w;
-                    if (ACC) {
-                        const R pt = mj * (tpr + en.t.y + PI);
-                        ax -= pt * gx;
-                        ay -= pt * gy;
-                        az -= pt * gz;
-                    }
-                    if (DU) du += mj * (tpr + (R)0.5 * PI) * (vx * gx + vy * gy + vz * gz);
+                    hydro_pair<R, VISC, ACC, DU>(dx, dy, dz, rr, hij, q, tvx, tvy, tvz, trho, tpr, tc, tf, en.v, en.t,
+                                                 alpha, beta, eta2, ax, ay, az, du, vmax);
                 }
             };
             auto flush = [&](int nl) {
@@ -1081,6 +1095,10 @@ struct LArgs {
     double *acc_sph, *dudt, *vsig;
     float alpha, beta, eta2;
     unsigned long long *counters;
+    // FP64 path: the masters
+    const double *pos, *vel, *h, *m, *rho, *P, *c, *bal;
+    double boxd[3];
+    double alpha_d, beta_d, eta2_d;
 };
 
 // one 48-byte record per source: everything a hydro pair reads from it, in
@@ -1146,39 +1164,10 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
             const float rr = sqrtf(d2);
             const float hij = 0.5f * hs;
             const float q = rr * __fdividef(1.0f, hij);
-            const float ih = __fdividef(1.0f, hij);
-            const float ih5 = ih * ih * ih * ih * ih;
-            float nW;
-            if (q <= 1.f) nW = kSigF * ih5 * (-3.f + 2.25f * q);
-            else {
-                const float tq = 2.f - q;
-                nW = __fdividef((float)(-0.75 * kSig) * ih5 * tq * tq, q + 1e-20f);
-            }
-            const float gx = nW * dx, gy = nW * dy, gz = nW * dz;
-            const float vx = tv.x - r1.x, vy = tv.y - r1.y, vz = tv.z - r1.z;
-            const float vr = vx * dx + vy * dy + vz * dz;
-            const float rhoij = 0.5f * (tt.x + r2.x);
-            float PI = 0.f;
-            float vsig;  // signal velocity (time-step estimate)
-            if (VISC == SPH3_VISC_MG83) {
-                const float cij = 0.5f * (tt.z + r2.z);
-                const float mu = __fdividef(hij * vr, rr * rr + hij * hij * eta2);
-                if (vr <= 0.f) PI = __fdividef(-alpha * cij * mu + beta * mu * mu, rhoij);
-                if (ACC) vsig = tt.z + r2.z - 3.f * __fdividef(vr, rr + 1e-5f);
-            } else {
-                const float w = __fdividef(vr, rr + 1e-5f);
-                vsig = tt.z + r2.z - 3.f * w;
-                if (vr <= 0.f) PI = __fdividef(-0.5f * alpha * vsig * w, rhoij);
-                if (VISC == SPH3_VISC_BALSARA) PI = 0.5f * (tf + A.pk_thm[j].w) * PI;
-            }
-            if (ACC) vmax = fmaxf(vmax, vsig);
-            if (ACC) {
-                const float pt = mj * (tt.y + r2.y + PI);
-                ax -= pt * gx;
-                ay -= pt * gy;
-                az -= pt * gz;
-            }
-            if (DU) du += mj * (tt.y + 0.5f * PI) * (vx * gx + vy * gy + vz * gz);
+            const V4<float> sv{r1.x, r1.y, r1.z, mj};
+            const V4<float> st{r2.x, r2.y, r2.z, VISC == SPH3_VISC_BALSARA ? A.pk_thm[j].w : 0.f};
+            hydro_pair<float, VISC, ACC, DU>(dx, dy, dz, rr, hij, q, tv.x, tv.y, tv.z, tt.x, tt.y, tt.z, tf, sv, st,
+                                             alpha, beta, eta2, ax, ay, az, du, vmax);
         }
         pairs += (unsigned long long)cnt;
         if (ACC) {
@@ -1188,6 +1177,60 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
             A.vsig[i] = (double)vmax;
         }
         if (DU) A.dudt[i] = (double)du;
+    }
+    pairs = warp_sum(pairs);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&A.counters[3], pairs);
+}
+
+// FP64 path over the same lists: the walk's FP64 pair arithmetic (the
+// reference's operation order, correctly rounded predicates) on the FP64
+// masters, with the periodic image the walk uses (source shifted by the
+// FP32-rounded box length), so the results equal the walk's.
+template <int VISC, bool ACC, bool DU>
+__global__ void __launch_bounds__(256) k_hydro_list_f64(LArgs A) {
+    unsigned long long pairs = 0;
+    const int64_t n = A.n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int cnt = A.nlist[i];
+        if (cnt > A.list_cap) continue;  // walked instead
+        const double tx = A.pos[i], ty = A.pos[n + i], tz = A.pos[2 * n + i], th = A.h[i];
+        const double tvx = A.vel[i], tvy = A.vel[n + i], tvz = A.vel[2 * n + i];
+        const double trho = A.rho[i], tpr = A.P[i] / (A.rho[i] * A.rho[i]), tc = A.c[i], tf = A.bal[i];
+        double ax = 0, ay = 0, az = 0, du = 0, vmax = 0;
+        const int *row = A.list + (size_t)i * A.list_cap;
+        for (int k = 0; k < cnt; ++k) {
+            const int j = row[k];
+            double pj[3] = {A.pos[j], A.pos[n + j], A.pos[2 * n + j]};
+            const double ti[3] = {tx, ty, tz};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double L = A.boxd[d];
+                if (L > 0.0) {
+                    const double dd = ti[d] - pj[d];
+                    if (dd > 0.5 * L) pj[d] += (double)(float)L;
+                    else if (dd < -0.5 * L) pj[d] += (double)(-(float)L);
+                }
+            }
+            const double ddx = __dsub_rn(tx, pj[0]);
+            const double ddy = __dsub_rn(ty, pj[1]);
+            const double ddz = __dsub_rn(tz, pj[2]);
+            const double drr = exact_dist(ddx, ddy, ddz);
+            const double dh = __dmul_rn(0.5, __dadd_rn(th, A.h[j]));
+            const double dq = __ddiv_rn(drr, dh);
+            const double rj = A.rho[j];
+            const V4<double> sv{A.vel[j], A.vel[n + j], A.vel[2 * n + j], A.m[j]};
+            const V4<double> st{rj, A.P[j] / (rj * rj), A.c[j], A.bal[j]};
+            hydro_pair<double, VISC, ACC, DU>(ddx, ddy, ddz, drr, dh, dq, tvx, tvy, tvz, trho, tpr, tc, tf, sv, st,
+                                              A.alpha_d, A.beta_d, A.eta2_d, ax, ay, az, du, vmax);
+        }
+        pairs += (unsigned long long)cnt;
+        if (ACC) {
+            A.acc_sph[i] = ax;
+            A.acc_sph[n + i] = ay;
+            A.acc_sph[2 * n + i] = az;
+            A.vsig[i] = vmax;
+        }
+        if (DU) A.dudt[i] = du;
     }
     pairs = warp_sum(pairs);
     if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&A.counters[3], pairs);
@@ -1412,7 +1455,13 @@ static void hydro_dispatch(const YArgs &A, bool acc, bool du, const Params &P, S
 }
 
 template <int V>
-static void list_dispatch(const LArgs &L, bool acc, bool du, int blocks, cudaStream_t st) {
+static void list_dispatch(const LArgs &L, bool fp64, bool acc, bool du, int blocks, cudaStream_t st) {
+    if (fp64) {
+        if (acc && du) k_hydro_list_f64<V, true, true><<<blocks, 256, 0, st>>>(L);
+        else if (acc) k_hydro_list_f64<V, true, false><<<blocks, 256, 0, st>>>(L);
+        else k_hydro_list_f64<V, false, true><<<blocks, 256, 0, st>>>(L);
+        return;
+    }
     if (acc && du) k_hydro_list<V, true, true><<<blocks, 256, 0, st>>>(L);
     else if (acc) k_hydro_list<V, true, false><<<blocks, 256, 0, st>>>(L);
     else k_hydro_list<V, false, true><<<blocks, 256, 0, st>>>(L);
@@ -1430,8 +1479,9 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
     A.list_cap = S.list_cap;
     A.only_overflow = 0;
     A.ovf = S.ovf;
-    if (P.precision != SPH3_PREC_FP64 && S.list_valid) {
+    if (S.list_valid) {
         // the list pass, then a walk for the particles whose lists overflowed
+        const bool fp64 = P.precision == SPH3_PREC_FP64;
         LArgs L;
         L.list = S.list; L.nlist = S.nlist; L.list_cap = S.list_cap;
         L.pk_pos = S.pk_pos; L.pk_hme = S.pk_hme; L.pk_vel = S.pk_vel; L.pk_thm = S.pk_thm;
@@ -1443,11 +1493,15 @@ void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cuda
         L.alpha = (float)P.alpha; L.beta = (float)P.beta; L.eta2 = (float)(P.eta * P.eta);
         L.counters = S.counters;
         L.hrec = S.hrec;
+        L.pos = S.pos; L.vel = S.vel; L.h = S.h; L.m = S.m; L.rho = S.rho; L.P = S.P; L.c = S.c; L.bal = S.bal;
+        for (int d = 0; d < 3; ++d) L.boxd[d] = P.box[d];
+        L.alpha_d = P.alpha; L.beta_d = P.beta; L.eta2_d = P.eta * P.eta;
         const int blocks = (int)std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 16);
-        k_pack_hrec<<<blocks, 256, 0, st>>>(L);
-        if (P.visc == SPH3_VISC_MG83) list_dispatch<SPH3_VISC_MG83>(L, want_acc, want_dudt, blocks, st);
-        else if (P.visc == SPH3_VISC_BALSARA) list_dispatch<SPH3_VISC_BALSARA>(L, want_acc, want_dudt, blocks, st);
-        else list_dispatch<SPH3_VISC_SIGNAL>(L, want_acc, want_dudt, blocks, st);
+        if (!fp64) k_pack_hrec<<<blocks, 256, 0, st>>>(L);
+        if (P.visc == SPH3_VISC_MG83) list_dispatch<SPH3_VISC_MG83>(L, fp64, want_acc, want_dudt, blocks, st);
+        else if (P.visc == SPH3_VISC_BALSARA)
+            list_dispatch<SPH3_VISC_BALSARA>(L, fp64, want_acc, want_dudt, blocks, st);
+        else list_dispatch<SPH3_VISC_SIGNAL>(L, fp64, want_acc, want_dudt, blocks, st);
         A.only_overflow = 1;
     }
     if (P.precision == SPH3_PREC_FP64) {
