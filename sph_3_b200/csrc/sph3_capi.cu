@@ -970,7 +970,11 @@ int sph3_first_step(sph3_ctx *c, double dt, void *stream) {
     std::vector<double> h0(1);
     CK(cudaMemcpyAsync(h0.data(), S.h, sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (!(h0[0] > 0.0)) launch_boot_h(S, P, st);
+    if (!(h0[0] > 0.0)) {
+        // the reference rule starts from its exact bootstrap; Newton needs only a start
+        if (P.h_mode == SPH3_H_REFSTEP) launch_boot_h(S, P, st);
+        else launch_h_guess(S, P, st);
+    }
     launch_h_search(S, P, st);
     launch_tree_refit_h(S, P, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);

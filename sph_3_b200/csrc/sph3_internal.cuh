@@ -281,6 +281,7 @@ void launch_identity_perm(State &S, cudaStream_t st);
 // tree.cu
 void launch_tree_build(State &S, const Params &P, cudaStream_t st);
 void launch_tree_refit_h(State &S, const Params &P, cudaStream_t st);
+void launch_h_guess(State &S, const Params &P, cudaStream_t st);
 // walk_sph.cu
 void launch_boot_h(State &S, const Params &P, cudaStream_t st);
 void launch_h_search(State &S, const Params &P, cudaStream_t st);

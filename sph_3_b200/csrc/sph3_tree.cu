@@ -366,6 +366,37 @@ void launch_tree_refit_h(State &S, const Params &P, cudaStream_t st) {
         k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d, P.eps_from_h, S.key, S.clouds, S.max_level);
 }
 
+// ------------------------------------------------------------ h start guess
+// A starting h for the Newton search when none is given: every particle of a
+// leaf gets the h at which a sphere of radius 2h would hold n_ngb particles
+// at the leaf's number density (its count over its octree cell's volume).
+// The search then converges in a few passes; the exact bootstrap of the
+// reference (k-th nearest neighbour, k_boot_h) stays for the reference rule.
+__global__ void k_h_guess(Tree T, const Cloud *clouds, const uint64_t *key, int max_level, int n_ngb, double *h,
+                          float4 *pk_hme) {
+    const int nn = T.depth_begin[max_level + 2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        const int2 r = T.range[i];
+        const int2 ch = T.child[i];
+        if ((ch.y & 255) != 0 || r.y == 0) continue;  // leaves only
+        const Cloud &cl = clouds[(int)(key[r.x] >> (3 * max_level))];
+        const int lvl = ch.y >> 8;
+        const double side = ldexp(cl.size, -lvl);
+        const double dens = (double)r.y / (side * side * side);
+        const double hg = 0.5 * cbrt(3.0 * (double)n_ngb / (4.0 * M_PI * dens));
+        for (int k = r.x; k < r.x + r.y; ++k) {
+            h[k] = hg;
+            pk_hme[k].x = (float)hg;
+        }
+    }
+}
+
+void launch_h_guess(State &S, const Params &P, cudaStream_t st) {
+    if (S.ncloud == 0 || S.n == 0) return;
+    S.list_valid = false;
+    k_h_guess<<<S.num_sms * 4, 256, 0, st>>>(S.tree, S.clouds, S.key, S.max_level, P.n_ngb, S.h, S.pk_hme);
+}
+
 // ------------------------------------------------------------ walk groups
 // Target groups for the walks: runs of at most kGroup consecutive particles
 // whose bounding box is small on the scale of their smoothing lengths (a
