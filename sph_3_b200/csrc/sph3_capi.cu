@@ -278,7 +278,7 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     CK(dalloc(&S.pk_vel, nn));
     CK(dalloc(&S.pk_thm, nn));
     CK(cudaMemset(S.pk_thm, 0, sizeof(float4) * nn));
-    c->cap_sortblk = (int)((nn + 2047) / 2048);
+    c->cap_sortblk = (int)((nn + kRsTileKeys - 1) / kRsTileKeys);
     CK(dalloc(&S.sort_hist, (size_t)256 * (c->cap_sortblk + 1)));
     const int cap = (int)std::min<int64_t>(2 * nn + ncloud + 64, (int64_t)INT32_MAX - 1);
     c->cap_nodes = cap;

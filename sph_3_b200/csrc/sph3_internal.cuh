@@ -46,6 +46,7 @@ constexpr int kBoxChunk = 4096;  // particles per root-cube reduction block
 // device counters (sph3_counters): 0..7 as documented in sph3.h, then walk
 // statistics
 constexpr int kRsOffsetThreads = 1024;  // threads of the one-block radix offset scan
+constexpr int kRsTileKeys = 4096;       // keys per radix-sort block (256 threads x 16)
 constexpr int kNumCounters = 16;
 constexpr int kCntVisitsH = 8;         // nodes popped by the h-search walks
 constexpr int kCntVisitsDensity = 9;   // ... density walks

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint64_t *key_in, cons
 namespace {
 
 constexpr int64_t kNoAllocMaxN = 65536;
-constexpr int kSortTile = 2048;  // keys per radix-sort block (as in sph3_sort.cu)
+constexpr int kSortTile = kRsTileKeys;  // keys per radix-sort block
 constexpr int64_t kMaxSortBlocks = kNoAllocMaxN / kSortTile;
 constexpr int64_t kMaxItems = (kNoAllocMaxN + kBoxChunk - 1) / kBoxChunk;
 

@@ -165,8 +165,8 @@ void launch_identity_perm(State &S, cudaStream_t st) {
 // within its tile with warp match (order = memory order inside a warp's
 // segment, then warp order).
 constexpr int kRsThreads = 256;
-constexpr int kRsItems = 8;
-constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys per block
+constexpr int kRsItems = kRsTileKeys / kRsThreads;
+constexpr int kRsTile = kRsThreads * kRsItems;
 constexpr int kRsWarps = kRsThreads / 32;
 
 __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t *key, int64_t n, int shift,
