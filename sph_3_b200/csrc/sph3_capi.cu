@@ -224,6 +224,16 @@ cudaError_t dalloc(T **p, size_t count) {
     return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
 }
 
+// a temporary device buffer freed on every return path
+template <typename T>
+struct DevTmp {
+    T *p = nullptr;
+    cudaError_t alloc(size_t count) { return dalloc(&p, count); }
+    ~DevTmp() {
+        if (p) cudaFree(p);
+    }
+};
+
 // neighbour lists of the mixed path: list_cap slots per particle (particle-major,
 // slot k of particle i at i * list_cap + k) and the count per particle
 int ensure_lists(sph3_ctx *c, int64_t nn) {
@@ -1126,22 +1136,19 @@ int sph3_gravity_direct_rows(sph3_ctx *c, const int64_t *rows, int64_t nrows, do
     int rc = rows_to_sorted(c, rows, nrows, srt);
     if (rc) return rc;
     cudaStream_t st = c->stream;
-    int64_t *drows = nullptr;
-    double *dacc = nullptr, *dphi = nullptr;
-    CK(cudaMalloc(&drows, sizeof(int64_t) * nrows));
-    CK(cudaMalloc(&dacc, sizeof(double) * 3 * nrows));
-    CK(cudaMalloc(&dphi, sizeof(double) * nrows));
-    CK(cudaMemcpyAsync(drows, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
-    launch_gravity_direct(c->S, c->P, drows, nrows, dacc, dphi, st);
+    DevTmp<int64_t> drows;
+    DevTmp<double> dacc, dphi;
+    CK(drows.alloc(nrows));
+    CK(dacc.alloc(3 * nrows));
+    CK(dphi.alloc(nrows));
+    CK(cudaMemcpyAsync(drows.p, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
+    launch_gravity_direct(c->S, c->P, drows.p, nrows, dacc.p, dphi.p, st);
     rc = check_launch();
     if (!rc) {
-        CK(cudaMemcpyAsync(acc, dacc, sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, st));
-        if (phi) CK(cudaMemcpyAsync(phi, dphi, sizeof(double) * nrows, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(acc, dacc.p, sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, st));
+        if (phi) CK(cudaMemcpyAsync(phi, dphi.p, sizeof(double) * nrows, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
     }
-    cudaFree(drows);
-    cudaFree(dacc);
-    cudaFree(dphi);
     return rc;
 }
 
@@ -1158,26 +1165,23 @@ int sph3_neighbours(sph3_ctx *c, const int64_t *rows, int64_t nrows, int64_t *of
     std::vector<int64_t> srt;
     rc = rows_to_sorted(c, rows, nrows, srt);
     if (rc) return rc;
-    int64_t *drows = nullptr, *doff = nullptr, *didx = nullptr;
-    CK(cudaMalloc(&drows, sizeof(int64_t) * nrows));
-    CK(cudaMalloc(&doff, sizeof(int64_t) * (nrows + 1)));
-    CK(cudaMalloc(&didx, sizeof(int64_t) * std::max<int64_t>(cap, 1)));
-    CK(cudaMemcpyAsync(drows, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
-    launch_neighbours(c->S, c->P, drows, nrows, doff, didx, cap, st);
+    DevTmp<int64_t> drows, doff, didx;
+    CK(drows.alloc(nrows));
+    CK(doff.alloc(nrows + 1));
+    CK(didx.alloc(std::max<int64_t>(cap, 1)));
+    CK(cudaMemcpyAsync(drows.p, srt.data(), sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
+    launch_neighbours(c->S, c->P, drows.p, nrows, doff.p, didx.p, cap, st);
     rc = check_launch();
     if (!rc) {
-        CK(cudaMemcpyAsync(offsets, doff, sizeof(int64_t) * (nrows + 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(offsets, doff.p, sizeof(int64_t) * (nrows + 1), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         const int64_t tot = std::min(offsets[nrows], cap);
-        if (tot > 0) CK(cudaMemcpy(idx, didx, sizeof(int64_t) * tot, cudaMemcpyDeviceToHost));
+        if (tot > 0) CK(cudaMemcpy(idx, didx.p, sizeof(int64_t) * tot, cudaMemcpyDeviceToHost));
         for (int64_t r = 0; r < nrows; ++r) {
             const int64_t b = std::min(offsets[r], cap), e = std::min(offsets[r + 1], cap);
             std::sort(idx + b, idx + e);
         }
     }
-    cudaFree(drows);
-    cudaFree(doff);
-    cudaFree(didx);
     return rc;
 }
 
