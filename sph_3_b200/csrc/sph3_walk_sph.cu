@@ -260,7 +260,10 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                 }
             } else {
                 thr[0] = 2.0 * h;
-                thr[1] = 2.0 * h * (1.0 + kNewtonDelta);
+                // the first pass counts at 2h only (a smaller reach: most groups
+                // are already in the window with the previous step's h); later
+                // passes also count at 2h (1 + delta) for the measured slope
+                thr[1] = pass == 0 ? thr[0] : 2.0 * h * (1.0 + kNewtonDelta);
             }
             float reach = 0.f;
             if (!conv) {
@@ -373,7 +376,8 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                     if (n0 == 0) {
                         hn = 2.0 * h;
                     } else {
-                        double sl = n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
+                        // slope of ln N over ln h: measured, or 3 (uniform density) on the first pass
+                        double sl = pass > 0 && n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
                         sl = fmin(fmax(sl, 1.0), 6.0);
                         hn = h * exp((log((double)A.n_ngb) - log((double)n0)) / sl);
                     }
