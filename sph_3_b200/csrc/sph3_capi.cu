@@ -180,7 +180,7 @@ void free_buffers(sph3_ctx *c) {
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.tree.bounds, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.tree.scan_tmp, S.tree.bounds, S.tree.parent, S.tree.arrive, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
                     S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -312,6 +312,9 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     CK(dalloc(&T.gw, 2 * (size_t)cap));
     CK(dalloc(&T.sw, 3 * (size_t)cap));
     CK(dalloc(&T.nchild_tmp, cap));
+    CK(dalloc(&T.parent, cap));
+    CK(dalloc(&T.arrive, cap));
+    CK(cudaMemset(T.arrive, 0, sizeof(int) * (size_t)cap));
     // a depth holds at most one node per particle
     CK(dalloc(&T.bounds, 8 * (size_t)(nn + ncloud + 64)));
     // scan_tmp doubles as depth_begin (+64) and scratch counters

@@ -93,6 +93,8 @@ struct Tree {
     int *nchild_tmp;    // [cap] scan input
     int *scan_tmp;      // [cap] scan output
     int *bounds;        // [8][n + ncloud + 64] octant starts of one depth's nodes
+    int *parent;        // [cap] parent node (-1 for a root)
+    int *arrive;        // [cap] children finished in the bottom-up passes (zero between passes)
     int *total;         // [4] scratch counters
 };
 

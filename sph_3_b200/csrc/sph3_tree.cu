@@ -39,16 +39,20 @@ __global__ void k_tree_roots(Tree T, Cloud *clouds, int ncloud, const uint64_t *
     int lvl = count > 0 ? common_level(key[first], key[first + count - 1], max_level) : max_level;
     T.range[c] = make_int2(first, count);
     T.child[c] = make_int2(-1, lvl << 8);
+    T.parent[c] = -1;
     cl.root = c;
 }
 
 // Children of each node of depth d: one warp per node finds where each
 // 3-bit digit of the next level starts inside the node's sorted key run and
 // stores the 8 starts (-1 for an empty octant) in T.bounds; nchild_tmp gets
-// the number of non-empty octants (0 for a leaf).  Small runs are scanned
-// with coalesced loads (a digit starts where it differs from the previous
-// key's); large runs binary-search the 7 digit boundaries, one per lane.
-constexpr int kTreeScanMax = 1024;  // runs up to this size are scanned linearly
+// the number of non-empty octants (0 for a leaf).  Digits are non-decreasing
+// inside a run, so the start of digit g is the first index whose digit is
+// >= g.  Runs of up to 128 keys are read whole (4 coalesced loads per lane)
+// and each start is the run start plus a ballot count; longer runs are
+// searched 5-ary, 4 lanes per digit probing 4 points per round (about
+// log5(count) dependent rounds instead of log2).
+constexpr int kTreeScanMax = 128;  // runs up to this size are read whole
 
 __global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
@@ -58,39 +62,48 @@ __global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, 
     for (int i = beg + warp; i < end; i += nwarp) {
         const int2 r = T.range[i];
         const int lvl = T.child[i].y >> 8;
-        int *bnd = T.bounds + 8 * (size_t)(i - beg);
         if (!(r.y > leaf_size && lvl < max_level)) {
             if (lane == 0) T.nchild_tmp[i - beg] = 0;
             continue;
         }
         const int shift = 3 * (max_level - lvl - 1);
         const int s = r.x, e = r.x + r.y;
-        if (lane < 8) bnd[lane] = -1;
-        __syncwarp();
+        int first;  // lanes 0..7: first index of the run with digit >= lane
         if (r.y <= kTreeScanMax) {
-            for (int b = s; b < e; b += 32) {
-                const int k = b + lane;
-                int dg = -1, prev = -1;
-                if (k < e) {
-                    dg = (int)((key[k] >> shift) & 7u);
-                    prev = k > s ? (int)((key[k - 1] >> shift) & 7u) : -1;
+            int dg[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = s + 32 * q + lane;
+                dg[q] = k < e ? (int)((key[k] >> shift) & 7u) : 8;
+            }
+            first = s;
+#pragma unroll
+            for (int g = 1; g < 8; ++g) {
+                int below = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) below += __popc(__ballot_sync(kFull, dg[q] < g));
+                if (lane == g) first = s + below;
+            }
+        } else {
+            const int g = lane >> 2, sub = lane & 3;
+            int a = s, b = e;  // the answer for digit g lies in [a, b]
+            while (__any_sync(kFull, a < b)) {
+                const int p = a + (int)((long long)(b - a) * (sub + 1) / 5);  // a <= p < b when a < b
+                const bool pred = a < b && (int)((key[p] >> shift) & 7u) < g;
+                const int t = __popc((__ballot_sync(kFull, pred) >> (4 * g)) & 0xFu);
+                const int pl = __shfl_sync(kFull, p, 4 * g + (t > 0 ? t - 1 : 0));
+                const int pr = __shfl_sync(kFull, p, 4 * g + (t < 4 ? t : 3));
+                if (a < b) {
+                    if (t > 0) a = pl + 1;
+                    if (t < 4) b = pr;
                 }
-                if (k < e && dg != prev) bnd[dg] = k;  // each digit starts once
             }
-        } else if (lane < 8) {
-            // first index with digit >= lane (digits are non-decreasing)
-            int a = s, b = e;
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                if ((int)((key[mid] >> shift) & 7u) < lane) a = mid + 1;
-                else b = mid;
-            }
-            const int nxt = __shfl_down_sync(0xffu, a, 1, 8);
-            const int stop = lane == 7 ? e : nxt;
-            bnd[lane] = a < stop ? a : -1;
+            first = __shfl_sync(kFull, a, 4 * (lane & 7));
         }
-        __syncwarp();
-        const int v = lane < 8 ? bnd[lane] : -1;
+        const int nxt = __shfl_down_sync(kFull, first, 1);
+        const int stop = lane == 7 ? e : nxt;
+        const int v = lane < 8 && first < stop ? first : -1;
+        if (lane < 8) T.bounds[8 * (size_t)(i - beg) + lane] = v;
         const int nch = __popc(__ballot_sync(kFull, v >= 0));
         if (lane == 0) T.nchild_tmp[i - beg] = nch;
     }
@@ -98,19 +111,33 @@ __global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, 
 
 // exclusive scan of the child counts of depth d; sets depth_begin[d + 2]
 __global__ void __launch_bounds__(1024) k_tree_scan(Tree T, int d, unsigned *status) {
-    // chunks of 4096 counts: 4 consecutive per thread, coalesced
+    // chunks of 16384 counts: 16 consecutive per thread (four 16-byte loads in
+    // flight), so a depth of ~10^5 nodes takes a handful of rounds
+    constexpr int kPer = 16, kChunk = 1024 * kPer;
     __shared__ int warp_tot[32];
     __shared__ int carry_s;
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
     const int m = end - beg;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int carry = 0;
-    for (int base = 0; base < m; base += 4096) {
-        const int idx = base + threadIdx.x * 4;
-        int v[4];
+    for (int base = 0; base < m; base += kChunk) {
+        const int idx = base + threadIdx.x * kPer;
+        const bool whole = idx + kPer <= m;
+        int v[kPer];
+        if (whole) {
+            const int4 *src = reinterpret_cast<const int4 *>(T.nchild_tmp + idx);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] = idx + k < m ? T.nchild_tmp[idx + k] : 0;
-        const int s = v[0] + v[1] + v[2] + v[3];
+            for (int q = 0; q < kPer / 4; ++q) {
+                const int4 t = src[q];
+                v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) v[k] = idx + k < m ? T.nchild_tmp[idx + k] : 0;
+        }
+        int s = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) s += v[k];
         const int incl = warp_incl_scan(s);
         if (lane == 31) warp_tot[w] = incl;
         __syncthreads();
@@ -121,9 +148,19 @@ __global__ void __launch_bounds__(1024) k_tree_scan(Tree T, int d, unsigned *sta
         __syncthreads();
         int run = carry + warp_tot[w] + incl - s;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (idx + k < m) T.scan_tmp[idx + k] = run;
-            run += v[k];
+        for (int k = 0; k < kPer; ++k) {
+            const int x = v[k];
+            v[k] = run;
+            run += x;
+        }
+        if (whole) {
+            int4 *dst = reinterpret_cast<int4 *>(T.scan_tmp + idx);
+#pragma unroll
+            for (int q = 0; q < kPer / 4; ++q) dst[q] = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kPer; ++k)
+                if (idx + k < m) T.scan_tmp[idx + k] = v[k];
         }
         if (threadIdx.x == 1023) carry_s = run;
         __syncthreads();
@@ -152,23 +189,34 @@ __global__ void k_tree_emit(Tree T, const uint64_t *key, int d, int leaf_size, i
             continue;
         }
         const int cf = end + T.scan_tmp[i - beg];
-        T.child[i] = make_int2(cf, nch | (lvl << 8));
         const int2 r = T.range[i];
         const int e = r.x + r.y;
         const int4 *bq = reinterpret_cast<const int4 *>(T.bounds + 8 * (size_t)(i - beg));
         const int4 b0 = bq[0], b1 = bq[1];
         const int st[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-        int c = 0;
+        // all 16 key loads before any store, so they are in flight together
+        int stops[8];
+        uint64_t kf[8], kl[8];
 #pragma unroll
         for (int dg = 0; dg < 8; ++dg) {
-            if (st[dg] < 0) continue;
             int stop = e;
 #pragma unroll
             for (int q = 7; q > dg; --q)
                 if (st[q] >= 0) stop = st[q];
-            const int cl = common_level(key[st[dg]], key[stop - 1], max_level);
+            stops[dg] = stop;
+            kf[dg] = st[dg] >= 0 ? __ldg(key + st[dg]) : 0;
+            kl[dg] = st[dg] >= 0 ? __ldg(key + stop - 1) : 0;
+        }
+        T.child[i] = make_int2(cf, nch | (lvl << 8));
+        int c = 0;
+#pragma unroll
+        for (int dg = 0; dg < 8; ++dg) {
+            if (st[dg] < 0) continue;
+            const int stop = stops[dg];
+            const int cl = common_level(kf[dg], kl[dg], max_level);
             T.range[cf + c] = make_int2(st[dg], stop - st[dg]);
             T.child[cf + c] = make_int2(-1, cl << 8);
+            T.parent[cf + c] = i;
             ++c;
         }
     }
@@ -323,47 +371,76 @@ __global__ void k_tree_totals(Tree T, int max_depth, unsigned long long *counter
     if (blockIdx.x == 0 && threadIdx.x == 0) counters[6] = (unsigned long long)nn;
 }
 
+// Last-arrival climb: after finishing node c, a thread counts itself in at
+// c's parent; the thread that completes the parent's count (its children's
+// results are all written and fenced) goes on with the parent.  No thread
+// ever waits, and each internal node is done exactly once.  The counter is
+// put back to zero for the next pass.
+__device__ __forceinline__ int climb(const Tree &T, int c) {
+    const int p = T.parent[c];
+    if (p < 0) return -1;
+    __threadfence();
+    const int nch = T.child[p].y & 255;
+    if (atomicAdd(T.arrive + p, 1) != nch - 1) return -1;
+    __threadfence();
+    T.arrive[p] = 0;
+    return p;
+}
+
 // hmax of every node from the current h (after an h search), bottom-up
 // Node hmax after the h search, bottom-up one depth per launch.  With eps = h
 // (eps_from_h) the softening maximum and the softening reach r_soft = bmax +
 // eps_max follow as well.
-__global__ void k_tree_refit_h(Tree T, const double *h, int d, int refit_eps, const uint64_t *key,
-                               const Cloud *clouds, int max_level) {
-    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+__device__ void node_refit_h(const Tree &T, const double *h, int i, int refit_eps, const uint64_t *key,
+                             const Cloud *clouds, int max_level) {
     const int cap = T.cap;
-    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        const int2 r = T.range[i];
-        const int2 ch = T.child[i];
-        const int nch = ch.y & 255;
-        double hm = 0;
-        if (nch == 0) {
-            for (int k = r.x; k < r.x + r.y; ++k) hm = fmax(hm, h[k]);
-        } else {
-            for (int c = ch.x; c < ch.x + nch; ++c) hm = fmax(hm, T.hmax[c]);
-        }
-        T.hmax[i] = hm;
-        T.box_h[i].w = (float)(hm * (1.0 + 1e-6));
-        T.sw[3 * i + 1].w = (float)(hm * (1.0 + 1e-6));
-        if (refit_eps && r.y > 0) {
-            T.epsmax[i] = hm;
-            const Cloud &cl = clouds[(int)(key[r.x] >> (3 * max_level))];
-            const double cx = T.com[i], cy = T.com[cap + i], cz = T.com[2 * cap + i];
-            const double ex = fmax(fabs(T.bmax[i] - cx), fabs(cx - T.bmin[i]));
-            const double ey = fmax(fabs(T.bmax[cap + i] - cy), fabs(cy - T.bmin[cap + i]));
-            const double ez = fmax(fabs(T.bmax[2 * cap + i] - cz), fabs(cz - T.bmin[2 * cap + i]));
-            const double bmax = sqrt(ex * ex + ey * ey + ez * ez);
-            const float r_soft = (float)fmin((bmax + hm) * (1.0 + 1e-5) + 1e-6 * cl.size, (double)FLT_MAX);
-            T.mono[i].z = r_soft;
-            T.gw[2 * i + 1].y = r_soft;
+    const int2 r = T.range[i];
+    const int2 ch = T.child[i];
+    const int nch = ch.y & 255;
+    double hm = 0;
+    if (nch == 0) {
+        for (int k = r.x; k < r.x + r.y; ++k) hm = fmax(hm, h[k]);
+    } else {
+        for (int c = ch.x; c < ch.x + nch; ++c) hm = fmax(hm, __ldcg(T.hmax + c));
+    }
+    T.hmax[i] = hm;
+    T.box_h[i].w = (float)(hm * (1.0 + 1e-6));
+    T.sw[3 * i + 1].w = (float)(hm * (1.0 + 1e-6));
+    if (refit_eps && r.y > 0) {
+        T.epsmax[i] = hm;
+        const Cloud &cl = clouds[(int)(key[r.x] >> (3 * max_level))];
+        const double cx = T.com[i], cy = T.com[cap + i], cz = T.com[2 * cap + i];
+        const double ex = fmax(fabs(T.bmax[i] - cx), fabs(cx - T.bmin[i]));
+        const double ey = fmax(fabs(T.bmax[cap + i] - cy), fabs(cy - T.bmin[cap + i]));
+        const double ez = fmax(fabs(T.bmax[2 * cap + i] - cz), fabs(cz - T.bmin[2 * cap + i]));
+        const double bmax = sqrt(ex * ex + ey * ey + ez * ez);
+        const float r_soft = (float)fmin((bmax + hm) * (1.0 + 1e-5) + 1e-6 * cl.size, (double)FLT_MAX);
+        T.mono[i].z = r_soft;
+        T.gw[2 * i + 1].y = r_soft;
+    }
+}
+
+// one launch: a thread per leaf, then up the last-arrival chain (hmax is a
+// maximum, so the order in which children finish does not matter)
+__global__ void k_tree_refit_h(Tree T, const double *h, int max_depth, int refit_eps, const uint64_t *key,
+                               const Cloud *clouds, int max_level) {
+    const int nn = T.depth_begin[max_depth];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        if ((T.child[i].y & 255) != 0) continue;
+        node_refit_h(T, h, i, refit_eps, key, clouds, max_level);
+        int c = i;
+        for (int up = 0; up < max_depth; ++up) {
+            c = climb(T, c);
+            if (c < 0) break;
+            node_refit_h(T, h, c, refit_eps, key, clouds, max_level);
         }
     }
 }
 
 void launch_tree_refit_h(State &S, const Params &P, cudaStream_t st) {
     if (S.ncloud == 0) return;
-    const int blocks = S.num_sms * 4;
-    for (int d = S.max_level + 1; d >= 0; --d)
-        k_tree_refit_h<<<blocks, 128, 0, st>>>(S.tree, S.h, d, P.eps_from_h, S.key, S.clouds, S.max_level);
+    k_tree_refit_h<<<S.num_sms * 8, 128, 0, st>>>(S.tree, S.h, S.max_level + 2, P.eps_from_h, S.key, S.clouds,
+                                                   S.max_level);
 }
 
 // ------------------------------------------------------------ h start guess
