@@ -52,6 +52,19 @@ def test_config_struct_layout_matches_header(lib):
     assert cfg.eps == 0.01 and list(cfg.box) == [0.0, 0.0, 0.0] and list(cfg.reserved_d) == [0.0] * 4
 
 
+def test_ref_binding_config_matches_package_config(lib):
+    # the stand-alone ctypes stub (copied next to the reference's sph_code/)
+    # must declare the same struct as the package's own binding
+    from sph_3_b200 import ref_binding
+    a = [(n, getattr(_lib.Config, n).offset, getattr(_lib.Config, n).size) for n, _ in _lib.Config._fields_]
+    b = [(n, getattr(ref_binding.Config, n).offset, getattr(ref_binding.Config, n).size)
+         for n, _ in ref_binding.Config._fields_]
+    assert a == b and ctypes.sizeof(_lib.Config) == ctypes.sizeof(ref_binding.Config)
+    cfg = ref_binding.Config()
+    lib.sph3_default_config(ctypes.byref(cfg))
+    assert cfg.list_cap == 128 and cfg.stack_cap == 768 and cfg.theta == 0.5
+
+
 def test_invalid_arguments_rejected_without_device(lib):
     out = ctypes.c_void_p()
     cfg = _lib.default_config()
