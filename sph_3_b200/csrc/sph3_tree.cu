@@ -245,6 +245,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
         double hm = 0, em = 0;
         if (nch == 0) {
+#pragma unroll 4
             for (int k = r.x; k < r.x + r.y; ++k) {
                 const double mk = a.m[k];
                 const double x = a.pos[k], y = a.pos[n + k], z = a.pos[2 * n + k];
@@ -259,7 +260,12 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
                 em = fmax(em, a.eps[k]);
             }
         } else {
-            for (int c = ch.x; c < ch.x + nch; ++c) {
+            // fixed trip count with a guard: the loads of all children are
+            // issued together (a node has at most 8), same summation order
+#pragma unroll
+            for (int q8 = 0; q8 < 8; ++q8) {
+                if (q8 >= nch) continue;
+                const int c = ch.x + q8;
                 const double mc = T.mass[c];
                 M += mc;
                 sx += mc * T.com[c];
@@ -294,6 +300,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         double Q[6] = {0, 0, 0, 0, 0, 0};
         if (quad) {
             if (nch == 0) {
+#pragma unroll 4
                 for (int k = r.x; k < r.x + r.y; ++k) {
                     const double mk = a.m[k];
                     const double dx = a.pos[k] - cx, dy = a.pos[n + k] - cy, dz = a.pos[2 * n + k] - cz;
@@ -306,7 +313,10 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
                     Q[5] += mk * (3 * dz * dz - d2);
                 }
             } else {
-                for (int c = ch.x; c < ch.x + nch; ++c) {
+#pragma unroll
+                for (int q8 = 0; q8 < 8; ++q8) {
+                    if (q8 >= nch) continue;
+                    const int c = ch.x + q8;
                     const double mc = T.mass[c];
                     const double dx = T.com[c] - cx, dy = T.com[cap + c] - cy, dz = T.com[2 * cap + c] - cz;
                     const double d2 = dx * dx + dy * dy + dz * dz;
