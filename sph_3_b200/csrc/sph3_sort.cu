@@ -250,17 +250,28 @@ __global__ void __launch_bounds__(kRsOffsetThreads) k_rs_offsets(uint32_t *hist,
     if (q == 0) hist[(size_t)nblocks * 256 + d] = tot[d] - own;  // exclusive digit base
 }
 
+// Stable scatter of one tile.  Each key's rank inside the tile (digit
+// start in the tile + earlier warps' count of the digit + rank inside its
+// warp, in memory order) is computed with warp match; the tile is then
+// staged in shared memory in digit order, so that every digit's run leaves
+// as consecutive addresses (coalesced stores instead of one scattered 8-byte
+// store per key).  The output is the same as scattering each key directly.
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
                                                            const uint32_t *val_in, uint64_t *key_out,
                                                            uint32_t *val_out, int64_t n, int shift,
                                                            const uint32_t *hist, int nblocks) {
     __shared__ uint32_t wcnt[kRsWarps][256];
-    __shared__ uint32_t goff[256];
+    __shared__ uint32_t goff[256];  // output start of the tile's keys of digit d
+    __shared__ uint32_t toff[256];  // start of digit d inside the tile
+    __shared__ uint32_t wsum[kRsWarps];
+    __shared__ uint64_t stage[kRsTile];  // keys in tile order, then the values
+    __shared__ uint8_t sdig[kRsTile];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
     goff[threadIdx.x] = hist[nblocks * 256 + threadIdx.x] + hist[blockIdx.x * 256 + threadIdx.x];
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (kRsItems * 32);
+    const int64_t tile = (int64_t)blockIdx.x * kRsTile;
+    const int64_t base = tile + (int64_t)w * (kRsItems * 32);
     uint64_t kk[kRsItems];
     uint32_t vv[kRsItems];
     uint32_t rank[kRsItems];
@@ -282,7 +293,8 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
         rank[t] = b + __popc(peers & lt);
     }
     __syncthreads();
-    // prefix over warps for each digit
+    // prefix over warps for each digit, and the tile's count of the digit
+    uint32_t cnt_d;
     {
         const int d = threadIdx.x;
         uint32_t run = 0;
@@ -292,16 +304,44 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
             wcnt[ww][d] = run;
             run += c;
         }
+        cnt_d = run;
+    }
+    // exclusive scan of the digit counts over the tile (256 threads = 256 digits)
+    {
+        const uint32_t incl = (uint32_t)warp_incl_scan((int)cnt_d);
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        uint32_t pre = 0;
+#pragma unroll
+        for (int ww = 0; ww < kRsWarps; ++ww) pre += ww < w ? wsum[ww] : 0u;
+        toff[threadIdx.x] = pre + incl - cnt_d;
     }
     __syncthreads();
+    uint32_t lpos[kRsItems];
 #pragma unroll
     for (int t = 0; t < kRsItems; ++t) {
-        int d = dig[t];
+        const int d = dig[t];
         if (d < 256) {
-            uint32_t pos = goff[d] + wcnt[w][d] + rank[t];
-            key_out[pos] = kk[t];
-            val_out[pos] = vv[t];
+            lpos[t] = toff[d] + wcnt[w][d] + rank[t];
+            stage[lpos[t]] = kk[t];
+            sdig[lpos[t]] = (uint8_t)d;
         }
+    }
+    __syncthreads();
+    const int cnt = (int)min((int64_t)kRsTile, n - tile);
+    for (int j = threadIdx.x; j < cnt; j += kRsThreads) {
+        const int d = sdig[j];
+        key_out[goff[d] + (uint32_t)j - toff[d]] = stage[j];
+    }
+    __syncthreads();
+    uint32_t *sval = reinterpret_cast<uint32_t *>(stage);
+#pragma unroll
+    for (int t = 0; t < kRsItems; ++t)
+        if (dig[t] < 256) sval[lpos[t]] = vv[t];
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += kRsThreads) {
+        const int d = sdig[j];
+        val_out[goff[d] + (uint32_t)j - toff[d]] = sval[j];
     }
 }
 
