@@ -221,6 +221,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- mixed (headline)
     ctx = setup("mixed")
+    free_b, total_b = torch.cuda.mem_get_info()
     clocks = Clocks(local_rank)
     e_start = ctx.energy()
     clocks.start()
@@ -374,6 +375,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": ck,
         "gpu_launches": kernels_per_step * args.steps if kernels_per_step > 0 else None,
         "gpu_launches_per_step": kernels_per_step,
+        "device_bytes_in_use": int(total_b - free_b),
         "cpu_baseline": cpu,
     }
     return line
