@@ -19,6 +19,7 @@ the same workload; rank 0 only.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -305,7 +306,16 @@ def run_ours(args, rank, world, local_rank):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     sm_mhz = ck.get("sm_mhz") or 1965.0
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp32_nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    try:  # measured on this GPU: packed-FP32 FMA chains on every SM
+        from sph_3_b200 import _lib
+        fp32_peak = _lib.probe_fp32_rate(local_rank, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        fp32_src = ("measured on this GPU: %.1f TFLOP/s of packed FP32 FMA chains (sph3_probe_fp32_rate); "
+                    "nominal at the sampled %.0f MHz: %.1f" % (fp32_peak, sm_mhz, fp32_nominal))
+    except Exception as exc:  # noqa: BLE001 - report the nominal rate instead
+        fp32_peak = fp32_nominal
+        fp32_src = ("nominal FP32 issue rate 148 SM x 128 lanes x 2 at the sampled median SM clock (%.0f MHz); "
+                    "the probe failed: %s" % (sm_mhz, exc))
     for k, msv in ph.items():
         bytes_alg = costs.BYTES.get(k, 0) * n
         kernels[k] = {"ms": msv, "share": msv / max(sum(ph.values()), 1e-9),
@@ -319,8 +329,7 @@ def run_ours(args, rank, world, local_rank):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=262144 launch "
                                   "(14.07 MB), scaled per particle to this N "
                                   "(profiles/k_gravity_f32_evrard262k.md)",
-                "peak_source": "nominal FP32 issue rate 148 SM x 128 lanes x 2 at the sampled median SM "
-                               "clock (%.0f MHz); MEASURED_PEAKS.json has no CUDA-core FP32 figure" % sm_mhz,
+                "peak_source": fp32_src + "; MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                 "work": "%.3g node + %.3g particle interactions per launch" % (cnt.get("grav_node", 0),
                                                                                cnt.get("grav_part", 0))}
     else:

@@ -304,6 +304,13 @@ int sph3_timestep(sph3_ctx *ctx, double c_cfl, int all_pairs, double *dt_min, vo
  * that benchmarks report. */
 int sph3_kernels_per_step(sph3_ctx *ctx, int64_t *out);
 
+/* Measured FP32 rate of GPU `device` in TFLOP/s: a grid of 8 blocks of 256
+ * threads per SM running independent FMA chains, packed (FFMA2) and scalar,
+ * each timed with CUDA events (about 20 ms in all); the larger rate.  No reference counterpart: it is the
+ * denominator benchmarks use for the walk kernels, which are bound by the FP32
+ * pipe rather than by HBM or the tensor cores. */
+int sph3_probe_fp32_rate(int device, double *tflops, void *stream);
+
 /* Morton sort that allocates no device memory -- it has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc: code running inside a
  * caller-owned pool or arena, or under a host framework that owns the

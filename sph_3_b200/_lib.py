@@ -105,6 +105,7 @@ SIGNATURES = {
     "sph3_counters": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_phase_times": (ctypes.c_int, [P, P, ctypes.c_int]),
     "sph3_kernels_per_step": (ctypes.c_int, [P, P]),
+    "sph3_probe_fp32_rate": (ctypes.c_int, [ctypes.c_int, P, P]),
     "sph3_timestep": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_int, P, P]),
     "sph3_morton_sort_noalloc": (ctypes.c_int, [P, I64, I32, P, P, P]),
 }
@@ -147,3 +148,11 @@ def default_config() -> Config:
     cfg = Config()
     load().sph3_default_config(ctypes.byref(cfg))
     return cfg
+
+
+def probe_fp32_rate(device: int = 0, stream=None) -> float:
+    """Measured FP32 rate (TFLOP/s) of GPU `device`: packed FMA chains on every
+    SM, timed with CUDA events (the walk kernels' roofline denominator)."""
+    v = ctypes.c_double()
+    check(load().sph3_probe_fp32_rate(int(device), ctypes.byref(v), stream), "probe_fp32_rate")
+    return float(v.value)

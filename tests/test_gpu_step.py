@@ -76,3 +76,14 @@ def test_energy_and_momentum_sums(oc):
     assert abs(e["U"] - float(np.sum(ic["m"] * ctx.get_field("u")))) < 1e-12
     assert abs(e["M"] - 1.0) < 1e-12
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_fp32_rate_probe_is_plausible():
+    """The measured FP32 rate used as the walk kernels' roofline denominator:
+    B200 nominal is 148 SM x 128 lanes x 2 flops x clock (74 TFLOP/s at
+    1965 MHz); the probe must land near it."""
+    from sph_3_b200 import _lib
+    r = _lib.probe_fp32_rate(0)
+    print("FP32 probe: %.1f TFLOP/s" % r)
+    assert 40.0 < r < 90.0
