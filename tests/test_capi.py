@@ -92,6 +92,11 @@ def test_no_gpu_fails_loudly(lib):
     from sph_3_b200 import Context, Sph3Error
     with pytest.raises(Sph3Error):
         Context()
+    # the roofline probe too: no CPU stand-in for a measured GPU rate
+    v = ctypes.c_double(-1.0)
+    assert lib.sph3_probe_fp32_rate(0, ctypes.byref(v), None) == _lib.C["SPH3_ERR_NO_DEVICE"]
+    assert v.value == -1.0
+    assert lib.sph3_probe_fp32_rate(0, None, None) == _lib.C["SPH3_ERR_INVALID_ARG"]
 
 
 def test_python_config_roundtrip(lib):
