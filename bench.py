@@ -133,16 +133,30 @@ def cpu_rows_time(ic, rows, n_ngb=64):
     return time.perf_counter() - t0
 
 
+def rows_for(ic, target_s, rng, threads):
+    """Rows whose CPU pass takes about target_s: a call has a fixed cost
+    (O(N) set-up of the derived arrays, thread start) of a few tenths of a
+    second, so the per-row cost is measured twice, the second time on a
+    sample large enough for that cost to be small."""
+    n = ic["pos"].shape[0]
+    k = min(n, max(4 * threads, 64))
+    t = cpu_rows_time(ic, rng.choice(n, k, replace=False))
+    k2 = int(min(n, max(k, 0.25 * target_s * k / max(t, 1e-9))))
+    if k2 > k:
+        t2 = cpu_rows_time(ic, rng.choice(n, k2, replace=False))
+        per_row = max(t2 - t * 0.5, 0.5 * t2) / k2  # discount part of the fixed cost
+    else:
+        per_row = t / k
+    return int(min(n, max(k, target_s / max(per_row, 1e-9))))
+
+
 def cpu_baseline(ic, target_s=12.0):
     import oracle as oc
     oc.build()
     threads = oc.num_threads()
     rng = np.random.default_rng(123)
     n = ic["pos"].shape[0]
-    probe = rng.choice(n, min(n, max(threads, 8)), replace=False)
-    t = cpu_rows_time(ic, probe)
-    per_row = t / probe.size
-    nrows = int(min(n, max(probe.size, target_s / max(per_row, 1e-9))))
+    nrows = rows_for(ic, target_s, rng, threads)
     rows = rng.choice(n, nrows, replace=False)
     t = cpu_rows_time(ic, rows)
     return {"value": nrows / t, "unit": "particle-updates/s", "cores": threads, "kind": "port",
@@ -403,9 +417,7 @@ def run_reference(args, rank, world):
     # cost does not depend on the h values beyond the iteration count
     ic["h"] = np.full(n, 0.5 * (64.0 / n) ** (1.0 / 3.0) * 1.2)
     ic["rho"] = np.full(n, 1.0)
-    probe = rng.choice(n, max(threads, 8), replace=False)
-    per_row = cpu_rows_time(ic, probe) / probe.size
-    rows_per_step = int(max(threads, min(n, 4.0 / max(per_row, 1e-9))))
+    rows_per_step = rows_for(ic, 4.0, rng, threads)
     for _ in range(args.warmup):
         cpu_rows_time(ic, rng.choice(n, max(threads, rows_per_step // 8), replace=False))
     t_tot = 0.0
