@@ -95,3 +95,65 @@ def serial_step(oc, st, dt, params=None):
     st["vel"] = st["vel"] + st["acc"] * dt / 2.0
     st["dudt"] = ut
     return st
+
+
+# ------------------------------------------------------------------ MPI order
+# sph_code/sph_mpi4_v4.py runs the same physics in another order and with
+# the Balsara-switched ("shear") viscosity: the first step (lines 150-263)
+# takes a_sph and du/dt with the same v; each loop iteration (lines 278-430)
+# kicks and drifts, then h, rho, a_g, P, c (old u), div/curl v, a_sph, kicks
+# with a = a_g + a_sph, and only then du/dt with the kicked v, followed by
+# u = u_prev + dt/2 (du/dt + du/dt_prev).
+
+def _shear(oc, st, f, want_acc, want_dudt, box):
+    dv, cv = oc.div_curl_rows(st["pos"], st["vel"], f["rho"], st["m"], f["h"], box=box)
+    acc, ut = oc.hydro_rows(st["pos"], st["vel"], f["rho"], f["P"], f["c"], f["h"], st["m"],
+                            oc.VISC_BALSARA, f["alpha"], f["beta"], f["eta"], divV=dv, curlV=cv, box=box,
+                            want_acc=want_acc, want_dudt=want_dudt)
+    return acc, ut, dv, cv
+
+
+def mpi4_first_step(oc, st, dt, params=None):
+    """Initial forces and the Euler u update of sph_mpi4_v4.py:150-263."""
+    st = {k: (np.array(v, dtype=np.float64, copy=True) if isinstance(v, np.ndarray) else v)
+          for k, v in st.items()}
+    if st.get("h") is None:
+        st["h"] = oc.smoothing_length_rows(st["pos"], k=_p(params, "n_boot", 50),
+                                           box=_p(params, "box", None))
+    f = _forces(oc, st, params)
+    acc_sph, ut, dv, cv = _shear(oc, st, f, True, True, f["box"])
+    st["h"] = f["h"]
+    st["rho"], st["P"], st["c"] = f["rho"], f["P"], f["c"]
+    st["divV"], st["curlV"] = dv, cv
+    st["acc_g"], st["acc_sph"] = f["acc_g"], acc_sph
+    st["acc"] = f["acc_g"] + acc_sph
+    st["u"] = st["u"] + ut * dt
+    st["u_prev"] = st["u"].copy()
+    st["ut_prev"] = ut.copy()
+    st["dudt"] = ut
+    return st
+
+
+def mpi4_step(oc, st, dt, params=None):
+    """One loop iteration of sph_mpi4_v4.py:278-430 on a copy of ``st``."""
+    st = {k: (np.array(v, dtype=np.float64, copy=True) if isinstance(v, np.ndarray) else v)
+          for k, v in st.items()}
+    box = _p(params, "box", None)
+    st["vel"] = st["vel"] + st["acc"] * dt / 2.0
+    st["pos"] = st["pos"] + st["vel"] * dt
+    f = _forces(oc, st, params)
+    acc_sph, _, dv, cv = _shear(oc, st, f, True, False, box)
+    st["acc_g"], st["acc_sph"] = f["acc_g"], acc_sph
+    st["acc"] = f["acc_g"] + acc_sph
+    st["vel"] = st["vel"] + st["acc"] * dt / 2.0
+    _, ut = oc.hydro_rows(st["pos"], st["vel"], f["rho"], f["P"], f["c"], f["h"], st["m"],
+                          oc.VISC_BALSARA, f["alpha"], f["beta"], f["eta"], divV=dv, curlV=cv, box=box,
+                          want_acc=False)
+    st["u"] = st["u_prev"] + 0.5 * dt * (ut + st["ut_prev"])
+    st["u_prev"] = st["u"].copy()
+    st["ut_prev"] = ut.copy()
+    st["h"] = f["h"]
+    st["rho"], st["P"], st["c"] = f["rho"], f["P"], f["c"]
+    st["divV"], st["curlV"] = dv, cv
+    st["dudt"] = ut
+    return st

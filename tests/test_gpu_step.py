@@ -8,9 +8,10 @@ from tests.conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _run_both(oc, n, steps, cfg_over, params, seed=3, dt=1e-3):
-    from oracle.step import serial_first_step, serial_step
+def _run_both(oc, n, steps, cfg_over, params, seed=3, dt=1e-3, order="serial"):
+    from oracle.step import mpi4_first_step, mpi4_step, serial_first_step, serial_step
     from sph_3_b200 import Config, Context
+    first, step = (serial_first_step, serial_step) if order == "serial" else (mpi4_first_step, mpi4_step)
     from sph_3_b200.ic import evrard
     ic = evrard(n, seed=seed)
     rng = np.random.default_rng(seed)
@@ -18,9 +19,9 @@ def _run_both(oc, n, steps, cfg_over, params, seed=3, dt=1e-3):
     eps = np.full(n, 0.01)
     h0 = oc.smoothing_length_rows(ic["pos"], k=params.get("n_boot", 50))
     st = dict(pos=ic["pos"], vel=ic["vel"], m=ic["m"], u=ic["u"], eps=eps, h=h0)
-    ref = serial_first_step(oc, st, dt, params)
+    ref = first(oc, st, dt, params)
     for _ in range(steps):
-        ref = serial_step(oc, ref, dt, params)
+        ref = step(oc, ref, dt, params)
     cfg = Config(**cfg_over)
     ctx = Context(cfg)
     ctx.set_particles(ic["pos"], ic["m"], vel=ic["vel"], u=ic["u"], h=h0, eps=eps)
@@ -39,6 +40,23 @@ def test_fp64_steps_match_reference_order(oc):
     ref, got, status = _run_both(oc, 1200, 3,
                                  dict(precision="fp64", h_mode="refstep", n_ngb=50, theta=0.0,
                                       h_max_iter=2000, use_graph=True), params)
+    assert status == 0
+    assert np.array_equal(got["h"], ref["h"])
+    for k in ("pos", "vel", "u", "rho"):
+        assert rel_err(got[k], ref[k]) < 1e-9, k
+    assert rel_err(got["acc"], ref["acc"], floor_frac=1e-3) < 1e-8
+    assert rel_err(got["dudt"], ref["dudt"], floor_frac=1e-3) < 1e-8
+
+
+def test_fp64_mpi4_order_balsara_matches_reference(oc):
+    """The MPI driver's order (sph_mpi4_v4.py: du/dt after the second kick)
+    with its Balsara-switched viscosity, FP64, exact gravity: three steps
+    agree with the oracle's composition of that driver to 1e-9."""
+    params = dict(n_ngb=50, gamma=5.0 / 3.0, alpha=1.0, beta=2.0, eta=0.1, G=1.0)
+    ref, got, status = _run_both(oc, 1200, 3,
+                                 dict(precision="fp64", h_mode="refstep", n_ngb=50, theta=0.0,
+                                      h_max_iter=2000, use_graph=True, step_order="mpi4", visc="balsara"),
+                                 params, seed=5, order="mpi4")
     assert status == 0
     assert np.array_equal(got["h"], ref["h"])
     for k in ("pos", "vel", "u", "rho"):
