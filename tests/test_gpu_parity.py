@@ -73,6 +73,34 @@ def test_gravity_fp64(golden, name):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_row_slice_variants_fp64(golden, name):
+    """The _mpi row-slice forms return rows [nbeg, nend) of the full fields
+    (the reference's per-rank calls), getAcc_g_smthx is the same field, and
+    the mimj partials of a row partition sum to the full gravity field."""
+    from sph_3_b200 import libsx, shear
+    g = golden(name)
+    gama, alpha, beta, eta, G = g["consts"]
+    n = g["pos"].shape[0]
+    b, e = n // 3, (2 * n) // 3
+    a = (g["pos"], g["vel"], g["rho"], g["P"], g["c"], g["h"], g["m"])
+    assert rel_err(libsx.getAcc_sph_mpi(b, e, *a, gama, eta, alpha, beta), g["acc_sph"][b:e]) < 1e-9
+    assert rel_err(libsx.get_dU_mpi(b, e, *a, gama, eta, alpha, beta), g["dudt"][b:e]) < 1e-9
+    dv, cv = shear.div_curlVel_mpi(b, e, g["pos"], g["vel"], g["rho"], g["m"], g["h"])
+    assert rel_err(dv, g["divV"][b:e]) < 1e-9 and rel_err(cv, g["curlV"][b:e]) < 1e-9
+    acc_sh = shear.getAcc_sph_shear_mpi(b, e, *a, g["divV"], g["curlV"], alpha)
+    assert rel_err(acc_sh, g["acc_sh"][b:e]) < 1e-9
+    du_sh = shear.get_dU_shear_mpi(b, e, *a, g["divV"], g["curlV"], alpha)
+    assert rel_err(du_sh, g["dudt_sh"][b:e]) < 1e-9
+    assert np.array_equal(libsx.getPressure(g["rho"], g["u"], gama), (gama - 1.0) * g["rho"] * g["u"])
+    libsx.configure(theta=0.0)
+    assert rel_err(libsx.getAcc_g_smth_mpi(b, e, g["pos"], g["m"], G, g["eps"]), g["acc_g"][b:e]) < 1e-10
+    assert rel_err(libsx.getAcc_g_smthx(g["pos"], g["m"], G, g["eps"]), g["acc_g"]) < 1e-10
+    parts = sum(libsx.getAcc_g_smth_mimj_mpi(p, q, g["pos"], g["m"], G, g["eps"])
+                for p, q in ((0, b), (b, e), (e, n)))
+    assert parts.shape == (n, 3) and rel_err(parts, g["acc_g"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_mixed_precision_errors(golden, name):
     """Mixed path (FP32 cell-relative pair arithmetic): rho within 1e-5,
     hydro acceleration and du/dt within 1e-4 (relative, floor 1 % of the
