@@ -397,10 +397,11 @@ __device__ __forceinline__ int climb(const Tree &T, int c) {
     return p;
 }
 
-// hmax of every node from the current h (after an h search), bottom-up
-// Node hmax after the h search, bottom-up one depth per launch.  With eps = h
-// (eps_from_h) the softening maximum and the softening reach r_soft = bmax +
-// eps_max follow as well.
+// Node hmax from the current h (after an h search): a leaf from its
+// particles, an internal node from its children (read through L2: they were
+// written by other threads of the same launch).  With eps = h (eps_from_h)
+// the softening maximum and the softening reach r_soft = bmax + eps_max
+// follow as well.
 __device__ void node_refit_h(const Tree &T, const double *h, int i, int refit_eps, const uint64_t *key,
                              const Cloud *clouds, int max_level) {
     const int cap = T.cap;
