@@ -15,6 +15,12 @@ value = total particles x steps / max over ranks of the timed region.
 --impl reference times the reference's CPU algorithm (the C restatement of
 sph_code/libsx.py in oracle/, all host threads) on a bounded row sample of
 the same workload; rank 0 only.
+
+--clouds K replaces the single cloud by a batched ensemble of K independent
+Evrard clouds (N log-uniform in [2048, 65536]) stepped by one launch
+sequence.  The roofline of the dominant kernel (the gravity walk, FP32-pipe
+bound) is taken against the FP32 rate measured on the same GPU in the same
+run (sph3_probe_fp32_rate).
 """
 from __future__ import annotations
 
