@@ -78,6 +78,8 @@ def _load():
         "orc_hydro": [I, P, P, P, P, P, P, P, P, P, C, D, D, D, P, I, P, P, P],
         "orc_grav_direct": [I, P, P, D, P, P, I, P, P],
         "orc_grav_sym": [I, P, P, D, P, P],
+        "orc_grav_mimj": [I, P, P, D, P, I, I, P],
+        "orc_smoothing_points": [I, P, I, P, C, P],
         "orc_pe": [I, P, P, D, P],
         "orc_ke": [I, P, P],
         "orc_timestep": [I, P, P, P, P, P, P, P, P, D, D, C, P, I, P, P],
@@ -208,11 +210,16 @@ def do_smoothingX(poz):
     subpos = _f64(subpos, (-1, 3))
     if subpos.shape == pos.shape and np.array_equal(subpos, pos):
         return smoothing_length_rows(pos)
-    out = np.zeros(subpos.shape[0])
-    for r in range(subpos.shape[0]):
-        d = pos - subpos[r]
-        out[r] = np.sort(np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2]))[50]
-    return out * 0.5
+    return smoothing_points(pos, subpos)
+
+
+def smoothing_points(pos, q, k=50):
+    """0.5 x the k-th (0-based) smallest distance from each row of q to the rows of pos."""
+    pos = _f64(pos, (-1, 3))
+    q = _f64(q, (-1, 3))
+    out = np.zeros(q.shape[0])
+    _load().orc_smoothing_points(pos.shape[0], _ptr(pos), q.shape[0], _ptr(q), int(k), _ptr(out))
+    return out
 
 
 def getPressure(rho, u, gama):
@@ -338,6 +345,14 @@ def getAcc_g_smth(pos, mass, G, epsilon):
     eps = np.broadcast_to(_f64(epsilon), (n,)).copy() if np.ndim(epsilon) == 0 else _f64(epsilon)
     out = np.zeros((n, 3))
     _load().orc_grav_sym(n, _ptr(pos), _ptr(mass), float(G), _ptr(eps), _ptr(out))
+    return out
+
+
+def getAcc_g_smth_mimj_mpi(nbeg, nend, pos, mass, G, epsilon):
+    pos = _f64(pos, (-1, 3)); n = pos.shape[0]; mass = _f64(mass)
+    eps = np.broadcast_to(_f64(epsilon), (n,)).copy() if np.ndim(epsilon) == 0 else _f64(epsilon)
+    out = np.zeros((n, 3))
+    _load().orc_grav_mimj(n, _ptr(pos), _ptr(mass), float(G), _ptr(eps), int(nbeg), int(nend), _ptr(out))
     return out
 
 

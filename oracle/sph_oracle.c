@@ -458,6 +458,53 @@ void orc_grav_sym(int64_t n, const double *pos, const double *mass, double G,
     }
 }
 
+/* getAcc_g_smth_mimj_mpi, sph_code/libsx.py:908-947: the (n, 3) partial
+ * field of the rows i in [nbeg, nend) (their j > i terms) and the reactions
+ * on the rows j > i, serial in the reference's loop order. */
+void orc_grav_mimj(int64_t n, const double *pos, const double *mass, double G,
+                   const double *eps, int64_t nbeg, int64_t nend, double *field) {
+    memset(field, 0, sizeof(double) * 3 * (size_t)n);
+    for (int64_t i = nbeg; i < nend; ++i) {
+        for (int64_t j = i + 1; j < n; ++j) {
+            double dx = pos[3 * j + 0] - pos[3 * i + 0];
+            double dy = pos[3 * j + 1] - pos[3 * i + 1];
+            double dz = pos[3 * j + 2] - pos[3 * i + 2];
+            double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            double fk = grav_fk(rr, 0.5 * (eps[i] + eps[j]));
+            field[3 * i + 0] += G * fk * dx * mass[j];
+            field[3 * j + 0] -= G * fk * dx * mass[i];
+            field[3 * i + 1] += G * fk * dy * mass[j];
+            field[3 * j + 1] -= G * fk * dy * mass[i];
+            field[3 * i + 2] += G * fk * dz * mass[j];
+            field[3 * j + 2] -= G * fk * dz * mass[i];
+        }
+    }
+}
+
+/* do_smoothingX((pos, subpos)), sph_code/libsx.py:752-774: for each of the m
+ * query points, 0.5 * (the k-th smallest distance to the n points of pos,
+ * 0-based; the reference uses k = 50). */
+void orc_smoothing_points(int64_t n, const double *pos, int64_t m, const double *q, int k,
+                          double *h_out) {
+#pragma omp parallel
+    {
+        double *dist = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t r = 0; r < m; ++r) {
+            for (int64_t j = 0; j < n; ++j) {
+                double dx = pos[3 * j + 0] - q[3 * r + 0];
+                double dy = pos[3 * j + 1] - q[3 * r + 1];
+                double dz = pos[3 * j + 2] - q[3 * r + 2];
+                dist[j] = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+            }
+            int64_t kk = k < n ? k : n - 1;
+            select_kth(dist, n, kk);
+            h_out[r] = dist[kk] * 0.5;
+        }
+        free(dist);
+    }
+}
+
 /* getPE, sph_code/libsx.py:583-620 (serial j > i double loop). */
 double orc_pe(int64_t n, const double *pos, const double *m, double G, const double *eps) {
     double PE = 0.0;

@@ -3,11 +3,14 @@ numba functions (sph_code/libsx.py, sph_code/shear.py) on seeded inputs.
 
 Run once, in a container that has the reference checked out:
 
-    python tests/golden/make_golden.py /path/to/reference
+    python tests/golden/make_golden.py /path/to/reference [set ...]
 
-The output ``*.npz`` files are committed; tests read only them.  Inputs are
-the Evrard-profile initial conditions used throughout the tests (r = R sqrt(U),
-isotropic directions, equal masses) at small N, plus edge cases.
+(or with the path in the SPH3_REFERENCE environment variable); sets are
+``hydro`` (evrard600, evrard1500 and the edge cases) and ``gravity``
+(grav_forms), all of them by default.  The output ``*.npz`` files are
+committed; tests read only them.  Inputs are the Evrard-profile initial
+conditions used throughout the tests (r = R sqrt(U), isotropic directions,
+equal masses) at small N, plus edge cases.
 """
 from __future__ import annotations
 
@@ -30,11 +33,41 @@ def evrard(n, seed, R=1.0, M=1.0):
     return pos, m
 
 
-def main(ref_root):
+def gravity_forms(libsx):
+    """Every gravity form of the reference on one unequal-mass, unequal-eps
+    set: the symmetric full field, its x twin, a row slice, the mimj partial
+    arrays of a three-way row partition, getPE, and do_smoothingX with query
+    points distinct from the particles (some outside the cloud, one on a
+    particle)."""
+    n = 700
+    pos, _ = evrard(n, 21)
+    rng = np.random.default_rng(2100)
+    m = (0.5 + rng.random(n)) / n
+    eps = 0.005 + 0.015 * rng.random(n)
+    G = 1.0
+    acc_sym = libsx.getAcc_g_smth(pos, m, G, eps)
+    acc_x = libsx.getAcc_g_smthx(pos, m, G, eps)
+    acc_rows = libsx.getAcc_g_smth_mpi(150, 420, pos, m, G, eps)
+    parts = np.array([[0, 230], [230, 520], [520, n]])
+    mimj = np.stack([libsx.getAcc_g_smth_mimj_mpi(int(b), int(e), pos, m, G, eps) for b, e in parts])
+    PE = libsx.getPE(pos, m, G, eps)
+    q = np.concatenate([rng.normal(scale=0.6, size=(120, 3)), 1.5 * rng.normal(size=(29, 3)), pos[[17]]])
+    hq = libsx.do_smoothingX((pos, q))
+    np.savez_compressed(os.path.join(HERE, "grav_forms.npz"), pos=pos, m=m, eps=eps, G=G,
+                        acc_sym=acc_sym, acc_x=acc_x, acc_rows=acc_rows, acc_rows_range=np.array([150, 420]),
+                        mimj=mimj, mimj_parts=parts, PE=PE, q=q, hq=hq)
+    print("wrote grav_forms", n)
+
+
+def main(ref_root, sets=("hydro", "gravity")):
     sys.path.insert(0, os.path.join(ref_root, "sph_code"))
     import libsx  # noqa: E402  (the reference)
     import shear  # noqa: E402  (the reference)
 
+    if "gravity" in sets:
+        gravity_forms(libsx)
+    if "hydro" not in sets:
+        return
     gama, alpha, beta, eta, G = 5.0 / 3.0, 1.0, 2.0, 0.1, 1.0
     cases = {"evrard600": (600, 7), "evrard1500": (1500, 11)}
     for name, (n, seed) in cases.items():
@@ -96,4 +129,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPH3_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [hydro] [gravity]  (or set SPH3_REFERENCE)")
+    main(root, tuple(sys.argv[2:]) or ("hydro", "gravity"))

@@ -96,3 +96,22 @@ def test_h_cap_flags(oc, golden):
     g = golden("evrard600")
     h, st = oc.h_smooth_rows(g["pos"], g["h0"] * 3.0, rows=np.arange(10), max_iter=3)
     assert np.all(st == -1)
+
+
+def test_gravity_forms_bitexact(oc, golden):
+    """Every gravity form (unequal masses and softening lengths), the mimj
+    partial arrays of a three-way partition, getPE and do_smoothingX with
+    distinct query points (sph_code/libsx.py:583-747, 752-774, 908-947)."""
+    g = golden("grav_forms")
+    pos, m, eps, G = g["pos"], g["m"], g["eps"], float(g["G"])
+    assert np.array_equal(oc.getAcc_g_smth(pos, m, G, eps), g["acc_sym"])
+    assert np.array_equal(oc.getAcc_g_smthx(pos, m, G, eps), g["acc_x"])
+    b, e = g["acc_rows_range"]
+    assert np.array_equal(oc.getAcc_g_smth_mpi(b, e, pos, m, G, eps), g["acc_rows"])
+    for k, (b, e) in enumerate(g["mimj_parts"]):
+        assert np.array_equal(oc.getAcc_g_smth_mimj_mpi(b, e, pos, m, G, eps), g["mimj"][k])
+    assert oc.getPE(pos, m, G, eps) == float(g["PE"])
+    assert np.array_equal(oc.do_smoothingX((pos, g["q"])), g["hq"])
+    # the three full forms agree bit for bit, and the partials sum to the field
+    assert np.array_equal(g["acc_sym"], g["acc_x"])
+    assert np.allclose(g["mimj"].sum(axis=0), g["acc_sym"], rtol=1e-12, atol=1e-12 * np.abs(g["acc_sym"]).max())
