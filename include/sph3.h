@@ -29,10 +29,18 @@
  *   sph3_compute(SPH3_DO_GRAVITY)         getAcc_g_smth* (libsx.py:623-747, 908-947)
  *        as a Barnes-Hut walk; GPU: bh_tree_iteration_v2.h:29-588
  *   sph3_gravity_direct_rows              getAcc_g_smth_mpi (libsx.py:667-705), FP64
+ *   sph3_gravity_pairsum                  getAcc_g_smth, getAcc_g_smth_mpi, getAcc_g_smthx,
+ *        getAcc_g_smth_mimj_mpi (libsx.py:623-747, 908-947) in the reference's
+ *        summation order (bit for bit)
+ *   sph3_potential_pairsum                getPE (libsx.py:583-620) as FP64 pair sums
+ *   sph3_kth_distance                     do_smoothingX((pos, subpos)) for query points
+ *        (libsx.py:752-774)
  *   sph3_first_step                       sph_serial.py:85-134
  *   sph3_step                             one loop body of sph_serial.py:142-196
  *        (or sph_mpi4_v4.py:278-430 with step_order = SPH3_ORDER_MPI4);
  *        GPU: hfvGpuSphBHtree_newCool_v8_KH.cu:985-1582
+ *   sph3_step_io                          the same loop body with its arrays in host
+ *        memory (sph_serial.py:142-193 keeps r, v, acc, h, u, ut_previous as NumPy arrays)
  *   sph3_energy                           getKE / getPE (libsx.py:569-620)
  *
  * Buffers: every pointer argument names memory of the kind its `on_device`
@@ -230,6 +238,26 @@ int sph3_first_step(sph3_ctx *ctx, double dt, void *stream);
 /* nsteps leapfrog kick-drift-kick steps of length dt. */
 int sph3_step(sph3_ctx *ctx, double dt, int32_t nsteps, void *stream);
 
+/* nsteps steps of length dt with the state moved in from and out to HOST
+ * buffers in the same call: the loop body of sph_code/sph_serial.py:142-193
+ * as the reference runs it, its arrays (r, v, acc, h, u, ut_previous) living
+ * in host memory.  in[k] holds field in_fields[k] ((n x components)
+ * row-major FP64, caller's order) and is written into the state before the
+ * steps; out[k] receives field out_fields[k] after them (SPH3_FIELD_NNGB
+ * too, as doubles).  Transfers overlap the step: each input is copied on a
+ * copy stream and scattered just before the step first needs it (h after
+ * the sort, u before the EOS, u_prev and dudt_prev before the kick that
+ * updates u; all others before the first kick), and each output leaves on a
+ * second copy stream as soon as it is final (positions after the sort, h
+ * after the h search, the rest at the end).  An input u without u_prev also
+ * sets u_prev (the reference's loop keeps u_previous = u between
+ * iterations).  Page-locked host buffers are needed for the overlap
+ * (pageable ones work, serialised).  The steps run without the captured
+ * graph; the call synchronises before it returns. */
+int sph3_step_io(sph3_ctx *ctx, double dt, int32_t nsteps, int32_t nin, const int32_t *in_fields,
+                 const double *const *in, int32_t nout, const int32_t *out_fields, double *const *out,
+                 void *stream);
+
 /* Global sums in FP64 of the current state: out[0] KE, out[1] thermal energy
  * sum m u, out[2] PE = 1/2 sum m phi, out[3] total, out[4..6] momentum,
  * out[7] mass.  Synchronises `stream`. */
@@ -245,11 +273,6 @@ int sph3_status(sph3_ctx *ctx, uint32_t *status, int clear);
 int sph3_gravity_direct_rows(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, double *acc,
                              double *phi);
 
-/* Neighbour sets {j : |r_ij| <= h_i + h_j} (the q <= 2 support of the
- * reference kernels) of the listed rows, as caller's indices in ascending
- * order: row k's set is idx[offsets[k] .. offsets[k+1]).  offsets has nrows+1
- * entries; at most cap indices are written (SPH3_STATUS_LIST_OVERFLOW past
- * it).  Host buffers. */
 /* The pairs the mixed path's hydro pass runs for the listed rows: the
  * neighbour lists the last density pass kept (|r_ij| <= h_i + h_j tested in
  * FP32 on cell-relative positions), as caller's indices in ascending order,
@@ -261,8 +284,49 @@ int sph3_gravity_direct_rows(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, 
 int sph3_pair_lists(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *offsets, int64_t *idx,
                     int64_t cap);
 
+/* Neighbour sets {j : |r_ij| <= h_i + h_j} (the q <= 2 support of the
+ * reference kernels, sph_code/libsx.py:34-38) of the listed rows, as caller's
+ * indices in ascending order: row k's set is idx[offsets[k] .. offsets[k+1]).
+ * offsets has nrows+1 entries; at most cap indices are written
+ * (SPH3_STATUS_LIST_OVERFLOW past it).  Host buffers. */
 int sph3_neighbours(sph3_ctx *ctx, const int64_t *rows, int64_t nrows, int64_t *offsets,
                     int64_t *idx, int64_t cap);
+
+/* Spline-softened gravity of the loaded particles (one system, open
+ * boundaries) as the reference's FP64 direct sums, in the reference's
+ * summation order, so the results equal the reference's bit for bit on the
+ * same inputs (a coincident pair adds 0, where the reference raises
+ * ZeroDivisionError).  G comes from the config, eps from the eps field.
+ *   form SPH3_GSUM_ROWS: rows [nbeg, nend) of a_i = sum_{j != i} ... in the
+ *     caller's order, out (nend - nbeg) x 3 -- getAcc_g_smth
+ *     (sph_code/libsx.py:623-662), getAcc_g_smth_mpi (:667-705) and
+ *     getAcc_g_smthx (:710-747), which agree bit for bit;
+ *   form SPH3_GSUM_MIMJ: the n x 3 partial array of
+ *     getAcc_g_smth_mimj_mpi(nbeg, nend, ...) (:908-947): the j > i terms of
+ *     rows i in [nbeg, nend) and their reactions on rows j > i; summed over a
+ *     row partition it is the full field.
+ * out is host (on_device = 0; the call synchronises) or device memory.
+ * O(n * rows) work: a checker and drop-in, not the step's gravity. */
+#define SPH3_GSUM_ROWS 0
+#define SPH3_GSUM_MIMJ 1
+int sph3_gravity_pairsum(sph3_ctx *ctx, int form, int64_t nbeg, int64_t nend, double *out, int on_device,
+                         void *stream);
+
+/* Softened potential energy of getPE (sph_code/libsx.py:583-620): the
+ * reference's j > i terms in its order per row i, the row sums added in row
+ * order (the reference chains all pairs into one sum, so the result can
+ * differ from it in the last bits).  One system, open boundaries. */
+int sph3_potential_pairsum(sph3_ctx *ctx, double *pe, void *stream);
+
+/* do_smoothingX((pos, subpos)) (sph_code/libsx.py:752-774) for query points:
+ * out[i] = 0.5 * (the value at 0-based index k of the sorted distances from
+ * query i to every loaded particle), the reference's h with k = 50.  The
+ * k-th squared distance is found exactly (radix select on its bits).  qpos
+ * (m x 3 row-major FP64) and out are host (on_device = 0) or device memory.
+ * SPH3_ERR_INVALID_ARG when k >= the particle count (the reference raises
+ * IndexError); open boundaries only. */
+int sph3_kth_distance(sph3_ctx *ctx, const double *qpos, int64_t m, int32_t k, double *out, int on_device,
+                      void *stream);
 
 /* Current Morton order: order[k] = caller's index of the k-th sorted particle,
  * keys[k] its 64-bit key (either pointer may be NULL).  Host buffers. */
@@ -317,17 +381,22 @@ int sph3_probe_fp32_rate(int device, double *tflops, void *stream);
  * device allocator, or a loop that cannot afford cudaMalloc's latency and
  * implicit synchronisation.  They pass device buffers only: pos ((n,3)
  * row-major FP64, read), order (n int64: caller index of the k-th sorted
- * particle) and keys (n uint64 Morton keys); either output may be NULL.
- * The result equals sph3_set_particles + sph3_morton_order for one system
- * with the same max_level (4..21).
+ * particle) and keys (n uint64 Morton keys); either output may be NULL, not
+ * both.  status (one device word, may be NULL) receives the SPH3_STATUS_*
+ * bits this call raised (SPH3_STATUS_NAN_INPUT: a non-finite coordinate,
+ * which is quantised to cell 0), written in stream order at the end of the
+ * call.  The result equals sph3_set_particles + sph3_morton_order for one
+ * system with the same max_level (4..21).
  * Limit: n <= 65536 (SPH3_ERR_TOO_LARGE above it).  The scratch is a fixed
  * static device array (about 3 MB) that every GPU loading the library holds
- * until the process exits; the first call on a device looks up its address,
- * so make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race.  Stream-ordered on `stream`;
- * does not synchronise.  Non-finite coordinates quantise to cell 0. */
+ * until the process exits; the first call on a device (and the first after a
+ * cudaDeviceReset) looks up its address, so make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  Stream-ordered on `stream`; does not synchronise.  Returns
+ * SPH3_ERR_CUDA without doing anything when a CUDA error is already pending
+ * on entry (the caller's own; it is left unread). */
 int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t max_level, int64_t *order,
-                             uint64_t *keys, void *stream);
+                             uint64_t *keys, unsigned *status, void *stream);
 
 #ifdef __cplusplus
 }

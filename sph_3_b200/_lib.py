@@ -107,7 +107,11 @@ SIGNATURES = {
     "sph3_kernels_per_step": (ctypes.c_int, [P, P]),
     "sph3_probe_fp32_rate": (ctypes.c_int, [ctypes.c_int, P, P]),
     "sph3_timestep": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_int, P, P]),
-    "sph3_morton_sort_noalloc": (ctypes.c_int, [P, I64, I32, P, P, P]),
+    "sph3_morton_sort_noalloc": (ctypes.c_int, [P, I64, I32, P, P, P, P]),
+    "sph3_gravity_pairsum": (ctypes.c_int, [P, ctypes.c_int, I64, I64, P, ctypes.c_int, P]),
+    "sph3_potential_pairsum": (ctypes.c_int, [P, P, P]),
+    "sph3_kth_distance": (ctypes.c_int, [P, P, I64, I32, P, ctypes.c_int, P]),
+    "sph3_step_io": (ctypes.c_int, [P, D, I32, I32, P, P, I32, P, P, P]),
 }
 
 _lib = None

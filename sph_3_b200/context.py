@@ -238,6 +238,51 @@ class Context:
         st = ctypes.c_void_p(stream) if stream is not None else None
         check(self.lib.sph3_step(self._ptr, float(dt), int(nsteps), st), "step")
 
+    def step_io(self, dt, inputs, outputs, nsteps=1):
+        """nsteps steps with the state moved in from and out to host arrays in
+        one call (sph3_step_io): inputs {field: array}, outputs {field:
+        C-contiguous float64 host array to fill, e.g. page-locked torch CPU
+        tensors}; transfers overlap the step."""
+        def host_ptr(a, name, shape):
+            if hasattr(a, "data_ptr"):
+                ok = (not a.is_cuda and a.is_contiguous() and str(a.dtype) == "torch.float64"
+                      and tuple(a.shape) in (shape, (self.n * FIELDS[name][1],)))
+                return a.data_ptr() if ok else None
+            a_ok = (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                    and a.size == self.n * FIELDS[name][1])
+            return a.ctypes.data if a_ok else None
+
+        def shape_of(name):
+            nc = FIELDS[name][1]
+            return (self.n, nc) if nc > 1 else (self.n,)
+
+        keep = []
+        in_f, in_p = [], []
+        for name, a in inputs.items():
+            if not hasattr(a, "data_ptr"):
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(a)
+            p = host_ptr(a, name, shape_of(name))
+            if p is None:
+                raise ValueError("step_io input %s must be a float64 host array of shape %s" % (name, shape_of(name)))
+            in_f.append(FIELDS[name][0])
+            in_p.append(p)
+        out_f, out_p = [], []
+        for name, a in outputs.items():
+            p = host_ptr(a, name, shape_of(name))
+            if p is None:
+                raise ValueError("step_io output %s must be a C-contiguous float64 host array of shape %s"
+                                 % (name, shape_of(name)))
+            out_f.append(FIELDS[name][0])
+            out_p.append(p)
+        fi = (ctypes.c_int32 * max(1, len(in_f)))(*in_f)
+        pi = (ctypes.c_void_p * max(1, len(in_p)))(*in_p)
+        fo = (ctypes.c_int32 * max(1, len(out_f)))(*out_f)
+        po = (ctypes.c_void_p * max(1, len(out_p)))(*out_p)
+        check(self.lib.sph3_step_io(self._ptr, float(dt), int(nsteps), len(in_f), fi, pi, len(out_f), fo, po, None),
+              "step_io")
+        del keep
+
     def energy(self):
         out = np.zeros(8)
         check(self.lib.sph3_energy(self._ptr, out.ctypes.data_as(ctypes.c_void_p), None), "energy")
@@ -291,6 +336,50 @@ class Context:
                                                 acc.ctypes.data_as(ctypes.c_void_p),
                                                 phi.ctypes.data_as(ctypes.c_void_p)), "gravity_direct_rows")
         return acc, phi
+
+    def gravity_pairsum(self, form="rows", nbeg=0, nend=None, device=False):
+        """Reference-order FP64 gravity (sph3_gravity_pairsum): form "rows" gives
+        rows [nbeg, nend) of getAcc_g_smth / _mpi / x, form "mimj" the (n, 3)
+        partial array of getAcc_g_smth_mimj_mpi(nbeg, nend, ...)."""
+        nend = self.n if nend is None else int(nend)
+        nbeg = int(nbeg)
+        code = {"rows": C["SPH3_GSUM_ROWS"], "mimj": C["SPH3_GSUM_MIMJ"]}[form]
+        rows = (nend - nbeg) if form == "rows" else self.n
+        if device:
+            import torch
+            out = torch.empty((max(rows, 0), 3), dtype=torch.float64, device="cuda")
+            check(self.lib.sph3_gravity_pairsum(self._ptr, code, nbeg, nend, ctypes.c_void_p(out.data_ptr()), 1,
+                                                _stream_ptr()), "gravity_pairsum")
+            return out
+        out = np.zeros((max(rows, 0), 3))
+        check(self.lib.sph3_gravity_pairsum(self._ptr, code, nbeg, nend, out.ctypes.data_as(ctypes.c_void_p), 0,
+                                            None), "gravity_pairsum")
+        return out
+
+    def potential_pairsum(self):
+        """getPE as FP64 pair sums in the reference's row order (sph3_potential_pairsum)."""
+        v = ctypes.c_double()
+        check(self.lib.sph3_potential_pairsum(self._ptr, ctypes.byref(v), None), "potential_pairsum")
+        return float(v.value)
+
+    def kth_distance(self, qpos, k=50, device=False):
+        """0.5 x the k-th (0-based) sorted distance from each query point to the
+        loaded particles (sph3_kth_distance; do_smoothingX with k = 50)."""
+        if _is_torch(qpos) and qpos.is_cuda:
+            import torch
+            q = qpos.detach().to(torch.float64).contiguous()
+            m = int(q.shape[0])
+            out = torch.empty(m, dtype=torch.float64, device=q.device)
+            check(self.lib.sph3_kth_distance(self._ptr, ctypes.c_void_p(q.data_ptr()), m, int(k),
+                                             ctypes.c_void_p(out.data_ptr()), 1, _stream_ptr()), "kth_distance")
+            return out
+        if _is_torch(qpos):
+            qpos = qpos.detach().cpu().numpy()
+        q = np.ascontiguousarray(qpos, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(q.shape[0])
+        check(self.lib.sph3_kth_distance(self._ptr, q.ctypes.data_as(ctypes.c_void_p), q.shape[0], int(k),
+                                         out.ctypes.data_as(ctypes.c_void_p), 0, None), "kth_distance")
+        return out
 
     def neighbours(self, rows, cap=None):
         rows = np.ascontiguousarray(rows, dtype=np.int64)

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <vector>
 
@@ -52,6 +53,12 @@ struct sph3_ctx {
     // timing
     cudaEvent_t ev[12] = {};
     double phase_ms[9] = {};
+    // host-buffer step (sph3_step_io): input / output staging in the caller's
+    // order, a copy stream per direction, events between them and the step
+    double *io_in = nullptr, *io_out = nullptr;
+    int64_t io_in_cap = 0, io_out_cap = 0;  // doubles
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t io_ev[8] = {};
 };
 
 namespace {
@@ -510,9 +517,17 @@ void record(sph3_ctx *c, int k, cudaStream_t st) {
     if (c->cfg.timing) cudaEventRecord(c->ev[k], st);
 }
 
+// Points inside one step where the host-buffer step moves its inputs in and
+// its outputs out, each called on the compute stream: after the gather that
+// follows the sort (new order in place, packs not yet built), after the h
+// search, before the kick that updates u, and at the end.
+struct StepHooks {
+    std::function<void(cudaStream_t)> after_gather, after_h, before_kick, at_end;
+};
+
 // One timestep, enqueued on st.  Switches the carried block half way (the
 // gather after the sort writes the other block).
-void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
+void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk = nullptr) {
     State &S = c->S;
     const Params &P = c->P;
     record(c, 0, st);
@@ -537,6 +552,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
         launch_gather_orig(S, c->orig_blk[c->cur], c->orig_blk[other], st);
         c->cur = other;
         point_carried(c);
+        if (hk && hk->after_gather) hk->after_gather(st);
         launch_pack(S, P, kPackPos | kPackHme | kPackVel, st);
     }
     record(c, 3, st);
@@ -544,6 +560,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
     record(c, 4, st);
     launch_h_search(S, P, st);
     launch_tree_refit_h(S, P, st);
+    if (hk && hk->after_h) hk->after_h(st);
     record(c, 5, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
     record(c, 6, st);
@@ -552,6 +569,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
     const bool serial = P.step_order == SPH3_ORDER_SERIAL;
     launch_hydro(S, P, true, serial, st);
     record(c, 8, st);
+    if (hk && hk->before_kick) hk->before_kick(st);
     if (serial) {
         launch_kick_update(S, P, dt, true, true, st);
     } else {
@@ -562,8 +580,57 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st) {
         launch_u_update(S, P, dt, st);
     }
     launch_energy(S, P, st);
+    if (hk && hk->at_end) hk->at_end(st);
     record(c, 11, st);
     c->inv_valid = false;
+}
+
+// staging and copy streams of sph3_step_io, made on first use
+int ensure_io(sph3_ctx *c, int64_t in_tot, int64_t out_tot) {
+    if (!c->h2d) {
+        CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+        for (auto &e : c->io_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (in_tot > c->io_in_cap) {
+        if (c->io_in) cudaFree(c->io_in);
+        c->io_in = nullptr;
+        c->io_in_cap = 0;
+        CK(dalloc(&c->io_in, (size_t)in_tot));
+        c->io_in_cap = in_tot;
+    }
+    if (out_tot > c->io_out_cap) {
+        if (c->io_out) cudaFree(c->io_out);
+        c->io_out = nullptr;
+        c->io_out_cap = 0;
+        CK(dalloc(&c->io_out, (size_t)out_tot));
+        c->io_out_cap = out_tot;
+    }
+    return SPH3_OK;
+}
+
+// when an input of the host-buffer step is scattered into the state: 0 before
+// the first kick, 1 after the gather (h: before the packs and the tree), 2
+// after the h search (u: before the EOS), 3 before the kick that updates u
+int io_stage_in(int f) {
+    switch (f) {
+        case SPH3_FIELD_H: return 1;
+        case SPH3_FIELD_U: return 2;
+        case SPH3_FIELD_U_PREV:
+        case SPH3_FIELD_DUDT_PREV: return 3;
+        default: return 0;
+    }
+}
+
+// when an output is final: 0 after the gather (positions), 1 after the h
+// search (h, neighbour counts), 2 at the end of the step
+int io_stage_out(int f) {
+    switch (f) {
+        case SPH3_FIELD_POS: return 0;
+        case SPH3_FIELD_H:
+        case SPH3_FIELD_NNGB: return 1;
+        default: return 2;
+    }
 }
 
 void accumulate_times(sph3_ctx *c, bool serial) {
@@ -705,6 +772,14 @@ int sph3_ctx_destroy(sph3_ctx *c) {
     if (S.energy) cudaFree(S.energy);
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
+    if (c->h2d) cudaStreamSynchronize(c->h2d);
+    if (c->d2h) cudaStreamSynchronize(c->d2h);
+    for (auto &e : c->io_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->io_in) cudaFree(c->io_in);
+    if (c->io_out) cudaFree(c->io_out);
+    if (c->h2d) cudaStreamDestroy(c->h2d);
+    if (c->d2h) cudaStreamDestroy(c->d2h);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return SPH3_OK;
@@ -1062,6 +1137,120 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
     return SPH3_OK;
 }
 
+int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int32_t *in_fields,
+                 const double *const *in, int32_t nout, const int32_t *out_fields, double *const *out,
+                 void *stream) {
+    if (!c || nsteps < 1 || nin < 0 || nout < 0 || (nin > 0 && (!in_fields || !in)) ||
+        (nout > 0 && (!out_fields || !out)))
+        return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    State &S = c->S;
+    const int64_t n = S.n;
+    std::vector<int64_t> in_off(nin), out_off(nout);
+    std::vector<int> in_nc(nin), out_nc(nout);
+    int64_t in_tot = 0, out_tot = 0;
+    bool has_u = false, has_uprev = false;
+    for (int k = 0; k < nin; ++k) {
+        int nc = 1;
+        if (!in[k] || !field_ptr(c, in_fields[k], &nc)) return SPH3_ERR_INVALID_ARG;
+        has_u |= in_fields[k] == SPH3_FIELD_U;
+        has_uprev |= in_fields[k] == SPH3_FIELD_U_PREV;
+        in_off[k] = in_tot;
+        in_nc[k] = nc;
+        in_tot += nc * n;
+    }
+    for (int k = 0; k < nout; ++k) {
+        int nc = 1;
+        if (!out[k] || (out_fields[k] != SPH3_FIELD_NNGB && !field_ptr(c, out_fields[k], &nc)))
+            return SPH3_ERR_INVALID_ARG;
+        out_off[k] = out_tot;
+        out_nc[k] = nc;
+        out_tot += nc * n;
+    }
+    if (n == 0) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int rc = ensure_io(c, std::max<int64_t>(in_tot, 1), std::max<int64_t>(out_tot, 1));
+    if (rc) return rc;
+    if ((rc = sync_packs(c, st, true))) return rc;
+    if (!c->P.gravity) CK(cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st));
+    // inputs: host -> staging on the copy stream, ordered by when the step needs them
+    CK(cudaEventRecord(c->io_ev[7], st));
+    CK(cudaStreamWaitEvent(c->h2d, c->io_ev[7], 0));
+    for (int stage = 0; stage < 4; ++stage) {
+        for (int k = 0; k < nin; ++k)
+            if (io_stage_in(in_fields[k]) == stage)
+                CK(cudaMemcpyAsync(c->io_in + in_off[k], in[k], sizeof(double) * in_nc[k] * n,
+                                   cudaMemcpyHostToDevice, c->h2d));
+        CK(cudaEventRecord(c->io_ev[stage], c->h2d));
+    }
+    // staging -> state in the current order (field pointers looked up when the
+    // hook runs: the carried block switches inside the step)
+    auto scatter = [&](int stage, cudaStream_t s) {
+        cudaStreamWaitEvent(s, c->io_ev[stage], 0);
+        for (int k = 0; k < nin; ++k) {
+            if (io_stage_in(in_fields[k]) != stage) continue;
+            int nc = 1;
+            double *dst = field_ptr(c, in_fields[k], &nc);
+            k_scatter_in<<<blocks_for(c, n), 256, 0, s>>>(c->io_in + in_off[k], dst, S.orig, n, nc);
+        }
+        // the reference's loop keeps u_previous = u between iterations
+        // (sph_serial.py:181-182): an input u alone sets both
+        if (stage == 3 && has_u && !has_uprev)
+            cudaMemcpyAsync(S.u_prev, S.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    };
+    // outputs: state -> staging in the caller's order as soon as each is final
+    auto gather = [&](int stage, cudaStream_t s) {
+        for (int k = 0; k < nout; ++k) {
+            if (io_stage_out(out_fields[k]) != stage) continue;
+            if (out_fields[k] == SPH3_FIELD_NNGB) {
+                k_gather_out_int<<<blocks_for(c, n), 256, 0, s>>>(S.nngb, c->io_out + out_off[k], c->inv, 0, n);
+            } else {
+                int nc = 1;
+                const double *src = field_ptr(c, out_fields[k], &nc);
+                k_gather_out<<<blocks_for(c, n), 256, 0, s>>>(src, c->io_out + out_off[k], c->inv, n, nc, 0, n);
+            }
+        }
+        cudaEventRecord(c->io_ev[4 + stage], s);
+    };
+    scatter(0, st);
+    for (int step = 0; step < nsteps; ++step) {
+        const bool first = step == 0, last = step == nsteps - 1;
+        StepHooks hk;
+        hk.after_gather = [&](cudaStream_t s) {
+            if (first) scatter(1, s);
+            if (last) {
+                k_invert<<<blocks_for(c, n), 256, 0, s>>>(S.orig, c->inv, n);
+                gather(0, s);
+            }
+        };
+        hk.after_h = [&](cudaStream_t s) {
+            if (first) scatter(2, s);
+            if (last) gather(1, s);
+        };
+        hk.before_kick = [&](cudaStream_t s) {
+            if (first) scatter(3, s);
+        };
+        hk.at_end = [&](cudaStream_t s) {
+            if (last) gather(2, s);
+        };
+        enqueue_step(c, dt, st, &hk);
+        if ((rc = check_launch())) return rc;
+    }
+    // staging -> host on the other copy stream, each group as soon as it is final
+    for (int stage = 0; stage < 3; ++stage) {
+        CK(cudaStreamWaitEvent(c->d2h, c->io_ev[4 + stage], 0));
+        for (int k = 0; k < nout; ++k)
+            if (io_stage_out(out_fields[k]) == stage)
+                CK(cudaMemcpyAsync(out[k], c->io_out + out_off[k], sizeof(double) * out_nc[k] * n,
+                                   cudaMemcpyDeviceToHost, c->d2h));
+    }
+    CK(cudaStreamSynchronize(c->d2h));
+    CK(cudaStreamSynchronize(st));
+    c->inv_valid = true;
+    return SPH3_OK;
+}
+
 int sph3_timestep(sph3_ctx *c, double c_cfl, int all_pairs, double *dt_min, void *stream) {
     if (!c || !dt_min || !(c_cfl > 0.0)) return SPH3_ERR_INVALID_ARG;
     if (!c->have) return SPH3_ERR_STATE;
@@ -1252,4 +1441,89 @@ int sph3_phase_times(sph3_ctx *c, double out[9], int clear) {
     return SPH3_OK;
 }
 
+// ------------------------------------------------------------ reference-order sums
+int sph3_gravity_pairsum(sph3_ctx *c, int form, int64_t nbeg, int64_t nend, double *out, int on_device,
+                         void *stream) {
+    if (!c || (form != SPH3_GSUM_ROWS && form != SPH3_GSUM_MIMJ)) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    const int64_t n = c->S.n;
+    if (nbeg < 0 || nend > n || nbeg > nend) return SPH3_ERR_INVALID_ARG;
+    const int64_t rows = form == SPH3_GSUM_ROWS ? nend - nbeg : n;
+    if (rows == 0) return SPH3_OK;
+    if (!out) return SPH3_ERR_INVALID_ARG;
+    if (c->S.ncloud > 1 || c->P.periodic) return SPH3_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int rc = ensure_inv(c, st);
+    if (rc) return rc;
+    double *src = c->tmp;  // [5][n] caller order
+    launch_caller_sources(c->S, c->inv, src, st);
+    double *dst = on_device ? out : c->staging;
+    if (form == SPH3_GSUM_ROWS) {
+        launch_grav_pairsum(src, n, nbeg, nend, 0, n, c->P.G, dst, st);
+    } else {
+        // rows below nbeg receive nothing
+        if (nbeg > 0) CK(cudaMemsetAsync(dst, 0, sizeof(double) * 3 * nbeg, st));
+        launch_grav_pairsum(src, n, nbeg, n, nbeg, nend, c->P.G, dst + 3 * nbeg, st);
+    }
+    rc = check_launch();
+    if (rc) return rc;
+    if (!on_device) {
+        CK(cudaMemcpyAsync(out, c->staging, sizeof(double) * 3 * rows, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return SPH3_OK;
+}
+
+int sph3_potential_pairsum(sph3_ctx *c, double *pe, void *stream) {
+    if (!c || !pe) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    const int64_t n = c->S.n;
+    *pe = 0.0;
+    if (n == 0) return SPH3_OK;
+    if (c->S.ncloud > 1 || c->P.periodic) return SPH3_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int rc = ensure_inv(c, st);
+    if (rc) return rc;
+    launch_caller_sources(c->S, c->inv, c->tmp, st);
+    launch_pe_rows(c->tmp, n, c->P.G, c->staging, st);
+    rc = check_launch();
+    if (rc) return rc;
+    std::vector<double> part(n);
+    CK(cudaMemcpyAsync(part.data(), c->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += part[i];
+    *pe = s;
+    return SPH3_OK;
+}
+
+int sph3_kth_distance(sph3_ctx *c, const double *qpos, int64_t m, int32_t k, double *out, int on_device,
+                      void *stream) {
+    if (!c || m < 0 || k < 0 || (m > 0 && (!qpos || !out))) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    if (m == 0) return SPH3_OK;
+    if ((int64_t)k >= c->S.n) return SPH3_ERR_INVALID_ARG;
+    if (c->P.periodic) return SPH3_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    int rc = SPH3_OK;
+    if (on_device) {
+        launch_kth_dist(qpos, m, c->S, k, out, st);
+        return check_launch();
+    }
+    DevTmp<double> dq, dout;
+    CK(dq.alloc(3 * m));
+    CK(dout.alloc(m));
+    CK(cudaMemcpyAsync(dq.p, qpos, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, st));
+    launch_kth_dist(dq.p, m, c->S, k, dout.p, st);
+    rc = check_launch();
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out, dout.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
 }  // extern "C"
+

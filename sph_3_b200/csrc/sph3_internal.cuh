@@ -297,6 +297,12 @@ int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev,
 void launch_gravity(State &S, const Params &P, cudaStream_t st);
 void launch_gravity_direct(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
                            double *acc_dev, double *phi_dev, cudaStream_t st);
+// exact.cu (reference-order FP64 sums in the caller's particle order)
+void launch_caller_sources(State &S, const int64_t *inv, double *dst, cudaStream_t st);
+void launch_grav_pairsum(const double *src, int64_t n, int64_t row0, int64_t row1, int64_t kb, int64_t split,
+                         double G, double *out, cudaStream_t st);
+void launch_pe_rows(const double *src, int64_t n, double G, double *part, cudaStream_t st);
+void launch_kth_dist(const double *q, int64_t mq, const State &S, int64_t kth, double *out, cudaStream_t st);
 // integrate.cu
 void launch_kick_drift(State &S, const Params &P, double dt, cudaStream_t st);
 void launch_kick_update(State &S, const Params &P, double dt, bool update_u, bool second_kick,

@@ -5,16 +5,18 @@ computation runs on the GPU through libsph3 (the octree walks replace the
 reference's O(N^2) loops).  NumPy inputs give NumPy outputs; torch CUDA
 tensors give torch CUDA tensors (no host copies).
 
-Defaults reproduce the reference's semantics: FP64 arithmetic, the
-reference's h rule (N_ngb = 50 +- 5, h -/+= 0.3 % per step), the
-signal-velocity viscosity.  Two deliberate differences, both configurable
-with :func:`configure`:
-  * gravity (getAcc_g_smth*, getPE) is a Barnes-Hut walk with
-    ``theta=0.5`` (monopole + quadrupole); ``configure(theta=0)`` makes it
-    the exact direct sum;
-  * the h search stops after ``h_max_iter`` steps (the reference can loop
-    forever) and flags SPH3_STATUS_H_NOT_CONVERGED.
-``configure(precision="mixed")`` switches to the FP32 cell-relative path.
+Defaults reproduce the reference's results: FP64 arithmetic, the reference's
+h rule (N_ngb = 50 +- 5, h -/+= 0.3 % per step), the signal-velocity
+viscosity, and gravity (getAcc_g_smth*, getPE) as direct sums in the
+reference's own summation order, which return its values bit for bit
+(sph3_gravity_pairsum; O(N^2) work, as in the reference).  Options, set with
+:func:`configure`:
+  * ``grav_method="tree"`` switches gravity to the Barnes-Hut walk with
+    ``theta`` (default 0.5; monopole + quadrupole), O(N log N);
+  * the h search stops after ``h_max_iter`` steps of the 0.3 % rule (default
+    10,000, a factor 1e13 in h) and flags SPH3_STATUS_H_NOT_CONVERGED, where
+    the reference loops forever;
+  * ``precision="mixed"`` switches to the FP32 cell-relative path.
 Each call loads the particles, sorts them and builds the tree; for repeated
 steps use :class:`sph_3_b200.Context` which keeps them resident.
 """
@@ -24,21 +26,28 @@ import numpy as np
 
 from .context import Config, Context
 
-_DEFAULT = Config(precision="fp64", h_mode="refstep", n_ngb=50, n_ngb_tol=5, h_max_iter=2000,
+_DEFAULT = Config(precision="fp64", h_mode="refstep", n_ngb=50, n_ngb_tol=5, h_max_iter=10000,
                   n_boot=50, theta=0.5, use_graph=False)
 _cfg = _DEFAULT
+_grav_method = "direct"  # "direct": reference-order sums; "tree": Barnes-Hut with theta
 _ctx = None
 
 
-def configure(**kw):
-    """Changes the settings used by every function of this module."""
-    global _cfg
+def configure(grav_method=None, **kw):
+    """Changes the settings used by every function of this module:
+    ``grav_method`` ("direct" or "tree") and any :class:`Config` field."""
+    global _cfg, _grav_method
+    if grav_method is not None:
+        if grav_method not in ("direct", "tree"):
+            raise ValueError("grav_method must be 'direct' or 'tree'")
+        _grav_method = grav_method
     _cfg = _cfg.replace(**kw)
 
 
 def reset():
-    global _cfg, _ctx
+    global _cfg, _ctx, _grav_method
     _cfg = _DEFAULT
+    _grav_method = "direct"
     if _ctx is not None:
         _ctx.close()
     _ctx = None
@@ -126,18 +135,21 @@ def smoothing_length_mpi(nbeg, nend, pos):
 
 
 def do_smoothingX(poz):
-    """do_smoothingX((pos, pos)) (libsx.py:752-774).  The reference's callers
-    pass the same array twice; a distinct second array is not supported."""
+    """h of each row of subpos: half the distance to its 51st-nearest row of
+    pos, itself included when it is one of them (libsx.py:752-774)."""
     pos, subpos = poz
     same = subpos is pos
-    if not same and not _torch_like(pos):
+    if not same and not _torch_like(pos) and not _torch_like(subpos):
         same = np.shape(subpos) == np.shape(pos) and np.array_equal(np.asarray(subpos), np.asarray(pos))
-    if not same and _torch_like(pos):
+    if not same and _torch_like(pos) and _torch_like(subpos):
         import torch
-        same = subpos.shape == pos.shape and bool(torch.equal(subpos, pos))
-    if not same:
-        raise NotImplementedError("do_smoothingX needs subpos == pos")
-    return smoothing_length_mpi(0, _n(pos), pos)
+        same = subpos.shape == pos.shape and subpos.device == pos.device and bool(torch.equal(subpos, pos))
+    if same:
+        return smoothing_length_mpi(0, _n(pos), pos)
+    ctx = _context()
+    ctx.set_particles(pos, _ones(pos))
+    out = ctx.kth_distance(subpos, 50, device=_torch_like(subpos) and getattr(subpos, "is_cuda", False))
+    return out
 
 
 # ------------------------------------------------------------ hydro
@@ -192,16 +204,26 @@ def _eps_array(epsilon, pos):
     return epsilon
 
 
-def _gravity(pos, mass, G, epsilon):
+def _gravity(pos, mass, G, epsilon, tree=True):
     ctx = _context(G=float(G))
     ctx.set_particles(pos, mass, eps=_eps_array(epsilon, pos))
-    ctx.compute("gravity")
+    if tree:
+        ctx.compute("gravity")
     return ctx
 
 
+def _grav_rows(pos, mass, G, epsilon, nbeg, nend, form="rows"):
+    dev = _torch_like(pos) and getattr(pos, "is_cuda", False)
+    if _grav_method == "direct":
+        ctx = _gravity(pos, mass, G, epsilon, tree=False)
+        return ctx.gravity_pairsum(form, nbeg, nend, device=dev)
+    ctx = _gravity(pos, mass, G, epsilon)
+    return _ret(None, pos, ctx, "acc_g", rows=(nbeg, nend))
+
+
 def getAcc_g_smth(pos, mass, G, epsilon):
-    """Spline-softened gravity (libsx.py:623-662) by a Barnes-Hut walk."""
-    return _ret(None, pos, _gravity(pos, mass, G, epsilon), "acc_g")
+    """Spline-softened gravity (libsx.py:623-662)."""
+    return _grav_rows(pos, mass, G, epsilon, 0, _n(pos))
 
 
 def getAcc_g_smthx(pos, mass, G, epsilon):
@@ -211,15 +233,18 @@ def getAcc_g_smthx(pos, mass, G, epsilon):
 
 def getAcc_g_smth_mpi(nbeg, nend, pos, mass, G, epsilon):
     """Rows [nbeg, nend) of the field (libsx.py:667-705)."""
-    return _ret(None, pos, _gravity(pos, mass, G, epsilon), "acc_g", rows=(nbeg, nend))
+    return _grav_rows(pos, mass, G, epsilon, nbeg, nend)
 
 
 def getAcc_g_smth_mimj_mpi(nbeg, nend, pos, mass, G, epsilon):
-    """(N, 3) partial field whose sum over a row partition is the full field
-    (libsx.py:908-947): rows [nbeg, nend) hold their full acceleration, the
-    others zero."""
-    ctx = _gravity(pos, mass, G, epsilon)
-    part = _ret(None, pos, ctx, "acc_g", rows=(nbeg, nend))
+    """The (N, 3) partial field of libsx.py:908-947: the j > i terms of rows
+    i in [nbeg, nend) and their reactions on the rows j > i, so the sum over a
+    row partition is the full field.  With grav_method="tree" it is instead
+    the full acceleration on rows [nbeg, nend) and zero elsewhere (the same
+    sum over a partition)."""
+    if _grav_method == "direct":
+        return _grav_rows(pos, mass, G, epsilon, nbeg, nend, form="mimj")
+    part = _grav_rows(pos, mass, G, epsilon, nbeg, nend)
     if _torch_like(part):
         import torch
         out = torch.zeros((_n(pos), 3), dtype=torch.float64, device=part.device)
@@ -238,6 +263,10 @@ def getKE(v, m):
 
 
 def getPE(pos, m, G, epsilon):
-    """Softened potential energy (libsx.py:583-620) = 1/2 sum m_i phi_i."""
+    """Softened potential energy (libsx.py:583-620): FP64 pair sums in the
+    reference's row order (grav_method="direct"), or 1/2 sum m_i phi_i of the
+    Barnes-Hut walk ("tree")."""
+    if _grav_method == "direct":
+        return _gravity(pos, m, G, epsilon, tree=False).potential_pairsum()
     ctx = _gravity(pos, m, G, epsilon)
     return float(ctx.energy()["PE"])

@@ -36,7 +36,8 @@ lib.sph3_set_field.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
 lib.sph3_compute.argtypes = [P, ctypes.c_uint32, P]
 lib.sph3_get_field.argtypes = [P, ctypes.c_int, P, I64, I64, ctypes.c_int, P]
 lib.sph3_ctx_destroy.argtypes = [P]
-SPH3_DO_DENSITY, SPH3_DO_GRAVITY = 0x8, 0x80
+lib.sph3_gravity_pairsum.argtypes = [P, ctypes.c_int, I64, I64, P, ctypes.c_int, P]
+SPH3_DO_DENSITY, SPH3_GSUM_ROWS = 0x8, 0
 SPH3_FIELD_RHO, SPH3_FIELD_ACC_G = 6, 12
 
 
@@ -73,15 +74,13 @@ def getAcc_g_smth(pos, mass, G, epsilon):
     pos = np.ascontiguousarray(pos, np.float64); n = len(mass)
     mass = np.ascontiguousarray(mass, np.float64)
     eps = np.full(n, float(epsilon)) if np.ndim(epsilon) == 0 else np.ascontiguousarray(epsilon, np.float64)
-    ctx = _ctx(G=float(G), theta=0.0)                  # theta = 0: the exact direct sum
+    ctx = _ctx(G=float(G))
     try:
-        z3 = np.zeros((n, 3)); z1 = np.zeros(n)
+        z3 = np.zeros((n, 3)); z1 = np.zeros(n); acc = np.empty((n, 3))
+        # the reference's direct sum in its own summation order (bit for bit)
         for rc in (lib.sph3_set_particles(ctx, n, _ptr(pos), _ptr(z3), _ptr(mass), _ptr(z1), _ptr(z1), _ptr(eps), 0, None),
-                   lib.sph3_compute(ctx, SPH3_DO_GRAVITY, None)):
+                   lib.sph3_gravity_pairsum(ctx, SPH3_GSUM_ROWS, 0, n, _ptr(acc), 0, None)):
             if rc: raise RuntimeError("sph3: %d" % rc)
-        acc = np.empty((n, 3))
-        rc = lib.sph3_get_field(ctx, SPH3_FIELD_ACC_G, _ptr(acc), 0, n, 0, None)
-        if rc: raise RuntimeError("sph3_get_field: %d" % rc)
         return acc
     finally:
         lib.sph3_ctx_destroy(ctx)

@@ -58,10 +58,16 @@ def test_density_hydro_fp64(golden, name):
 
 @pytest.mark.parametrize("name", CASES)
 def test_gravity_fp64(golden, name):
+    """Default (reference-order direct sums): bit-exact; the Barnes-Hut walk at
+    theta = 0 (exact in value, tree order) to 1e-10 and at theta = 0.5 to the
+    stated 1e-3 median."""
     from sph_3_b200 import libsx
     g = golden(name)
     G = g["consts"][4]
-    libsx.configure(theta=0.0)
+    assert np.array_equal(libsx.getAcc_g_smth(g["pos"], g["m"], G, g["eps"]), g["acc_g_sym"])
+    assert np.array_equal(libsx.getAcc_g_smth(g["pos"], g["m"], G, g["eps"]), g["acc_g"])
+    assert abs(libsx.getPE(g["pos"], g["m"], G, g["eps"]) - float(g["PE"])) < 1e-13 * abs(float(g["PE"]))
+    libsx.configure(grav_method="tree", theta=0.0)
     acc = libsx.getAcc_g_smth(g["pos"], g["m"], G, g["eps"])
     assert rel_err(acc, g["acc_g"]) < 1e-10
     assert abs(libsx.getPE(g["pos"], g["m"], G, g["eps"]) - float(g["PE"])) < 1e-10 * abs(float(g["PE"]))
@@ -70,6 +76,72 @@ def test_gravity_fp64(golden, name):
     err = np.linalg.norm(acc - g["acc_g"], axis=1) / np.linalg.norm(g["acc_g"], axis=1)
     assert np.median(err) < 1e-3 and np.percentile(err, 99) < 1e-2
     assert abs(libsx.getKE(g["vel"], g["m"]) - float(g["KE"])) < 1e-12 * float(g["KE"])
+
+
+def test_gravity_forms_bitexact(golden):
+    """Every gravity form of the reference on unequal masses and softening
+    lengths, per call: the full field and its x twin, a row slice, each mimj
+    partial array of a three-way partition (libsx.py:908-947: the j > i terms
+    of the slice rows plus their reactions on later rows), all bit for bit;
+    getPE to 1e-13; do_smoothingX with query points that are not the
+    particles, bit for bit."""
+    from sph_3_b200 import libsx
+    g = golden("grav_forms")
+    pos, m, eps, G = g["pos"], g["m"], g["eps"], float(g["G"])
+    assert np.array_equal(libsx.getAcc_g_smth(pos, m, G, eps), g["acc_sym"])
+    assert np.array_equal(libsx.getAcc_g_smthx(pos, m, G, eps), g["acc_x"])
+    b, e = g["acc_rows_range"]
+    assert np.array_equal(libsx.getAcc_g_smth_mpi(b, e, pos, m, G, eps), g["acc_rows"])
+    for k, (b, e) in enumerate(g["mimj_parts"]):
+        part = libsx.getAcc_g_smth_mimj_mpi(int(b), int(e), pos, m, G, eps)
+        assert part.shape == (pos.shape[0], 3)
+        assert np.array_equal(part, g["mimj"][k]), "partition %d" % k
+    assert abs(libsx.getPE(pos, m, G, eps) - float(g["PE"])) < 1e-13 * abs(float(g["PE"]))
+    assert np.array_equal(libsx.do_smoothingX((pos, g["q"])), g["hq"])
+
+
+def test_gravity_forms_torch_inputs(golden):
+    """The same calls with torch CUDA tensors return CUDA tensors holding the
+    same bits."""
+    import torch
+    from sph_3_b200 import libsx
+    g = golden("grav_forms")
+
+    def T(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+    pos, m, eps, G = T(g["pos"]), T(g["m"]), T(g["eps"]), float(g["G"])
+    b, e = (int(x) for x in g["mimj_parts"][1])
+    part = libsx.getAcc_g_smth_mimj_mpi(b, e, pos, m, G, eps)
+    assert part.is_cuda and np.array_equal(part.cpu().numpy(), g["mimj"][1])
+    hq = libsx.do_smoothingX((pos, T(g["q"])))
+    assert hq.is_cuda and np.array_equal(hq.cpu().numpy(), g["hq"])
+
+
+def test_gravity_forms_edge_cases():
+    """Edge cases of the reference-order entry points: empty slices, a slice
+    at the end, the k-th distance with k at the particle count (the
+    reference's IndexError) and a coincident pair (0 contribution)."""
+    from sph_3_b200 import libsx
+    from sph_3_b200._lib import Sph3Error
+    rng = np.random.default_rng(5)
+    n = 257
+    pos = rng.random((n, 3))
+    m = np.full(n, 1.0 / n)
+    eps = np.full(n, 0.02)
+    full = libsx.getAcc_g_smth(pos, m, 1.0, eps)
+    assert libsx.getAcc_g_smth_mpi(10, 10, pos, m, 1.0, eps).shape == (0, 3)
+    assert np.array_equal(libsx.getAcc_g_smth_mpi(n - 1, n, pos, m, 1.0, eps), full[n - 1:])
+    empty = libsx.getAcc_g_smth_mimj_mpi(100, 100, pos, m, 1.0, eps)
+    assert empty.shape == (n, 3) and not empty.any()
+    import oracle
+    assert np.array_equal(libsx.getAcc_g_smth_mimj_mpi(n - 1, n, pos, m, 1.0, eps),
+                          oracle.getAcc_g_smth_mimj_mpi(n - 1, n, pos, m, 1.0, eps))
+    with pytest.raises(Sph3Error):
+        libsx.do_smoothingX((pos[:50], pos[:3] + 0.5))
+    two = pos.copy()
+    two[7] = two[3]
+    assert np.array_equal(libsx.getAcc_g_smth(two, m, 1.0, eps), oracle.getAcc_g_smth(two, m, 1.0, eps))
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -92,9 +164,13 @@ def test_row_slice_variants_fp64(golden, name):
     du_sh = shear.get_dU_shear_mpi(b, e, *a, g["divV"], g["curlV"], alpha)
     assert rel_err(du_sh, g["dudt_sh"][b:e]) < 1e-9
     assert np.array_equal(libsx.getPressure(g["rho"], g["u"], gama), (gama - 1.0) * g["rho"] * g["u"])
-    libsx.configure(theta=0.0)
+    assert np.array_equal(libsx.getAcc_g_smth_mpi(b, e, g["pos"], g["m"], G, g["eps"]), g["acc_g"][b:e])
+    assert np.array_equal(libsx.getAcc_g_smthx(g["pos"], g["m"], G, g["eps"]), g["acc_g"])
+    parts = sum(libsx.getAcc_g_smth_mimj_mpi(p, q, g["pos"], g["m"], G, g["eps"])
+                for p, q in ((0, b), (b, e), (e, n)))
+    assert parts.shape == (n, 3) and rel_err(parts, g["acc_g"]) < 1e-12
+    libsx.configure(grav_method="tree", theta=0.0)
     assert rel_err(libsx.getAcc_g_smth_mpi(b, e, g["pos"], g["m"], G, g["eps"]), g["acc_g"][b:e]) < 1e-10
-    assert rel_err(libsx.getAcc_g_smthx(g["pos"], g["m"], G, g["eps"]), g["acc_g"]) < 1e-10
     parts = sum(libsx.getAcc_g_smth_mimj_mpi(p, q, g["pos"], g["m"], G, g["eps"])
                 for p, q in ((0, b), (b, e), (e, n)))
     assert parts.shape == (n, 3) and rel_err(parts, g["acc_g"]) < 1e-10
