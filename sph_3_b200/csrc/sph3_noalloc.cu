@@ -12,11 +12,16 @@
 // The array is g_sort_scratch: kNoAllocMaxN = 65536 particles, about 3 MB.
 // It exists once per GPU that loads the library and stays until the process
 // exits.  In host code its name is only a host-side stand-in, not a device
-// address, so the entry point resolves the real address once per device with
-// cudaGetSymbolAddress (the first call on a device does this; make that
-// first call before any stream capture).  Every call on a device shares the
-// array and it keeps the last call's contents: calls that overlap on the GPU
-// (different streams without ordering) race on it.
+// address, so the entry point resolves the real address with
+// cudaGetSymbolAddress once per device and CUDA context (the first call on a
+// device does this, and again the first call after cudaDeviceReset; make
+// that first call before any stream capture).  Every call on a device shares
+// the array and it keeps the last call's contents: calls that overlap on the
+// GPU (different streams without ordering) race on it.
+//
+// Device-side conditions (non-finite coordinates) are collected in a status
+// word inside the scratch, cleared at the start of every call and copied at
+// its end into the caller's optional device word `status`.
 //
 // The work is the same as the context path's sort (sph3_sort.cu): root cube
 // of the particles, 3 * max_level-bit Morton keys, stable 8-bit LSD radix
@@ -69,14 +74,37 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char *g_dev_ptr[kMaxDevices] = {};
+void *g_dev_ctx[kMaxDevices] = {};  // the CUDA context the cached address belongs to
 
-// device address of g_sort_scratch on the current device (set up once per device)
+// The current CUDA context (driver handle), looked up through the runtime's
+// driver entry point so the library needs no link against libcuda.
+using CtxGetCurrentFn = int (*)(void **);
+void *current_context() {
+    static CtxGetCurrentFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+        tried = true;
+    }
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// device address of g_sort_scratch on the current device, looked up once per
+// device and context (a cudaDeviceReset makes a new context, in which the
+// module and its array are loaded again, possibly elsewhere)
 int scratch_for_current_device(unsigned char **out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return SPH3_ERR_NO_DEVICE;
     if (dev < 0 || dev >= kMaxDevices) return SPH3_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_dev_ptr[dev]) {
+    void *ctx = current_context();
+    if (!g_dev_ptr[dev] || ctx == nullptr || ctx != g_dev_ctx[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
         if (e != cudaSuccess || p == nullptr) {
@@ -84,6 +112,7 @@ int scratch_for_current_device(unsigned char **out) {
             return SPH3_ERR_CUDA;
         }
         g_dev_ptr[dev] = static_cast<unsigned char *>(p);
+        g_dev_ctx[dev] = current_context();
     }
     *out = g_dev_ptr[dev];
     return SPH3_OK;
@@ -112,11 +141,12 @@ __global__ void k_na_setup(const double *pos_rm, int64_t n, double *pos_cm, int4
 }
 
 __global__ void k_na_output(const uint64_t *key, const uint32_t *val, int64_t n, int64_t *order,
-                            uint64_t *keys_out) {
+                            uint64_t *keys_out, const unsigned *status, unsigned *status_out) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         if (order) order[k] = (int64_t)val[k];
         if (keys_out) keys_out[k] = key[k];
     }
+    if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *status_out = *status;
 }
 
 }  // namespace
@@ -125,11 +155,16 @@ __global__ void k_na_output(const uint64_t *key, const uint32_t *val, int64_t n,
 using namespace sph3;
 
 extern "C" int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t max_level, int64_t *order,
-                                        uint64_t *keys, void *stream) {
+                                        uint64_t *keys, unsigned *status_out, void *stream) {
     if (n < 0 || (n > 0 && !pos) || (!order && !keys) || max_level < 4 || max_level > 21)
         return SPH3_ERR_INVALID_ARG;
     if (n > kNoAllocMaxN) return SPH3_ERR_TOO_LARGE;
-    if (n == 0) return SPH3_OK;
+    if (n == 0) return status_out ? (cudaMemsetAsync(status_out, 0, sizeof(unsigned), (cudaStream_t)stream) ==
+                                             cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA)
+                                  : SPH3_OK;
+    // an error left pending by the caller's own work is not this call's: leave
+    // it for the caller to read and do nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return SPH3_ERR_CUDA;
     unsigned char *s = nullptr;
     int rc = scratch_for_current_device(&s);
     if (rc) return rc;
@@ -152,6 +187,7 @@ extern "C" int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t ma
     k_box_partial<<<nitems, 256, 0, st>>>(items, pos_cm, n, part, status);
     k_cloud_boxes<<<1, 32, 0, st>>>(cloud, item_begin, part, max_level, 0, 0.0, 0.0, 0.0);
     k_keys<<<blocks, 256, 0, st>>>(cloud, 1, pos_cm, n, max_level, kA, vA);
+    if (cudaGetLastError() != cudaSuccess) return SPH3_ERR_CUDA;
     const int nb = (int)((n + kSortTile - 1) / kSortTile);
     const int passes = (3 * max_level + 7) / 8;
     uint64_t *kin = kA, *kout = kB;
@@ -168,6 +204,7 @@ extern "C" int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t ma
         vin = vout;
         vout = tv;
     }
-    k_na_output<<<blocks, 256, 0, st>>>(kin, vin, n, order, keys);
+    if (cudaGetLastError() != cudaSuccess) return SPH3_ERR_CUDA;
+    k_na_output<<<blocks, 256, 0, st>>>(kin, vin, n, order, keys, status, status_out);
     return cudaGetLastError() == cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA;
 }

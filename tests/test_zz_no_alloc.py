@@ -14,7 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc_sort(pos_np, max_level):
+def _noalloc_sort(pos_np, max_level, want_order=True, want_keys=True):
     import torch
     from sph_3_b200 import _lib
     lib = _lib.load()
@@ -22,13 +22,16 @@ def _noalloc_sort(pos_np, max_level):
     pos = torch.from_numpy(np.ascontiguousarray(pos_np)).cuda()
     order = torch.full((n,), -1, dtype=torch.int64, device="cuda")
     keys = torch.zeros(n, dtype=torch.int64, device="cuda")
+    status = torch.full((1,), 0x5A5A, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     rc = lib.sph3_morton_sort_noalloc(ctypes.c_void_p(pos.data_ptr()), n, max_level,
-                                      ctypes.c_void_p(order.data_ptr()), ctypes.c_void_p(keys.data_ptr()),
-                                      ctypes.c_void_p(stream))
+                                      ctypes.c_void_p(order.data_ptr()) if want_order else None,
+                                      ctypes.c_void_p(keys.data_ptr()) if want_keys else None,
+                                      ctypes.c_void_p(status.data_ptr()), ctypes.c_void_p(stream))
     assert rc == 0, _lib.error_string(rc)
     torch.cuda.synchronize()
-    return order.cpu().numpy(), keys.cpu().numpy().view(np.uint64)
+    return (order.cpu().numpy() if want_order else None,
+            keys.cpu().numpy().view(np.uint64) if want_keys else None, int(status.cpu()[0]))
 
 
 def _allocating_sort(pos_np, max_level):
@@ -45,19 +48,45 @@ def test_noalloc_sort_matches_allocating_entry_point_twice():
     from sph_3_b200.ic import evrard
     cases = [(evrard(50000, seed=21)["pos"], 16), (evrard(65536, seed=22)["pos"] * 3.0 + 0.25, 21)]
     for pos, lvl in cases:  # two calls in a row on the shared static scratch
-        o1, k1 = _noalloc_sort(pos, lvl)
+        o1, k1, st = _noalloc_sort(pos, lvl)
         o2, k2 = _allocating_sort(pos, lvl)
+        assert st == 0
         assert np.array_equal(k1, k2)
         assert np.array_equal(o1, o2)
 
 
-def test_noalloc_sort_rejects_sizes_above_its_maximum():
+@pytest.mark.parametrize("n", [1, 7, 4095, 4097])
+def test_noalloc_sort_small_sizes_and_single_outputs(n):
+    """Sizes below and around one sort tile (4,096 keys), with each output
+    alone, against the allocating path."""
+    pos = np.random.default_rng(n).normal(size=(n, 3))
+    o2, k2 = _allocating_sort(pos, 16)
+    o1, k1, st = _noalloc_sort(pos, 16)
+    assert st == 0 and np.array_equal(o1, o2) and np.array_equal(k1, k2)
+    o1, _, _ = _noalloc_sort(pos, 16, want_keys=False)
+    _, k1, _ = _noalloc_sort(pos, 16, want_order=False)
+    assert np.array_equal(o1, o2) and np.array_equal(k1, k2)
+
+
+def test_noalloc_sort_reports_non_finite_input():
+    pos = np.random.default_rng(3).random((1000, 3))
+    pos[17, 1] = np.nan
+    _, _, st = _noalloc_sort(pos, 16)
+    from sph_3_b200 import _lib
+    assert st & _lib.C["SPH3_STATUS_NAN_INPUT"]
+    _, _, st = _noalloc_sort(pos[:17], 16)  # cleared by the next call
+    assert st == 0
+
+
+def test_noalloc_sort_rejects_bad_arguments():
     import torch
     from sph_3_b200 import _lib
     lib = _lib.load()
     n = 65537
     pos = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
     order = torch.zeros(n, dtype=torch.int64, device="cuda")
-    rc = lib.sph3_morton_sort_noalloc(ctypes.c_void_p(pos.data_ptr()), n, 16, ctypes.c_void_p(order.data_ptr()),
-                                      None, None)
-    assert rc == _lib.C["SPH3_ERR_TOO_LARGE"]
+    p, o = ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(order.data_ptr())
+    assert lib.sph3_morton_sort_noalloc(p, n, 16, o, None, None, None) == _lib.C["SPH3_ERR_TOO_LARGE"]
+    for lvl in (3, 22):
+        assert lib.sph3_morton_sort_noalloc(p, 100, lvl, o, None, None, None) == _lib.C["SPH3_ERR_INVALID_ARG"]
+    assert lib.sph3_morton_sort_noalloc(p, 100, 16, None, None, None, None) == _lib.C["SPH3_ERR_INVALID_ARG"]
