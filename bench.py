@@ -45,13 +45,15 @@ DT = 1e-3
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=N_DEFAULT)
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-errors", action="store_true")
+    p.add_argument("--no-ensemble", action="store_true")
     p.add_argument("--leaf", type=int, default=0)
     p.add_argument("--clouds", type=int, default=0,
                    help="batched ensemble instead of one cloud: this many independent Evrard clouds, N "
@@ -64,18 +66,39 @@ def parse():
 
 # ------------------------------------------------------------ clocks
 class Clocks:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """SM clock and throttle-reason samples while the timed region runs: NVML
+    every 10 ms from a thread (nvidia-smi at 200 ms if NVML is missing)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.01):
         self.index = index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of reason names)
         self.lines = []
+        self._stop = threading.Event()
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:  # noqa: BLE001 - fall back to nvidia-smi
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -85,55 +108,94 @@ class Clocks:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        pn = self.nvml
+        while not self._stop.is_set():
+            try:
+                sm = float(pn.nvmlDeviceGetClockInfo(self.h, pn.NVML_CLOCK_SM))
+                r = int(pn.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((sm, self.smax, {k for k, b in self.bits.items() if r & b}))
+            except Exception:  # noqa: BLE001
+                pass
+            self._stop.wait(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
+            f = [x.strip() for x in line.strip().split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
+                self.samples.append((float(f[1]), float(f[2]),
+                                     {nm for k, nm in enumerate(self.NAMES) if f[5 + k].lower().startswith("active")}))
             except ValueError:
                 continue
-            for k, nm in enumerate(names):
-                if f[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+
+    def stop(self):
+        self._stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=2)
+            src = "nvml, %d ms" % round(self.period * 1e3)
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            src = "nvidia-smi, 200 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
+        sm = [x[0] for x in self.samples]
+        reasons = set()
+        for x in self.samples:
+            reasons |= x[2]
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_min_mhz": float(np.min(sm)) if sm else None,
+                "sm_max_mhz": self.samples[-1][1] if self.samples else None,
+                "reasons": sorted(reasons), "samples": len(sm), "source": src}
 
 
 # ------------------------------------------------------------ CPU baseline
+WORKLOAD = ("Evrard collapse N=%d, N_ngb=64, theta=0.5, eps=0.01, dt=1e-3, one full KDK step per update")
+
+
+def cpu_state(n, seed=0, n_ngb=64):
+    """The CPU measurements' shared, untimed set-up (both arms use it): the
+    Evrard ICs and, since an O(N^2) h search over all N particles is out of
+    reach on the host, h and rho from the profile's expected number density
+    n(r) = N / (2 pi r) (M = R = 1): h = 0.5 (3 N_ngb / (4 pi n(r)))^(1/3),
+    rho = n(r) / N.  The per-row cost of the reference's loops does not depend
+    on these values except through the h search's iteration count, which
+    cpu_rows_time settles before timing."""
+    from sph_3_b200.ic import evrard
+    ic = evrard(n, seed=seed)
+    r = np.maximum(np.linalg.norm(ic["pos"], axis=1), 1e-6)
+    nd = n / (2.0 * np.pi * r)
+    ic["h"] = 0.5 * (3.0 * n_ngb / (4.0 * np.pi * nd)) ** (1.0 / 3.0)
+    ic["rho"] = nd / n
+    return ic
+
+
 def cpu_rows_time(ic, rows, n_ngb=64):
     """Wall time of the reference CPU algorithm (oracle C restatement, all
     threads) for the given rows: h search, density, direct gravity,
-    hydro acceleration and du/dt, each an all-N loop per row."""
+    hydro acceleration and du/dt, each an all-N loop per row.  Before the
+    clock starts, the rows' h is brought into the window (untimed), as the
+    driver's loop calls the h search with the previous step's h."""
     import oracle as oc
     pos, m = ic["pos"], ic["m"]
     n = pos.shape[0]
     eps = np.full(n, 0.01)
-    h = ic["h"]
+    h = ic["h"].copy()
+    h[rows] = oc.h_smooth_rows(pos, h, rows, n_ngb=n_ngb, tol=5, max_iter=2000)[0]
     u = ic["u"]
     gama = 5.0 / 3.0
+    rho = ic["rho"]
+    P = (gama - 1.0) * rho * u
+    c = np.sqrt(gama * (gama - 1.0) * u)
     t0 = time.perf_counter()
     oc.h_smooth_rows(pos, h, rows, n_ngb=n_ngb, tol=5, max_iter=2000)
     oc.density_rows(pos, m, h, rows)
     oc.grav_direct_rows(pos, m, 1.0, eps, rows)
-    rho = ic["rho"]
-    P = (gama - 1.0) * rho * u
-    c = np.sqrt(gama * (gama - 1.0) * u)
     oc.hydro_rows(pos, ic["vel"], rho, P, c, h, m, 0, 1.0, 2.0, 0.1, rows=rows, want_dudt=False)
     oc.hydro_rows(pos, ic["vel"], rho, P, c, h, m, 0, 1.0, 2.0, 0.1, rows=rows, want_acc=False)
     return time.perf_counter() - t0
@@ -156,24 +218,28 @@ def rows_for(ic, target_s, rng, threads):
     return int(min(n, max(k, target_s / max(per_row, 1e-9))))
 
 
-def cpu_baseline(ic, target_s=12.0):
+def cpu_sample_desc(nrows, n, secs):
+    return ("%d random rows x all %d particles of the N=%d Evrard step (h search from an in-window h, density, "
+            "direct gravity, hydro accel, du/dt), %.1f s wall; rows / time = particle-updates/s" %
+            (nrows, n, n, secs))
+
+
+def cpu_baseline(n, target_s=12.0):
     import oracle as oc
     oc.build()
     threads = oc.num_threads()
+    ic = cpu_state(n)
     rng = np.random.default_rng(123)
-    n = ic["pos"].shape[0]
     nrows = rows_for(ic, target_s, rng, threads)
     rows = rng.choice(n, nrows, replace=False)
     t = cpu_rows_time(ic, rows)
     return {"value": nrows / t, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-            "sample": "%d random rows x all %d particles of the N=%d Evrard step (h search, density, "
-                      "direct gravity, hydro accel, du/dt), %.1f s wall; extrapolated per particle" %
-                      (nrows, n, n, t)}
+            "sample": cpu_sample_desc(nrows, n, t)}
 
 
 # ------------------------------------------------------------ GPU arm
-# DRAM bytes per particle of one gravity launch, from the ncu capture
-# summarised in profiles/k_gravity_f32_evrard262k.md (14.07 MB at N=262144)
+# DRAM bytes per particle of one gravity launch, from an ncu capture of the
+# gravity walk at N=262144 (dram__bytes_read.sum + dram__bytes_write.sum = 14.07 MB)
 GRAV_DRAM_BYTES_PER_PARTICLE = 14.07e6 / 262144
 
 
@@ -182,6 +248,71 @@ def make_ic(n, seed, clouds=0):
     if clouds:
         return evrard_batch(ncloud=clouds, seed=seed, n_min=2048, n_max=65536)
     return evrard(n, seed=seed)
+
+
+def stated_errors(ctx, n, grav_rows=4096, sph_rows=256):
+    """Errors of the mixed path stated beside the throughput, measured on the
+    benchmark's own state after the timed steps (outside the timed region):
+    Barnes-Hut gravity against the FP64 direct sum (GPU, sph3_gravity_direct_rows)
+    on grav_rows random particles; density, hydro acceleration and du/dt
+    recomputed at the current state against the oracle (the reference's FP64
+    formulas on the host) on sph_rows random particles, with the GPU's own h,
+    and for the hydro terms its own rho, P, c."""
+    import oracle as oc
+    rng = np.random.default_rng(99)
+    rows = rng.choice(n, grav_rows, replace=False)
+    acc = ctx.get_field("acc_g")[rows]
+    ref, _ = ctx.gravity_direct_rows(rows)
+    eg = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    ctx.compute("density", "acc_sph", "dudt")
+    f = {k: ctx.get_field(k) for k in ("pos", "vel", "m", "h", "rho", "P", "c", "acc_sph", "dudt")}
+    r2 = rng.choice(n, sph_rows, replace=False)
+    rho = oc.density_rows(f["pos"], f["m"], f["h"], r2)
+    erho = np.abs(f["rho"][r2] - rho) / rho
+    a, du = oc.hydro_rows(f["pos"], f["vel"], f["rho"], f["P"], f["c"], f["h"], f["m"], rows=r2)
+    ea = np.linalg.norm(f["acc_sph"][r2] - a, axis=1) / np.linalg.norm(a, axis=1)
+    edu = np.abs(f["dudt"][r2] - du) / np.maximum(np.abs(du), 1e-6 * np.sqrt(np.mean(du ** 2)))
+
+    def stats(e):
+        return {"median": float(np.median(e)), "p95": float(np.percentile(e, 95)),
+                "p99": float(np.percentile(e, 99)), "max": float(np.max(e))}
+
+    return {"gravity_bh_theta0.5_vs_fp64_direct": dict(stats(eg), rows=int(grav_rows), bound_median=1e-3),
+            "density_vs_oracle": dict(stats(erho), rows=int(sph_rows), bound_max=1e-5),
+            "hydro_accel_vs_oracle": dict(stats(ea), rows=int(sph_rows)),
+            "dudt_vs_oracle": dict(stats(edu), rows=int(sph_rows)),
+            "how": "after the timed steps, outside the timed region; relative errors per particle "
+                   "(vector norm for accelerations)"}
+
+
+def run_ensemble(args, local_rank, timed, world, ncloud=256):
+    """The batched-ensemble workload: ncloud Evrard clouds, N log-uniform in
+    [2048, 65536], M and R in [0.5, 2], one launch sequence per pass, walk
+    parameters from the autotuner (cached per workload shape), mixed and
+    FP64 step times."""
+    from sph_3_b200 import Config, Context, autotune
+    from sph_3_b200.ic import evrard_batch
+    b = evrard_batch(ncloud=ncloud, seed=0, n_min=2048, n_max=65536)
+    nt = int(b["counts"].sum())
+    out = {"workload": "%d independent Evrard clouds, N log-uniform in [2048, 65536] (N=%d in total), "
+                       "M, R uniform in [0.5, 2], one full KDK step of every cloud per update" % (ncloud, nt),
+           "n_total": nt}
+    for prec in ("mixed", "fp64"):
+        ctx = Context(Config(precision=prec), device=local_rank)
+        ctx.set_clouds(b["counts"])
+        ctx.set_particles(b["pos"], b["m"], vel=b["vel"], u=b["u"])
+        ctx.first_step(DT)
+        if prec == "mixed":
+            best, times = autotune.autotune(ctx, steps=3, warmup=2,
+                                            grid={"leaf_size": (8, 12, 16, 24), "walk_warps": (2, 4, 8),
+                                                  "stack_cap": (768,)})
+            out["autotuned"] = best
+        k = 10 if prec == "mixed" else 4
+        ms = timed(ctx, k, 3)
+        out[prec] = {"ms_per_step": ms / k, "value": world * nt * k / (ms / 1e3), "status": ctx.status_names()}
+        ctx.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -272,18 +403,18 @@ def run_ours(args, rank, world, local_rank):
     # ---- e2e through host buffers (pinned), C ABI per step
     e2e = None
     if not args.no_e2e:
+        # the reference loop's state (sph_serial.py:142-193 keeps r, v, acc, h,
+        # u, ut_previous as host arrays): in from and out to page-locked host
+        # buffers every step, through the one C-ABI call that overlaps the
+        # transfers with the step (sph3_step_io)
         fields = ["pos", "vel", "u", "h", "acc", "dudt_prev"]
         host = {f: torch.from_numpy(ctx.get_field(f)).pin_memory() for f in fields}
         outs = {f: torch.empty_like(host[f]).pin_memory() for f in fields}
         bytes_in = sum(host[f].numel() * 8 for f in fields)
-        k_e2e = max(2, min(args.steps, 5))
+        k_e2e = max(3, min(args.steps, 10))
 
         def e2e_step():
-            for f in fields:
-                ctx.set_field(f, host[f])
-            ctx.step(DT, 1)
-            for f in fields:
-                ctx.get_field(f, out=outs[f])
+            ctx.step_io(DT, host, outs)
 
         e2e_step()
         torch.cuda.synchronize()
@@ -301,18 +432,32 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": world * n * k_e2e / dt_e2e, "unit": "particle-updates/s",
                "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(bytes_in),
                "ms_per_step": 1e3 * dt_e2e / k_e2e,
-               "path": "sph3_set_field x6 (pinned host) -> sph3_step -> sph3_get_field x6"}
+               "path": "sph3_step_io: 6 fields in from page-locked host buffers, one KDK step, 6 fields out, "
+                       "transfers on two copy streams overlapping the step"}
+    errors = None
+    if not args.no_errors and rank == 0:
+        errors = stated_errors(ctx, n)
     ctx.close()
 
     # ---- FP64 path, same code
     fp64 = None
     if not args.no_fp64:
         c64 = setup("fp64")
-        ms64 = timed(c64, max(3, args.steps // 2), max(2, args.warmup // 2))
-        k64 = max(3, args.steps // 2)
+        k64 = max(3, args.steps // 4)
+        ms64 = timed(c64, k64, max(3, args.warmup // 2))
         fp64 = {"value": world * n * k64 / (ms64 / 1e3), "ms_per_step": ms64 / k64,
                 "status": c64.status_names()}
+        # per-phase FP64 times (events between phases, no graph), as for the mixed path
+        c64.set_config(c64.config.replace(timing=True))
+        c64.phase_times(clear=True)
+        c64.step(DT, 3)
+        fp64["kernels_ms"] = {k: v / 3 for k, v in c64.phase_times().items()}
         c64.close()
+
+    # ---- batched ensemble (256 clouds), autotuned, in the same process
+    ensemble = None
+    if not args.no_ensemble and not args.clouds:
+        ensemble = run_ensemble(args, local_rank, timed, world)
 
     # ---- roofline of the dominant kernel
     g_flops = (cnt.get("grav_node", 0) * costs.GRAV_NODE_QUAD + cnt.get("grav_part", 0) * costs.GRAV_PART)
@@ -347,8 +492,7 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "TFLOP/s", "frac": ach / fp32_peak,
                 "traffic": GRAV_DRAM_BYTES_PER_PARTICLE * n,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=262144 launch "
-                                  "(14.07 MB), scaled per particle to this N "
-                                  "(profiles/k_gravity_f32_evrard262k.md)",
+                                  "(14.07 MB), scaled per particle to this N",
                 "peak_source": fp32_src + "; MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                 "work": "%.3g node + %.3g particle interactions per launch" % (cnt.get("grav_node", 0),
                                                                                cnt.get("grav_part", 0))}
@@ -360,15 +504,7 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and not args.no_cpu and not args.clouds:
-        # CPU reference needs rho for the hydro rows: use the GPU's FP64 state
-        icb = dict(ic)
-        c2 = Context(Config(precision="fp64", gravity=False), device=local_rank)
-        c2.set_particles(ic["pos"], ic["m"], vel=ic["vel"], u=ic["u"])
-        c2.compute("boot_h", "h", "density")
-        icb["h"] = c2.get_field("h")
-        icb["rho"] = c2.get_field("rho")
-        c2.close()
-        cpu = cpu_baseline(icb)
+        cpu = cpu_baseline(n)
 
     drift = abs((e_end["E"] - e_start["E"]) / e_start["E"]) if e_start["E"] != 0 else None
     line = {
@@ -385,16 +521,19 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f32 pair arithmetic, f64 state/accumulators",
         "data": "synthetic seeded Evrard ICs (r = sqrt(U), isotropic, equal mass)",
-        "config": {"workload": ("Evrard collapse N=%d, N_ngb=64, theta=0.5, eps=0.01, dt=1e-3, one full "
-                                "KDK step per update" % n) if not args.clouds else
+        "config": {"workload": (WORKLOAD % n) if not args.clouds else
                                ("batched ensemble of %d independent Evrard clouds (N=%d in total, each N "
                                 "log-uniform in [2048, 65536]), N_ngb=64, theta=0.5, eps=0.01, dt=1e-3, one "
                                 "full KDK step of every cloud per update, one launch sequence" % (args.clouds, n)),
                    "n_per_gpu": n, "parallelism": "replicas",
-                   "l2": "working set ~0.5 GB per GPU > 126 MB L2 (no flush needed)",
-                   "cuda_graph": True, "overrides": list(args.set)},
+                   "l2": "working set ~0.5 GB per GPU > 126 MB L2 (no flush needed)"},
+        "run": {"cuda_graph": True, "overrides": list(args.set)},
         "fp64": fp64,
         "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+        "mixed_over_fp64_per_phase": ({k: fp64["kernels_ms"][k] / v for k, v in ph.items() if v > 0}
+                                      if fp64 else None),
+        "errors": errors,
+        "ensemble": ensemble,
         "energy_drift_timed_region": drift,
         "status": status,
         "e2e": e2e,
@@ -411,18 +550,18 @@ def run_ours(args, rank, world, local_rank):
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU algorithm (the oracle's C restatement of
+    sph_code/libsx.py, all host threads) on the same workload: each step is a
+    bounded sample of rows of the N = 1M step, timed whole; value = rows
+    processed / time."""
     if rank != 0:
         return None
     n = args.n
-    ic = make_ic(n, seed=0)
     import oracle as oc
     oc.build()
     threads = oc.num_threads()
+    ic = cpu_state(n)
     rng = np.random.default_rng(7)
-    # h from a kd-free bootstrap on a subsample is not needed: the CPU loop
-    # cost does not depend on the h values beyond the iteration count
-    ic["h"] = np.full(n, 0.5 * (64.0 / n) ** (1.0 / 3.0) * 1.2)
-    ic["rho"] = np.full(n, 1.0)
     rows_per_step = rows_for(ic, 4.0, rng, threads)
     for _ in range(args.warmup):
         cpu_rows_time(ic, rng.choice(n, max(threads, rows_per_step // 8), replace=False))
@@ -437,13 +576,14 @@ def run_reference(args, rank, world):
         "impl": "reference",
         "metric": "particle-updates/sec per SPH+gravity step at N=1M (mixed FP32/FP64)",
         "value": value, "unit": "particle-updates/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * n / value, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded Evrard ICs",
-        "config": {"workload": "Evrard collapse N=%d, N_ngb=64, one full step per update" % n},
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / args.steps,
+        "ms_per_full_step_extrapolated": 1e3 * n / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic seeded Evrard ICs (r = sqrt(U), isotropic, equal mass)",
+        "config": {"workload": WORKLOAD % n, "n_per_gpu": n, "parallelism": "replicas",
+                   "l2": "working set ~0.5 GB per GPU > 126 MB L2 (no flush needed)"},
         "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-                         "sample": "%d random rows x all %d particles per step (h search, density, direct "
-                                   "gravity, hydro accel, du/dt), extrapolated per particle" %
-                                   (rows_per_step, n)},
+                         "sample": "each step: " + cpu_sample_desc(rows_per_step, n, t_tot / args.steps)},
         "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -1123,7 +1123,7 @@ __device__ __forceinline__ float min_image(float d, float L) {
 }
 
 template <int VISC, bool ACC, bool DU>
-__global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
+__global__ void __launch_bounds__(128, 7) k_hydro_list(LArgs A) {
     unsigned long long pairs = 0;
     const float alpha = A.alpha, beta = A.beta, eta2 = A.eta2;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n;
@@ -1137,9 +1137,15 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
         const float th = tt.w;
         const float tf = VISC == SPH3_VISC_BALSARA ? A.pk_thm[i].w : 0.f;
         float ax = 0.f, ay = 0.f, az = 0.f, du = 0.f, vmax = 0.f;
-        const int *row = A.list + (size_t)i * A.list_cap;
-        // software pipeline: the next source's record is in flight while this pair runs
-        int jn = cnt > 0 ? row[0] : 0;
+        // The row's indices come 4 at a time (16-byte loads, one chunk ahead:
+        // a row holds list_cap slots, a multiple of 8, so whole chunks stay
+        // inside it) and the next source's record is in flight while this
+        // pair runs, so a pair waits on one load, not on an index load followed
+        // by a record load.
+        const int4 *row4 = reinterpret_cast<const int4 *>(A.list + (size_t)i * A.list_cap);
+        int4 ids = cnt > 0 ? row4[0] : make_int4(0, 0, 0, 0);
+        int4 ids_next = cnt > 4 ? row4[1] : ids;
+        int jn = ids.x;
         float4 q0, q1, q2;
         if (cnt > 0) {
             q0 = A.hrec[3 * jn];
@@ -1149,8 +1155,14 @@ __global__ void __launch_bounds__(256) k_hydro_list(LArgs A) {
         for (int k = 0; k < cnt; ++k) {
             const float4 r0 = q0, r1 = q1, r2 = q2;  // {pos}, {vx, vy, vz, m}, {rho, P/rho^2, c, h}
             const int j = jn;
-            if (k + 1 < cnt) {
-                jn = row[k + 1];
+            const int kn = k + 1;
+            if (kn < cnt) {
+                const int u = kn & 3;
+                if (u == 0) {
+                    ids = ids_next;
+                    if (kn + 4 < cnt) ids_next = row4[(kn >> 2) + 1];
+                }
+                jn = u == 0 ? ids.x : (u == 1 ? ids.y : (u == 2 ? ids.z : ids.w));
                 q0 = A.hrec[3 * jn];
                 q1 = A.hrec[3 * jn + 1];
                 q2 = A.hrec[3 * jn + 2];
@@ -1466,9 +1478,11 @@ static void list_dispatch(const LArgs &L, bool fp64, bool acc, bool du, int bloc
         else k_hydro_list_f64<V, false, true><<<blocks, 256, 0, st>>>(L);
         return;
     }
-    if (acc && du) k_hydro_list<V, true, true><<<blocks, 256, 0, st>>>(L);
-    else if (acc) k_hydro_list<V, true, false><<<blocks, 256, 0, st>>>(L);
-    else k_hydro_list<V, false, true><<<blocks, 256, 0, st>>>(L);
+    // 128-thread blocks at <= 72 registers: 7 blocks (28 warps) per SM
+    const int b128 = (int)std::min<int64_t>((L.n + 127) / 128, (int64_t)blocks * 2);
+    if (acc && du) k_hydro_list<V, true, true><<<b128, 128, 0, st>>>(L);
+    else if (acc) k_hydro_list<V, true, false><<<b128, 128, 0, st>>>(L);
+    else k_hydro_list<V, false, true><<<b128, 128, 0, st>>>(L);
 }
 
 void launch_hydro(State &S, const Params &P, bool want_acc, bool want_dudt, cudaStream_t st) {

@@ -5,11 +5,13 @@ import json
 import os
 import subprocess
 import sys
+import time
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_json_line():
+    t0 = time.time()
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "3000",
                           "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=600,
                          cwd=ROOT)
@@ -26,3 +28,9 @@ def test_reference_arm_json_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    # the timed steps are measured (not extrapolated) and fit in the run
+    assert 0 < d["ms_per_step"] * d["steps"] < 1e3 * (time.time() - t0)
+    # the same workload string as the GPU arm's line
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"]["workload"] == bench.WORKLOAD % 3000

@@ -5,6 +5,9 @@ through size-free properties (the CPU oracle cannot run them):
   periodic unit box, hydro only, to t = 0.05: mixed vs the FP64 GPU path (L1
   of density), total energy conservation, and the blast radius against the
   Sedov-Taylor solution R = xi0 (E t^2 / rho)^(1/5), xi0 = 1.15 for gamma = 5/3;
+  at the evolved state of each path, density, hydro acceleration and du/dt
+  against the oracle (the reference's formulas with the periodic minimum
+  image) on 2,048 sampled rows, with the GPU's own h, v, rho, P, c;
 * Kelvin-Helmholtz slab, 4,194,304 particles, 200 steps: energy and momentum
   conservation, no status flags, mixed vs FP64 density.
 Both use the global time step of the reference's per-particle criterion."""
@@ -14,7 +17,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _run(ic, prec, t_end=None, nsteps=None, dt_max=1e-3):
+def _run(ic, prec, t_end=None, nsteps=None, dt_max=1e-3, check=None):
     from sph_3_b200 import Config, Context
     from sph_3_b200 import validate as V
     ctx = Context(Config(precision=prec, gravity=False, box=ic["box"]))
@@ -33,15 +36,46 @@ def _run(ic, prec, t_end=None, nsteps=None, dt_max=1e-3):
     assert ctx.status() == 0, ctx.status_names()
     out = {k: ctx.get_field(k) for k in ("pos", "vel", "rho", "u", "m")}
     out["E0"], out["E1"], out["t"], out["steps"] = E0, ctx.energy(), t, steps
+    if check is not None:
+        check(ctx)
     ctx.close()
     return out
 
 
-def test_sedov_128_cubed_to_t005():
+def _check_vs_oracle(oc, box, prec, tol_rho, tol_med, tol_max, nrows=2048):
+    """Density, hydro acceleration and du/dt of the context's current state
+    against the oracle on sampled rows (periodic minimum image)."""
+
+    def check(ctx):
+        ctx.compute("density", "acc_sph", "dudt")
+        assert ctx.status() == 0, ctx.status_names()
+        f = {k: ctx.get_field(k) for k in ("pos", "vel", "m", "h", "rho", "P", "c", "acc_sph", "dudt")}
+        rows = np.random.default_rng(11).choice(f["pos"].shape[0], nrows, replace=False)
+        # the blast and its shell are few rows of a 2M lattice: sample them too
+        hot = np.argsort(-ctx.get_field("u"))[:256]
+        rows = np.unique(np.concatenate([rows, hot]))
+        rho = oc.density_rows(f["pos"], f["m"], f["h"], rows, box=box)
+        e_rho = np.abs(f["rho"][rows] - rho) / rho
+        acc, du = oc.hydro_rows(f["pos"], f["vel"], f["rho"], f["P"], f["c"], f["h"], f["m"], rows=rows,
+                                box=box)
+        e_acc = np.linalg.norm(f["acc_sph"][rows] - acc, axis=1) / np.maximum(
+            np.linalg.norm(acc, axis=1), 1e-6 * np.sqrt(np.mean(np.sum(acc ** 2, axis=1))))
+        e_du = np.abs(f["dudt"][rows] - du) / np.maximum(np.abs(du), 1e-6 * np.sqrt(np.mean(du ** 2)))
+        print("Sedov t=0.05 %s vs oracle on %d rows: rho max %.2e; a_hydro median %.2e max %.2e; "
+              "du/dt median %.2e max %.2e" % (prec, rows.size, e_rho.max(), np.median(e_acc), e_acc.max(),
+                                              np.median(e_du), e_du.max()))
+        assert e_rho.max() < tol_rho
+        assert np.median(e_acc) < tol_med and e_acc.max() < tol_max
+        assert np.median(e_du) < tol_med and e_du.max() < tol_max
+
+    return check
+
+
+def test_sedov_128_cubed_to_t005(oc):
     from sph_3_b200.ic import sedov
     ic = sedov(n_side=128, seed=0)
-    mix = _run(ic, "mixed", t_end=0.05)
-    f64 = _run(ic, "fp64", t_end=0.05)
+    mix = _run(ic, "mixed", t_end=0.05, check=_check_vs_oracle(oc, ic["box"], "mixed", 1e-5, 1e-5, 1e-3))
+    f64 = _run(ic, "fp64", t_end=0.05, check=_check_vs_oracle(oc, ic["box"], "fp64", 1e-10, 1e-10, 1e-9))
 
     def drift(o):
         e0 = o["E0"]["KE"] + o["E0"]["U"]
