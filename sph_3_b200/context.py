@@ -94,9 +94,18 @@ def _is_torch(a):
     return type(a).__module__.startswith("torch")
 
 
+# CUDA's handle of the legacy default stream (cudaStreamLegacy)
+_CUDA_STREAM_LEGACY = 1
+
+
 def _stream_ptr():
+    """torch's current stream as a cudaStream_t for the C ABI.  torch reports
+    its legacy default stream as handle 0, which the C ABI reads as "the
+    context's own stream" (not ordered with torch's work), so that one is
+    passed as cudaStreamLegacy."""
     import torch
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h = torch.cuda.current_stream().cuda_stream
+    return ctypes.c_void_p(h if h else _CUDA_STREAM_LEGACY)
 
 
 class Context:
