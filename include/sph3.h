@@ -172,7 +172,9 @@ typedef struct sph3_config {
     int32_t eps_from_h;  /* 1: gravitational softening eps = h after every h search, as the reference GPU
                           * driver's set_eps_of_gas_to_h (Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:584-593);
                           * 0 (default): eps stays as set (the benchmark fixes eps = 0.01) */
-    int32_t reserved_i[1];
+    int32_t step_potential; /* 1: every step's gravity walk also computes the potential; 0 (default): the
+                          * steps compute accelerations only (the reference's loop computes no energies)
+                          * and sph3_energy runs the walk with the potential when it needs a fresh one */
     double gamma;        /* adiabatic index (5/3) */
     double alpha;        /* artificial viscosity alpha (1) */
     double beta;         /* beta of the MG83 form (2) */
@@ -260,7 +262,9 @@ int sph3_step_io(sph3_ctx *ctx, double dt, int32_t nsteps, int32_t nin, const in
 
 /* Global sums in FP64 of the current state: out[0] KE, out[1] thermal energy
  * sum m u, out[2] PE = 1/2 sum m phi, out[3] total, out[4..6] momentum,
- * out[7] mass.  Synchronises `stream`. */
+ * out[7] mass.  When the potential is older than the positions (steps run
+ * with step_potential = 0), it first runs the gravity walk with the potential.
+ * Synchronises `stream`. */
 int sph3_energy(sph3_ctx *ctx, double out[8], void *stream);
 
 /* Device status word (SPH3_STATUS_* bits) accumulated since the last clear.

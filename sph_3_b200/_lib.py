@@ -61,7 +61,7 @@ class Config(ctypes.Structure):
         ("list_cap", ctypes.c_int32),
         ("mac", ctypes.c_int32),
         ("eps_from_h", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 1),
+        ("step_potential", ctypes.c_int32),
         ("gamma", ctypes.c_double),
         ("alpha", ctypes.c_double),
         ("beta", ctypes.c_double),

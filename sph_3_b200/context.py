@@ -57,6 +57,7 @@ class Config:
     list_cap: int = 128            # neighbour-list slots per particle for the hydro pass (0: walk)
     mac: str = "bh"                # multipole acceptance: "bh" (d > s/theta) | "bh_offset" (+ com offset)
     eps_from_h: bool = False       # softening eps = h after every h search (reference GPU driver option)
+    step_potential: bool = False   # every step's gravity also computes the potential (else on demand)
     gamma: float = 5.0 / 3.0
     alpha: float = 1.0
     beta: float = 2.0
@@ -76,7 +77,7 @@ class Config:
         for name in ("n_ngb", "n_ngb_tol", "h_max_iter", "n_boot", "leaf_size", "stack_cap", "max_level",
                      "walk_warps", "list_cap"):
             setattr(c, name, int(getattr(self, name)))
-        for name in ("gravity", "quadrupole", "use_graph", "timing", "eps_from_h"):
+        for name in ("gravity", "quadrupole", "use_graph", "timing", "eps_from_h", "step_potential"):
             setattr(c, name, 1 if getattr(self, name) else 0)
         for name in ("gamma", "alpha", "beta", "eta", "G", "theta", "eps"):
             setattr(c, name, float(getattr(self, name)))

@@ -45,6 +45,7 @@ struct sph3_ctx {
     bool tree_dirty = true;
     bool h_dirty_tree = false;  // node hmax stale
     bool order_dirty = false;   // positions changed since the last sort
+    bool phi_valid = false;     // the potential matches the current positions, masses and eps
     // graphs (one per carried-block parity)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt[2] = {0, 0};
@@ -172,6 +173,7 @@ int validate(const sph3_config *c) {
     if (c->list_cap < 0 || c->list_cap > 1024 || c->list_cap % 8) return SPH3_ERR_INVALID_ARG;
     if (c->mac != SPH3_MAC_BH && c->mac != SPH3_MAC_BH_OFFSET) return SPH3_ERR_INVALID_ARG;
     if (c->eps_from_h != 0 && c->eps_from_h != 1) return SPH3_ERR_INVALID_ARG;
+    if (c->step_potential != 0 && c->step_potential != 1) return SPH3_ERR_INVALID_ARG;
     if (c->stack_cap < 7 * (c->max_level + 2) + 32 || c->stack_cap > 4096) return SPH3_ERR_INVALID_ARG;
     if (!(c->theta >= 0.0) || !(c->eps > 0.0) || !(c->gamma >= 1.0)) return SPH3_ERR_INVALID_ARG;
     for (int d = 0; d < 3; ++d)
@@ -564,7 +566,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
     record(c, 5, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
     record(c, 6, st);
-    if (P.gravity) launch_gravity(S, P, st);
+    if (P.gravity) launch_gravity(S, P, st, c->cfg.step_potential != 0);
     record(c, 7, st);
     const bool serial = P.step_order == SPH3_ORDER_SERIAL;
     launch_hydro(S, P, true, serial, st);
@@ -583,6 +585,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
     if (hk && hk->at_end) hk->at_end(st);
     record(c, 11, st);
     c->inv_valid = false;
+    c->phi_valid = !P.gravity || c->cfg.step_potential != 0;
 }
 
 // staging and copy streams of sph3_step_io, made on first use
@@ -922,6 +925,7 @@ int sph3_set_particles(sph3_ctx *c, int64_t n, const double *pos, const double *
         launch_check_finite(S, st);
     }
     c->have = true;
+    c->phi_valid = false;
     rc = resort_all(c, st);
     if (rc) return rc;
     CK(cudaStreamSynchronize(st));
@@ -950,10 +954,15 @@ int sph3_set_field(sph3_ctx *c, int field, const double *src, int on_device, voi
             // the next step, which sorts anyway
             c->order_dirty = true;
             c->S.list_valid = false;
+            c->phi_valid = false;
             break;
         case SPH3_FIELD_VEL: c->pack_dirty |= kPackVel; break;
         case SPH3_FIELD_MASS:
-        case SPH3_FIELD_EPS: c->pack_dirty |= kPackHme; c->tree_dirty = true; break;
+        case SPH3_FIELD_EPS:
+            c->pack_dirty |= kPackHme;
+            c->tree_dirty = true;
+            c->phi_valid = false;
+            break;
         case SPH3_FIELD_H:
             c->pack_dirty |= kPackHme;
             c->h_dirty_tree = true;
@@ -1020,6 +1029,7 @@ int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
         launch_h_search(S, P, st);
         c->h_dirty_tree = true;
         c->bal_dirty = true;
+        if (P.eps_from_h) c->phi_valid = false;  // eps follows h
     }
     if ((rc = sync_packs(c, st))) return rc;
     if (what & SPH3_DO_DENSITY) {
@@ -1035,7 +1045,10 @@ int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
         c->bal_dirty = false;
     }
     if ((rc = sync_packs(c, st))) return rc;
-    if (what & SPH3_DO_GRAVITY) launch_gravity(S, P, st);
+    if (what & SPH3_DO_GRAVITY) {
+        launch_gravity(S, P, st, true);
+        c->phi_valid = true;
+    }
     if (what & (SPH3_DO_ACC_SPH | SPH3_DO_DUDT))
         launch_hydro(S, P, (what & SPH3_DO_ACC_SPH) != 0, (what & SPH3_DO_DUDT) != 0, st);
     rc = check_launch();
@@ -1066,8 +1079,9 @@ int sph3_first_step(sph3_ctx *c, double dt, void *stream) {
     launch_h_search(S, P, st);
     launch_tree_refit_h(S, P, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
-    if (P.gravity) launch_gravity(S, P, st);
+    if (P.gravity) launch_gravity(S, P, st, true);
     else cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st);
+    c->phi_valid = true;
     launch_hydro(S, P, true, true, st);
     launch_first_u(S, P, dt, st);
     launch_energy(S, P, st);
@@ -1286,6 +1300,16 @@ int sph3_energy(sph3_ctx *c, double out[8], void *stream) {
     if (!c->have) return SPH3_ERR_STATE;
     CK(cudaSetDevice(c->device));
     cudaStream_t st = pick(c, stream);
+    if (!c->phi_valid && c->S.n > 0) {
+        // the steps ran without the potential: one gravity walk with it
+        int rc = sync_packs(c, st);
+        if (rc) return rc;
+        if (c->P.gravity && !c->P.periodic) launch_gravity(c->S, c->P, st, true);
+        else CK(cudaMemsetAsync(c->S.phi, 0, sizeof(double) * c->S.n, st));
+        rc = check_launch();
+        if (rc) return rc;
+        c->phi_valid = true;
+    }
     launch_energy(c->S, c->P, st);
     CK(cudaMemcpyAsync(out, c->S.energy, sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

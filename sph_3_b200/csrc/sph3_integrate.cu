@@ -149,14 +149,17 @@ __global__ void __launch_bounds__(256) k_energy_part(int64_t n, const double *ve
     }
 }
 
-__global__ void k_energy_final(const double *part, int nb, double *out) {
-    if (threadIdx.x < 8) {
-        double t = 0;
-        for (int b = 0; b < nb; ++b) t += part[b * 8 + threadIdx.x];
-        out[threadIdx.x] = t;
-    }
+// one warp per sum: lane l adds the partials l, l + 32, ... in order, then a
+// fixed butterfly combines the lanes (the same order every call)
+__global__ void __launch_bounds__(256) k_energy_final(const double *part, int nb, double *out) {
+    __shared__ double tot[8];
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double t = 0;
+    for (int b = lane; b < nb; b += 32) t += part[b * 8 + q];
+    t = warp_sum(t);
+    if (lane == 0) tot[q] = t;
     __syncthreads();
-    if (threadIdx.x == 0) out[3] = out[0] + out[1] + out[2];
+    if (threadIdx.x < 8) out[threadIdx.x] = threadIdx.x == 3 ? tot[0] + tot[1] + tot[2] : tot[threadIdx.x];
 }
 
 void launch_energy(State &S, const Params &P, cudaStream_t st) {
@@ -166,7 +169,7 @@ void launch_energy(State &S, const Params &P, cudaStream_t st) {
         return;
     }
     k_energy_part<<<kEnergyBlocks, 256, 0, st>>>(S.n, S.vel, S.m, S.u, S.phi, S.energy_part);
-    k_energy_final<<<1, 32, 0, st>>>(S.energy_part, kEnergyBlocks, S.energy);
+    k_energy_final<<<1, 256, 0, st>>>(S.energy_part, kEnergyBlocks, S.energy);
 }
 
 // ------------------------------------------------------------ time step

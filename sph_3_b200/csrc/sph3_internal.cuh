@@ -294,7 +294,7 @@ void launch_eos(State &S, const Params &P, cudaStream_t st);
 int launch_neighbours(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
                       int64_t *offsets_dev, int64_t *idx_dev, int64_t cap, cudaStream_t st);
 // walk_grav.cu
-void launch_gravity(State &S, const Params &P, cudaStream_t st);
+void launch_gravity(State &S, const Params &P, cudaStream_t st, bool with_phi);
 void launch_gravity_direct(State &S, const Params &P, const int64_t *rows_sorted_dev, int64_t nrows,
                            double *acc_dev, double *phi_dev, cudaStream_t st);
 // exact.cu (reference-order FP64 sums in the caller's particle order)

@@ -306,6 +306,95 @@ __device__ __forceinline__ void flush_leaves_compact(const int2 *range, const in
     __syncwarp();
 }
 
+// A staged candidate as NF 32-bit fields (coordinates, h, mass, an index
+// carried as float bits, ...).
+template <int NF>
+struct SoaV {
+    float v[NF];
+};
+
+// As flush_leaves_compact, with the staged candidates kept as NF arrays of 64
+// floats (field f of slot e at tile[64 f + e]) instead of 4-wide entries:
+// load(j, keep) returns the fields of candidate j.  interact(ne) sees entries
+// [0, ne); an odd last batch gets one pad entry (slot ne) with every field
+// set to pad[f], so the entries can be run in pairs, two consecutive entries
+// loading as one float2 per field: a ready packed FP32 operand.
+template <int NF, class Load, class Interact>
+__device__ __forceinline__ void flush_leaves_compact_soa(const int2 *range, const int *leafq, int nleaf, int *lfirst,
+                                                         int *lpre, float *tile, const SoaV<NF> &pad, Load &load,
+                                                         Interact &interact) {
+    const int lane = lane_id();
+    int fill = 0;
+    for (int base = 0; base < nleaf; base += 32) {
+        int cnt = 0, fst = 0;
+        if (base + lane < nleaf) {
+            int2 r = range[leafq[base + lane]];
+            fst = r.x;
+            cnt = r.y;
+        }
+        const int incl = warp_incl_scan(cnt);
+        const int tot = __shfl_sync(kFull, incl, 31);
+        __syncwarp();
+        lfirst[lane] = fst;
+        lpre[lane] = incl - cnt;
+        __syncwarp();
+        const int nl = min(32, nleaf - base);
+        auto fetch = [&](int c0, SoaV<NF> &out) -> bool {
+            const int t = c0 + lane;
+            if (t >= tot) return false;
+            int lo = 0, hi = nl - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (lpre[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            bool keep = true;
+            out = load(lfirst[lo] + (t - lpre[lo]), keep);
+            return keep;
+        };
+        SoaV<NF> cur;
+        bool have = fetch(0, cur);
+        for (int c0 = 0; c0 < tot; c0 += 32) {
+            const unsigned kb = __ballot_sync(kFull, have);
+            if (have) {
+                const int at = fill + __popc(kb & lanemask_lt());
+#pragma unroll
+                for (int f = 0; f < NF; ++f) tile[64 * f + at] = cur.v[f];
+            }
+            fill += __popc(kb);
+            __syncwarp();
+            have = c0 + 32 < tot ? fetch(c0 + 32, cur) : false;
+            if (fill >= 32) {
+                interact(32);
+                __syncwarp();
+                const bool mv = lane < fill - 32;
+                SoaV<NF> rest;
+                if (mv) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) rest.v[f] = tile[64 * f + 32 + lane];
+                }
+                __syncwarp();
+                if (mv) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) tile[64 * f + lane] = rest.v[f];
+                }
+                fill -= 32;
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+    }
+    if (fill > 0) {
+        if ((fill & 1) && lane == 0) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) tile[64 * f + fill] = pad.v[f];
+        }
+        __syncwarp();
+        interact(fill);
+    }
+    __syncwarp();
+}
+
 // Periodic images needed by a group whose reach is R.  Per axis a 3-bit
 // mask: bit 0 the identity, bit 1 the shift -L (reach crosses 0), bit 2 the
 // shift +L (reach crosses L).  Image codes 0..26 combine one option per axis

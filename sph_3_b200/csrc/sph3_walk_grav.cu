@@ -178,8 +178,10 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
     return guard;
 }
 
-// FP64 path: one target per lane, AoS tiles of the FP64 masters.
-template <bool QUAD>
+// FP64 path: one target per lane, AoS tiles of the FP64 masters.  PHI: also
+// the potential (only the node terms are skipped without it; a near pair's
+// softened potential comes with its force).
+template <bool QUAD, bool PHI>
 __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64(GArgs A) {
     using R = double;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
                 ax -= mr3 * dx;
                 ay -= mr3 * dy;
                 az -= mr3 * dz;
-                ph -= M * rinv;
+                if (PHI) ph -= M * rinv;
                 if (QUAD) {
                     const V4<R> b4 = t[e].b;
                     const R qyz = t[e].qyz;
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
                     ax += Qx * rinv5 - tq * dx;
                     ay += Qy * rinv5 - tq * dy;
                     az += Qz * rinv5 - tq * dz;
-                    ph -= (R)0.5 * rQr * rinv5;
+                    if (PHI) ph -= (R)0.5 * rQr * rinv5;
                 }
             }
         };
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
             A.acc_g[i] = A.G * ax;
             A.acc_g[A.n + i] = A.G * ay;
             A.acc_g[2 * A.n + i] = A.G * az;
-            A.phi[i] = A.G * ph;
+            if (PHI) A.phi[i] = A.G * ph;
         }
     }
     n_node = warp_sum(n_node);
@@ -398,7 +400,7 @@ __device__ __forceinline__ void spline_near2(float2 r2, float2 r, float2 rinv, f
 // 24 resident warps per SM (at most 85 registers): the walk part is latency-bound
 constexpr int kGravMinWarpsPerSM = 24;
 
-template <bool QUAD>
+template <bool QUAD, bool PHI>
 __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWarps) k_gravity_f32(GArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTileF));
@@ -467,7 +469,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
                 const float2 rinv2 = __fmul2_rn(rinv, rinv);
                 const float2 rinv3 = __fmul2_rn(rinv2, rinv);
                 float2 s = __fmul2_rn(M, rinv3);
-                pp = __ffma2_rn(M, rinv, pp);
+                if (PHI) pp = __ffma2_rn(M, rinv, pp);
                 if (QUAD) {
                     const float4 c4 = tile.nc[buf][p], d4 = tile.nd[buf][p], e4 = tile.ne[buf][p];
                     float2 qx = __fmul2_rn(lo2(c4), dx);  // Qn d
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
                     const float2 rinv5 = __fmul2_rn(rinv3, rinv2);
                     const float2 rinv7 = __fmul2_rn(rinv5, rinv2);
                     s = __ffma2_rn(__fmul2_rn(w, f2(-2.5f)), rinv7, s);
-                    pp = __ffma2_rn(__fmul2_rn(w, f2(-0.5f)), rinv5, pp);
+                    if (PHI) pp = __ffma2_rn(__fmul2_rn(w, f2(-0.5f)), rinv5, pp);
                     ax = __ffma2_rn(qx, rinv5, ax);
                     ay = __ffma2_rn(qy, rinv5, ay);
                     az = __ffma2_rn(qz, rinv5, az);
@@ -554,7 +556,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
                 ax = __ffma2_rn(mf, dx, ax);
                 ay = __ffma2_rn(mf, dy, ay);
                 az = __ffma2_rn(mf, dz, az);
-                pp = __ffma2_rn(m, pk, pp);
+                if (PHI) pp = __ffma2_rn(m, pk, pp);
             }
         };
         auto flush_leaves_fn = [&](int nl) {
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
             A.acc_g[i] = A.G * (double)fx;
             A.acc_g[A.n + i] = A.G * (double)fy;
             A.acc_g[2 * A.n + i] = A.G * (double)fz;
-            A.phi[i] = -A.G * (double)P;
+            if (PHI) A.phi[i] = -A.G * (double)P;
         }
     }
     n_node = warp_sum(n_node);
@@ -598,22 +600,22 @@ static void allow_smem_g(const void *kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-template <bool QUAD>
+template <bool QUAD, bool PHI>
 static void launch_grav_t(const GArgs &A, State &S, const Params &P, cudaStream_t st) {
     // persistent grid: 32 warps' worth of blocks per SM
     const int blocks = S.num_sms * (32 / P.walk_warps), threads = P.walk_warps * 32;
     if (P.precision == SPH3_PREC_FP64) {
         const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTile<double>)) * P.walk_warps;
-        allow_smem_g((const void *)k_gravity_f64<QUAD>);
-        k_gravity_f64<QUAD><<<blocks, threads, sm, st>>>(A);
+        allow_smem_g((const void *)k_gravity_f64<QUAD, PHI>);
+        k_gravity_f64<QUAD, PHI><<<blocks, threads, sm, st>>>(A);
     } else {
         const size_t sm = warp_mem_bytes(P.stack_cap, sizeof(GTileF)) * P.walk_warps;
-        allow_smem_g((const void *)k_gravity_f32<QUAD>);
-        k_gravity_f32<QUAD><<<blocks, threads, sm, st>>>(A);
+        allow_smem_g((const void *)k_gravity_f32<QUAD, PHI>);
+        k_gravity_f32<QUAD, PHI><<<blocks, threads, sm, st>>>(A);
     }
 }
 
-void launch_gravity(State &S, const Params &P, cudaStream_t st) {
+void launch_gravity(State &S, const Params &P, cudaStream_t st, bool with_phi) {
     if (S.n == 0) return;
     GArgs A;
     A.groups = S.groups;
@@ -647,8 +649,13 @@ void launch_gravity(State &S, const Params &P, cudaStream_t st) {
     A.status = S.status;
     A.counters = S.counters;
     cudaMemsetAsync(A.work, 0, sizeof(int), st);
-    if (P.quadrupole) launch_grav_t<true>(A, S, P, st);
-    else launch_grav_t<false>(A, S, P, st);
+    if (P.quadrupole) {
+        if (with_phi) launch_grav_t<true, true>(A, S, P, st);
+        else launch_grav_t<true, false>(A, S, P, st);
+    } else {
+        if (with_phi) launch_grav_t<false, true>(A, S, P, st);
+        else launch_grav_t<false, false>(A, S, P, st);
+    }
 }
 
 // ------------------------------------------------------------ FP64 direct sum

@@ -308,8 +308,41 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                         }
                     }
                 };
+                // FP32: candidates staged as coordinate arrays and tested two per
+                // packed instruction (d2 bit for bit as in the scalar loop above)
+                float *xs = reinterpret_cast<float *>(wm.tile), *ys = xs + 64, *zs = ys + 64;
+                auto load_xyz = [&](int j, bool &keep) {
+                    const float3 q = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+                    SoaV<3> f;
+                    f.v[0] = q.x + s.x;
+                    f.v[1] = q.y + s.y;
+                    f.v[2] = q.z + s.z;
+                    keep = reaches(gb, make_float3(f.v[0], f.v[1], f.v[2]), reach);
+                    return f;
+                };
+                auto interact_xyz = [&](int ne) {
+                    if (conv) return;
+                    pairs += ne;
+                    const float2 ntx = make_float2(-(float)tx, -(float)tx);
+                    const float2 nty = make_float2(-(float)ty, -(float)ty);
+                    const float2 ntz = make_float2(-(float)tz, -(float)tz);
+                    for (int e = 0; e < ne; e += 2) {
+                        const float2 dx = __fadd2_rn(*reinterpret_cast<const float2 *>(xs + e), ntx);
+                        const float2 dy = __fadd2_rn(*reinterpret_cast<const float2 *>(ys + e), nty);
+                        const float2 dz = __fadd2_rn(*reinterpret_cast<const float2 *>(zs + e), ntz);
+                        float2 d2 = __fmul2_rn(dz, dz);
+                        d2 = __ffma2_rn(dy, dy, d2);
+                        d2 = __ffma2_rn(dx, dx, d2);
+#pragma unroll
+                        for (int k = 0; k < K; ++k) cnt[k] += (d2.x < thr2f[k]) + (d2.y < thr2f[k]);
+                    }
+                };
                 auto flush = [&](int nl) {
-                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                    if constexpr (sizeof(R) == 4)
+                        flush_leaves_compact_soa<3>(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, xs,
+                                                    SoaV<3>{{1e18f, 1e18f, 1e18f}}, load_xyz, interact_xyz);
+                    else
+                        flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
                 };
                 collect_leaves(a, wm, gi.root, gb, reach, false, s, flush);
             }
@@ -737,18 +770,51 @@ __device__ __forceinline__ void density_body(const DArgs &A) {
             // list, and the density terms are summed per target with a
             // segmented warp reduction (fixed order: deterministic).  Lanes no
             // longer idle while the lane with the most neighbours finishes.
-            auto interact_bal = [&](const E *t, int ne) {
+            // the balanced pass's tile: six arrays of 64 floats (x, y, z, h, m and
+            // the source index as float bits), so pass 1 tests two candidates
+            // per packed FP32 instruction (the same roundings as pass 1 above)
+            float *sx = reinterpret_cast<float *>(wm.tile), *sy = sx + 64, *sz = sy + 64, *sh = sz + 64,
+                  *sm = sh + 64, *sj = sm + 64;
+            auto load_soa = [&](int j, bool &keep) {
+                const float4 hm = A.pk_hme[j];
+                const float3 q = rel_to(a.pk_pos[j], gi.ref, gi.s10);
+                SoaV<6> v;
+                v.v[0] = q.x + s.x;
+                v.v[1] = q.y + s.y;
+                v.v[2] = q.z + s.z;
+                v.v[3] = hm.x;
+                v.v[4] = hm.y;
+                v.v[5] = __int_as_float(j);
+                keep = reaches(gb, make_float3(v.v[0], v.v[1], v.v[2]), hmax_g + hm.x);
+                return v;
+            };
+            // Mixed path without div/curl: pass 2 balanced over the warp.  The
+            // in-support (target, entry) pairs of the tile become a task list
+            // ordered by target; lane k runs task k of each chunk of 32 (target
+            // values by shuffle), writes the pair into the target's neighbour
+            // list, and the density terms are summed per target with a
+            // segmented warp reduction (fixed order: deterministic).  Lanes no
+            // longer idle while the lane with the most neighbours finishes.
+            auto interact_bal = [&](int ne) {
                 if (gi.active) pairs += ne;
                 unsigned mask = 0;
                 if (gi.active) {
-                    for (int e = 0; e < ne; ++e) {
-                        const V4<R> p = t[e].p;
-                        const float dx = (float)tx - (float)p.x;
-                        const float dy = (float)ty - (float)p.y;
-                        const float dz = (float)tz - (float)p.z;
-                        const float hs = (float)th + (float)p.w;
-                        mask |= (unsigned)(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= hs * hs) << e;
+                    const float2 ntx = make_float2(-(float)tx, -(float)tx);
+                    const float2 nty = make_float2(-(float)ty, -(float)ty);
+                    const float2 ntz = make_float2(-(float)tz, -(float)tz);
+                    const float2 th2 = make_float2((float)th, (float)th);
+                    for (int e = 0; e < ne; e += 2) {
+                        const float2 dx = __fadd2_rn(*reinterpret_cast<const float2 *>(sx + e), ntx);
+                        const float2 dy = __fadd2_rn(*reinterpret_cast<const float2 *>(sy + e), nty);
+                        const float2 dz = __fadd2_rn(*reinterpret_cast<const float2 *>(sz + e), ntz);
+                        const float2 hs = __fadd2_rn(th2, *reinterpret_cast<const float2 *>(sh + e));
+                        const float2 hs2 = __fmul2_rn(hs, hs);
+                        float2 d2 = __fmul2_rn(dz, dz);
+                        d2 = __ffma2_rn(dy, dy, d2);
+                        d2 = __ffma2_rn(dx, dx, d2);
+                        mask |= ((unsigned)(d2.x <= hs2.x) | ((unsigned)(d2.y <= hs2.y) << 1)) << e;
                     }
+                    if (ne < 32) mask &= (1u << ne) - 1u;  // the pad entry of an odd batch
                 }
                 const int c = __popc(mask);
                 const int incl = warp_incl_scan(c);
@@ -778,22 +844,22 @@ __device__ __forceinline__ void density_body(const DArgs &A) {
                     const int toff = __shfl_sync(kFull, off, tl & 31);
                     float v = 0.f;
                     if (valid) {
-                        const E en = t[e];
                         if (A.list) {
                             const int slot = base + (k - toff);
-                            if (slot < A.list_cap) A.list[(size_t)(gi.first + tl) * A.list_cap + slot] = en.get_j();
+                            if (slot < A.list_cap)
+                                A.list[(size_t)(gi.first + tl) * A.list_cap + slot] = __float_as_int(sj[e]);
                         }
-                        const float dx = qx - (float)en.p.x;
-                        const float dy = qy - (float)en.p.y;
-                        const float dz = qz - (float)en.p.z;
+                        const float dx = qx - sx[e];
+                        const float dy = qy - sy[e];
+                        const float dz = qz - sz[e];
                         const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float ih = __fdividef(2.0f, qh + (float)en.p.w);
+                        const float ih = __fdividef(2.0f, qh + sh[e]);
                         const float q = (d2 > 0.f ? d2 * rsqrtf(d2) : 0.f) * ih;
                         const float ih3 = ih * ih * ih;
                         const float tq = 2.0f - q;
                         const float w_in = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.0f);
                         const float w_out = 0.25f * tq * tq * tq;
-                        v = (float)en.q.x * (kSigF * ih3 * (q <= 1.0f ? w_in : w_out));
+                        v = sm[e] * (kSigF * ih3 * (q <= 1.0f ? w_in : w_out));
                     }
                     // segmented suffix sums over equal keys (keys are non-decreasing)
 #pragma unroll
@@ -812,7 +878,9 @@ __device__ __forceinline__ void density_body(const DArgs &A) {
             };
             auto flush = [&](int nl) {
                 if constexpr (sizeof(R) == 4 && !DC)
-                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact_bal);
+                    flush_leaves_compact_soa<6>(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, sx,
+                                                SoaV<6>{{1e18f, 1e18f, 1e18f, 0.f, 0.f, 0.f}}, load_soa,
+                                                interact_bal);
                 else
                     flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
             };

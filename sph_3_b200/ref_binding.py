@@ -24,7 +24,7 @@ class Config(ctypes.Structure):           # mirrors sph3_config in include/sph3.
         ("n_ngb", I32), ("n_ngb_tol", I32), ("h_max_iter", I32), ("n_boot", I32),
         ("leaf_size", I32), ("stack_cap", I32), ("max_level", I32), ("gravity", I32),
         ("quadrupole", I32), ("use_graph", I32), ("timing", I32), ("walk_warps", I32),
-        ("list_cap", I32), ("mac", I32), ("eps_from_h", I32), ("reserved_i", I32 * 1),
+        ("list_cap", I32), ("mac", I32), ("eps_from_h", I32), ("step_potential", I32),
         ("gamma", F64), ("alpha", F64), ("beta", F64), ("eta", F64), ("G", F64), ("theta", F64), ("eps", F64), ("box", F64 * 3),
         ("reserved_d", F64 * 4)]]
 

@@ -105,3 +105,25 @@ def test_fp32_rate_probe_is_plausible():
     r = _lib.probe_fp32_rate(0)
     print("FP32 probe: %.1f TFLOP/s" % r)
     assert 40.0 < r < 90.0
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_potential_on_demand_equals_every_step(prec):
+    """Steps that skip the potential (the default) give the same
+    accelerations, and sph3_energy computes the same PE on demand, as steps
+    that compute it every step."""
+    from sph_3_b200 import Config, Context
+    from sph_3_b200.ic import evrard
+    ic = evrard(20000, seed=9)
+    out = []
+    for every in (False, True):
+        ctx = Context(Config(precision=prec, step_potential=every))
+        ctx.set_particles(ic["pos"], ic["m"], vel=ic["vel"], u=ic["u"])
+        ctx.first_step(1e-3)
+        ctx.step(1e-3, 3)
+        out.append((ctx.get_field("acc"), ctx.energy(), ctx.get_field("phi")))
+        assert ctx.status() == 0
+        ctx.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1]["PE"] == out[1][1]["PE"] and out[0][1]["E"] == out[1][1]["E"]
+    assert np.array_equal(out[0][2], out[1][2])
