@@ -58,6 +58,15 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+def build_ref(ref_root=None):
+    """Compile oracle/_ref/ref_timestep (the reference's own GPU time-step
+    kernel behind a small driver, oracle/build_ref.sh) where the reference is
+    checked out; returns the binary's path, or None when it is not."""
+    cmd = ["sh", os.path.join(_HERE, "build_ref.sh")] + ([ref_root] if ref_root else [])
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else None
+
+
 def _load():
     global _lib
     if _lib is not None:

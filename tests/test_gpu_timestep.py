@@ -57,3 +57,28 @@ def test_neighbour_max_is_bounded_by_all_pairs_max(oc):
     dt_a, _ = ctx.timestep(0.25, all_pairs=True)
     assert np.all(dt_a <= dt_n * (1 + 1e-12))
     ctx.close()
+
+
+def test_timestep_vs_reference_kernel_golden(golden):
+    """sph3_timestep over every particle (the reference's loop) against the
+    reference's own float32 GPU kernel on the same float32-exact state
+    (tests/golden/timestep_ref.npz): relative 1e-5; div v is recomputed here
+    from the positions and velocities (FP64), the kernel took it rounded."""
+    from sph_3_b200 import Config, Context
+    g = golden("timestep_ref")
+    ctx = Context(Config(precision="fp64", eps=0.01))
+    ctx.set_particles(g["pos"], g["m"], vel=g["vel"], u=g["u"], h=g["h"], eps=g["eps"])
+    ctx.set_field("rho", g["rho"])
+    ctx.set_field("c", g["c"])
+    ctx.set_field("acc", g["acc_tot"])
+    ctx.set_field("acc_g", g["acc_g"])
+    dt, dt_min = ctx.timestep(float(g["c_cfl"]), all_pairs=True)
+    ref = g["dt"].astype(np.float64)
+    err = np.abs(dt - ref) / ref
+    print("time step vs the reference kernel: max rel %.2e" % err.max())
+    assert err.max() < 1e-5
+    assert dt_min == pytest.approx(ref.min(), rel=1e-5)
+    dh = ctx.get_field("dhdt")
+    dref = g["dhdt"].astype(np.float64)
+    assert np.max(np.abs(dh - dref)) < 1e-5 * np.max(np.abs(dref))
+    ctx.close()

@@ -115,3 +115,17 @@ def test_gravity_forms_bitexact(oc, golden):
     # the three full forms agree bit for bit, and the partials sum to the field
     assert np.array_equal(g["acc_sym"], g["acc_x"])
     assert np.allclose(g["mimj"].sum(axis=0), g["acc_sym"], rtol=1e-12, atol=1e-12 * np.abs(g["acc_sym"]).max())
+
+
+def test_timestep_oracle_vs_reference_kernel(oc, golden):
+    """The oracle's FP64 restatement of the time-step criterion against the
+    reference's own GPU kernel dt_array_indiv_dt (float32, run unchanged by
+    tests/golden/make_timestep.py) on the same float32-exact inputs:
+    relative 1e-6 (measured 1.8e-7: the float32 kernel's rounding)."""
+    g = golden("timestep_ref")
+    dt, dh = oc.timestep_rows(g["pos"], g["vel"], g["acc_tot"], g["acc_g"], g["h"], g["c"], g["divV"], g["eps"],
+                              float(g["c_cfl"]), float(g["alpha"]))
+    ref = g["dt"].astype(np.float64)
+    assert np.max(np.abs(dt - ref) / ref) < 1e-6
+    dref = g["dhdt"].astype(np.float64)
+    assert np.max(np.abs(dh - dref)) < 1e-6 * np.max(np.abs(dref))
