@@ -239,8 +239,9 @@ def cpu_baseline(n, target_s=12.0):
 
 # ------------------------------------------------------------ GPU arm
 # DRAM bytes per particle of one gravity launch, from an ncu capture of the
-# gravity walk at N=262144 (dram__bytes_read.sum + dram__bytes_write.sum = 14.07 MB)
-GRAV_DRAM_BYTES_PER_PARTICLE = 14.07e6 / 262144
+# step's gravity walk at N=524288 (dram__bytes_read.sum + dram__bytes_write.sum
+# = 31.12 + 1.79 MB)
+GRAV_DRAM_BYTES_PER_PARTICLE = 32.91e6 / 524288
 
 
 def make_ic(n, seed, clouds=0):
@@ -488,11 +489,11 @@ def run_ours(args, rank, world, local_rank):
     dom = max(ph, key=lambda k: ph[k])
     if dom == "gravity":
         ach = g_flops / (ph["gravity"] / 1e3) / 1e12
-        roof = {"kernel": "k_gravity_f32<QUAD>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+        roof = {"kernel": "k_gravity_f32<QUAD, no potential>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": ach / fp32_peak,
                 "traffic": GRAV_DRAM_BYTES_PER_PARTICLE * n,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=262144 launch "
-                                  "(14.07 MB), scaled per particle to this N",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=524288 launch "
+                                  "(32.91 MB), scaled per particle to this N",
                 "peak_source": fp32_src + "; MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                 "work": "%.3g node + %.3g particle interactions per launch" % (cnt.get("grav_node", 0),
                                                                                cnt.get("grav_part", 0))}
