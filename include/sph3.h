@@ -251,7 +251,9 @@ int sph3_step(sph3_ctx *ctx, double dt, int32_t nsteps, void *stream);
  * the sort, u before the EOS, u_prev and dudt_prev before the kick that
  * updates u; all others before the first kick), and each output leaves on a
  * second copy stream as soon as it is final (positions after the sort, h
- * after the h search, the rest at the end).  An input u without u_prev also
+ * after the h search, u, u_prev, dudt_prev, dudt, rho, P, c, acc_sph and
+ * vsig after the u update -- which the serial order runs before the gravity
+ * walk -- the rest at the end).  An input u without u_prev also
  * sets u_prev (the reference's loop keeps u_previous = u between
  * iterations).  Page-locked host buffers are needed for the overlap
  * (pageable ones work, serialised).  The steps run without the captured

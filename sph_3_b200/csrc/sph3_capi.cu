@@ -59,7 +59,7 @@ struct sph3_ctx {
     double *io_in = nullptr, *io_out = nullptr;
     int64_t io_in_cap = 0, io_out_cap = 0;  // doubles
     cudaStream_t h2d = nullptr, d2h = nullptr;
-    cudaEvent_t io_ev[8] = {};
+    cudaEvent_t io_ev[10] = {};
 };
 
 namespace {
@@ -524,7 +524,7 @@ void record(sph3_ctx *c, int k, cudaStream_t st) {
 // follows the sort (new order in place, packs not yet built), after the h
 // search, before the kick that updates u, and at the end.
 struct StepHooks {
-    std::function<void(cudaStream_t)> after_gather, after_h, before_kick, at_end;
+    std::function<void(cudaStream_t)> after_gather, after_h, before_kick, after_u, at_end;
 };
 
 // One timestep, enqueued on st.  Switches the carried block half way (the
@@ -566,20 +566,33 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
     record(c, 5, st);
     launch_density(S, P, P.visc == SPH3_VISC_BALSARA, st);
     record(c, 6, st);
-    if (P.gravity) launch_gravity(S, P, st, c->cfg.step_potential != 0);
-    record(c, 7, st);
     const bool serial = P.step_order == SPH3_ORDER_SERIAL;
-    launch_hydro(S, P, true, serial, st);
-    record(c, 8, st);
-    if (hk && hk->before_kick) hk->before_kick(st);
+    const bool phi = c->cfg.step_potential != 0;
     if (serial) {
-        launch_kick_update(S, P, dt, true, true, st);
+        // the serial driver's order, with the hydro pass and the u update
+        // (which need no gravity) before the gravity walk, so that u and the
+        // hydro results are final while gravity runs
+        launch_hydro(S, P, true, true, st);
+        record(c, 7, st);
+        if (hk && hk->before_kick) hk->before_kick(st);
+        launch_kick_update(S, P, dt, true, false, st);
+        if (hk && hk->after_u) hk->after_u(st);
+        record(c, 8, st);
+        if (P.gravity) launch_gravity(S, P, st, phi);
+        record(c, 9, st);
+        launch_kick_update(S, P, dt, false, true, st);
     } else {
+        if (P.gravity) launch_gravity(S, P, st, phi);
+        record(c, 7, st);
+        launch_hydro(S, P, true, false, st);
+        record(c, 8, st);
+        if (hk && hk->before_kick) hk->before_kick(st);
         launch_kick_update(S, P, dt, false, true, st);
         record(c, 9, st);
         launch_hydro(S, P, false, true, st);
         record(c, 10, st);
         launch_u_update(S, P, dt, st);
+        if (hk && hk->after_u) hk->after_u(st);
     }
     launch_energy(S, P, st);
     if (hk && hk->at_end) hk->at_end(st);
@@ -626,13 +639,23 @@ int io_stage_in(int f) {
 }
 
 // when an output is final: 0 after the gather (positions), 1 after the h
-// search (h, neighbour counts), 2 at the end of the step
+// search (h, neighbour counts), 2 after the u update (u, its history, the
+// density-pass and hydro results), 3 at the end of the step
 int io_stage_out(int f) {
     switch (f) {
         case SPH3_FIELD_POS: return 0;
         case SPH3_FIELD_H:
         case SPH3_FIELD_NNGB: return 1;
-        default: return 2;
+        case SPH3_FIELD_U:
+        case SPH3_FIELD_U_PREV:
+        case SPH3_FIELD_DUDT:
+        case SPH3_FIELD_DUDT_PREV:
+        case SPH3_FIELD_RHO:
+        case SPH3_FIELD_P:
+        case SPH3_FIELD_C:
+        case SPH3_FIELD_ACC_SPH:
+        case SPH3_FIELD_VSIG: return 2;
+        default: return 3;
     }
 }
 
@@ -647,11 +670,13 @@ void accumulate_times(sph3_ctx *c, bool serial) {
     add(3, 3, 4);
     add(4, 4, 5);
     add(5, 5, 6);
-    add(6, 6, 7);
-    if (serial) {
-        add(7, 7, 8);
-        add(8, 8, 11);
+    if (serial) {  // hydro, u update, gravity, second kick (see enqueue_step)
+        add(7, 6, 7);
+        add(8, 7, 8);
+        add(6, 8, 9);
+        add(8, 9, 11);
     } else {
+        add(6, 6, 7);
         add(7, 7, 8);
         add(8, 8, 9);
         add(7, 9, 10);
@@ -1189,8 +1214,8 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
     if ((rc = sync_packs(c, st, true))) return rc;
     if (!c->P.gravity) CK(cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st));
     // inputs: host -> staging on the copy stream, ordered by when the step needs them
-    CK(cudaEventRecord(c->io_ev[7], st));
-    CK(cudaStreamWaitEvent(c->h2d, c->io_ev[7], 0));
+    CK(cudaEventRecord(c->io_ev[9], st));
+    CK(cudaStreamWaitEvent(c->h2d, c->io_ev[9], 0));
     for (int stage = 0; stage < 4; ++stage) {
         for (int k = 0; k < nin; ++k)
             if (io_stage_in(in_fields[k]) == stage)
@@ -1245,14 +1270,17 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
         hk.before_kick = [&](cudaStream_t s) {
             if (first) scatter(3, s);
         };
-        hk.at_end = [&](cudaStream_t s) {
+        hk.after_u = [&](cudaStream_t s) {
             if (last) gather(2, s);
+        };
+        hk.at_end = [&](cudaStream_t s) {
+            if (last) gather(3, s);
         };
         enqueue_step(c, dt, st, &hk);
         if ((rc = check_launch())) return rc;
     }
     // staging -> host on the other copy stream, each group as soon as it is final
-    for (int stage = 0; stage < 3; ++stage) {
+    for (int stage = 0; stage < 4; ++stage) {
         CK(cudaStreamWaitEvent(c->d2h, c->io_ev[4 + stage], 0));
         for (int k = 0; k < nout; ++k)
             if (io_stage_out(out_fields[k]) == stage)
