@@ -188,8 +188,8 @@ void free_buffers(sph3_ctx *c) {
                     c->staging, c->inv, S.nngb, S.key, S.key_alt, S.perm, S.perm_alt, S.pk_pos, S.pk_hme,
                     S.pk_vel, S.pk_thm, S.sort_hist, S.tree.range, S.tree.child, S.tree.mass, S.tree.com,
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
-                    S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1, S.tree.nchild_tmp,
-                    S.tree.scan_tmp, S.tree.bounds, S.tree.parent, S.tree.arrive, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
+                    S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1,
+                    S.tree.meta, S.tree.parent, S.tree.arrive, S.tree.lvl, S.tree.lb, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
                     S.box_item_begin, S.box_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -298,7 +298,10 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     CK(dalloc(&S.pk_thm, nn));
     CK(cudaMemset(S.pk_thm, 0, sizeof(float4) * nn));
     c->cap_sortblk = (int)((nn + kRsTileKeys - 1) / kRsTileKeys);
-    CK(dalloc(&S.sort_hist, (size_t)256 * (c->cap_sortblk + 1)));
+    // the one-sweep sort's scratch: 8 passes' histograms, tile counters, and a
+    // look-back word per (pass, tile, digit); at least the table of the
+    // three-kernel pass (256 x (tiles + 1))
+    CK(dalloc(&S.sort_hist, (size_t)8 * 256 + 64 + (size_t)8 * 256 * (c->cap_sortblk + 1)));
     const int cap = (int)std::min<int64_t>(2 * nn + ncloud + 64, (int64_t)INT32_MAX - 1);
     c->cap_nodes = cap;
     Tree &T = S.tree;
@@ -320,16 +323,19 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     CK(dalloc(&T.quad1, cap));
     CK(dalloc(&T.gw, 2 * (size_t)cap));
     CK(dalloc(&T.sw, 3 * (size_t)cap));
-    CK(dalloc(&T.nchild_tmp, cap));
     CK(dalloc(&T.parent, cap));
     CK(dalloc(&T.arrive, cap));
     CK(cudaMemset(T.arrive, 0, sizeof(int) * (size_t)cap));
     // a depth holds at most one node per particle
-    CK(dalloc(&T.bounds, 8 * (size_t)(nn + ncloud + 64)));
-    // scan_tmp doubles as depth_begin (+64) and scratch counters
-    CK(dalloc(&T.scan_tmp, (size_t)cap + 128));
-    T.depth_begin = T.scan_tmp + cap;
-    T.total = T.scan_tmp + cap + 96;
+    CK(dalloc(&T.meta, 128));
+    T.depth_begin = T.meta;
+    T.total = T.meta + 96;
+    CK(dalloc(&T.lvl, kLvlEpoch + 1));
+    CK(cudaMemset(T.lvl, 0, sizeof(int) * (kLvlEpoch + 1)));
+    // a depth holds at most n + clouds + 64 nodes: tiles of 64 nodes of the level pass
+    const size_t ntiles = (size_t)(nn + ncloud + 64) / 64 + 2;
+    CK(dalloc(&T.lb, ntiles));
+    CK(cudaMemset(T.lb, 0, sizeof(unsigned long long) * ntiles));
     c->cap_groups = std::max(ngroups, 1);
     CK(dalloc(&S.groups, c->cap_groups));
     CK(dalloc(&S.group_cloud, c->cap_groups));

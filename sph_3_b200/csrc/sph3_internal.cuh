@@ -90,13 +90,14 @@ struct Tree {
     float4 *sw;         // [cap][3] SPH: {box_c}, {box_h}, {first child, nch | level << 8, 0, 0}
     int cap;
     int *depth_begin;   // [max_depth + 2] node id where each depth starts
-    int *nchild_tmp;    // [cap] scan input
-    int *scan_tmp;      // [cap] scan output
-    int *bounds;        // [8][n + ncloud + 64] octant starts of one depth's nodes
+    int *meta;          // [128] depth_begin (first 96) and the scratch counters `total`
     int *parent;        // [cap] parent node (-1 for a root)
     int *arrive;        // [cap] children finished in the bottom-up passes (zero between passes)
     int *total;         // [4] scratch counters
+    int *lvl;           // [kLvlEpoch + 1] per-depth tile counters of the level pass, then the build epoch
+    unsigned long long *lb;  // [tiles of the largest depth] look-back words of the level pass
 };
+constexpr int kLvlEpoch = 64;  // index of the build counter in Tree::lvl (tile counters before it)
 
 // ------------------------------------------------------------ state
 struct State {
@@ -134,7 +135,7 @@ struct State {
     double *energy_part = nullptr;     // per-block FP64 partial sums [nblk][8]
     double *energy = nullptr;          // [8]
     // scratch for the sort
-    uint32_t *sort_hist = nullptr;     // [256 * nblocks]
+    uint32_t *sort_hist = nullptr;     // sort scratch (histograms, tile counters, look-back words)
     int sort_blocks = 0;
     int key_bits = 0;
     int max_level = 0;

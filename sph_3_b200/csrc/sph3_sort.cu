@@ -256,10 +256,12 @@ __global__ void __launch_bounds__(kRsOffsetThreads) k_rs_offsets(uint32_t *hist,
 // staged in shared memory in digit order, so that every digit's run leaves
 // as consecutive addresses (coalesced stores instead of one scattered 8-byte
 // store per key).  The output is the same as scattering each key directly.
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
-                                                           const uint32_t *val_in, uint64_t *key_out,
-                                                           uint32_t *val_out, int64_t n, int shift,
-                                                           const uint32_t *hist, int nblocks) {
+// offsets(d, count of digit d in this tile) gives the output start of the
+// tile's keys of digit d (called by thread d once the counts are known).
+template <class Offsets>
+__device__ __forceinline__ void rs_scatter_tile(const uint64_t *key_in, const uint32_t *val_in, uint64_t *key_out,
+                                                uint32_t *val_out, int64_t n, int shift, int tile_index,
+                                                Offsets &offsets) {
     __shared__ uint32_t wcnt[kRsWarps][256];
     __shared__ uint32_t goff[256];  // output start of the tile's keys of digit d
     __shared__ uint32_t toff[256];  // start of digit d inside the tile
@@ -268,9 +270,8 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
     __shared__ uint8_t sdig[kRsTile];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
-    goff[threadIdx.x] = hist[nblocks * 256 + threadIdx.x] + hist[blockIdx.x * 256 + threadIdx.x];
     __syncthreads();
-    const int64_t tile = (int64_t)blockIdx.x * kRsTile;
+    const int64_t tile = (int64_t)tile_index * kRsTile;
     const int64_t base = tile + (int64_t)w * (kRsItems * 32);
     uint64_t kk[kRsItems];
     uint32_t vv[kRsItems];
@@ -316,6 +317,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
         for (int ww = 0; ww < kRsWarps; ++ww) pre += ww < w ? wsum[ww] : 0u;
         toff[threadIdx.x] = pre + incl - cnt_d;
     }
+    goff[threadIdx.x] = offsets(threadIdx.x, cnt_d);  // output start of the tile's keys of the digit
     __syncthreads();
     uint32_t lpos[kRsItems];
 #pragma unroll
@@ -345,17 +347,112 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_i
     }
 }
 
+// The tile scatter with offsets from the digit-major table of k_rs_offsets
+// (one tile per block, in block order).
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t *key_in,
+                                                           const uint32_t *val_in, uint64_t *key_out,
+                                                           uint32_t *val_out, int64_t n, int shift,
+                                                           const uint32_t *hist, int nblocks) {
+    auto offsets = [&](int d, uint32_t) { return hist[nblocks * 256 + d] + hist[blockIdx.x * 256 + d]; };
+    rs_scatter_tile(key_in, val_in, key_out, val_out, n, shift, blockIdx.x, offsets);
+}
+
+// ---- one sweep per digit pass (the context's sort)
+// All passes' digit histograms in one read of the keys (per-warp private
+// tables in shared memory, then one atomic per bin and block); the scatter
+// of each pass then takes its tiles in order from an atomic counter and finds
+// each digit's offset over the earlier tiles by decoupled look-back: a tile
+// publishes its count of each digit (AGG), adds up its predecessors' counts
+// back to one that knows its inclusive prefix (INCL) and publishes its own.
+// One launch per pass instead of histogram + table scan + scatter.  Every
+// predecessor tile was taken by a running block, so each wait ends; waits are
+// bounded all the same and raise SPH3_STATUS_SORT if one ever ran out.
+constexpr int kHaThreads = 128;
+constexpr int kMaxPasses = 8;
+constexpr uint32_t kOsAgg = 1u << 30, kOsIncl = 2u << 30, kOsMask = (1u << 30) - 1u;
+constexpr int kOsMaxSpin = 1 << 22;
+
+__global__ void __launch_bounds__(kHaThreads) k_rs_hist_all(const uint64_t *key, int64_t n, int passes,
+                                                            uint32_t *hist_all) {
+    __shared__ uint32_t h[kHaThreads / 32][kMaxPasses][256];
+    const int w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (kHaThreads / 32) * kMaxPasses * 256; i += kHaThreads) (&h[0][0][0])[i] = 0;
+    __syncthreads();
+    for (int64_t k = (int64_t)blockIdx.x * kHaThreads + threadIdx.x; k < n; k += (int64_t)gridDim.x * kHaThreads) {
+        const uint64_t kv = key[k];
+        for (int p = 0; p < passes; ++p) atomicAdd(&h[w][p][(kv >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kHaThreads) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int q = 0; q < kHaThreads / 32; ++q) t += (&h[q][0][0])[i];
+        if (t) atomicAdd(hist_all + i, t);
+    }
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_onesweep(const uint64_t *key_in, const uint32_t *val_in,
+                                                            uint64_t *key_out, uint32_t *val_out, int64_t n,
+                                                            int pass, const uint32_t *hist_all, uint32_t *state,
+                                                            int *tile_ctr, unsigned *status) {
+    __shared__ int s_tile;
+    __shared__ uint32_t wtot[kRsWarps];
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr + pass, 1);
+    // exclusive scan over digits of this pass's global histogram: digit bases
+    const int d0 = threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t hd = hist_all[pass * 256 + d0];
+    const uint32_t incl = (uint32_t)warp_incl_scan((int)hd);
+    if (lane == 31) wtot[w] = incl;
+    __syncthreads();
+    uint32_t dbase = incl - hd;
+#pragma unroll
+    for (int q = 0; q < kRsWarps; ++q) dbase += q < w ? wtot[q] : 0u;
+    const int tile = s_tile;
+    uint32_t *st = state + (size_t)tile * 256;
+    auto offsets = [&](int d, uint32_t cnt) -> uint32_t {
+        if (tile == 0) {
+            atomicExch(st + d, kOsIncl | cnt);
+            return dbase;
+        }
+        atomicExch(st + d, kOsAgg | cnt);
+        uint32_t excl = 0;
+        int j = tile - 1, spins = 0;
+        while (j >= 0) {
+            const uint32_t v = atomicAdd(state + (size_t)j * 256 + d, 0u);
+            if ((v & ~kOsMask) == 0u) {
+                if (++spins > kOsMaxSpin) {
+                    atomicOr(status, SPH3_STATUS_SORT);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            excl += v & kOsMask;
+            if ((v & ~kOsMask) == kOsIncl) break;
+            --j;
+        }
+        atomicExch(st + d, kOsIncl | (excl + cnt));
+        return dbase + excl;
+    };
+    rs_scatter_tile(key_in, val_in, key_out, val_out, n, 8 * pass, tile, offsets);
+}
+
 void launch_radix_sort(State &S, cudaStream_t st) {
     if (S.n <= 1) return;
     const int nb = (int)((S.n + kRsTile - 1) / kRsTile);
     const int passes = (S.key_bits + 7) / 8;
     uint64_t *kin = S.key, *kout = S.key_alt;
     uint32_t *vin = S.perm, *vout = S.perm_alt;
+    // scratch: all passes' histograms, the tile counters, the look-back words
+    uint32_t *hist_all = S.sort_hist;
+    int *tile_ctr = reinterpret_cast<int *>(S.sort_hist + kMaxPasses * 256);
+    uint32_t *state = S.sort_hist + kMaxPasses * 256 + 64;
+    cudaMemsetAsync(S.sort_hist, 0, sizeof(uint32_t) * ((size_t)kMaxPasses * 256 + 64 + (size_t)passes * nb * 256), st);
+    k_rs_hist_all<<<(int)std::min<int64_t>(nb, (int64_t)S.num_sms * 4), kHaThreads, 0, st>>>(kin, S.n, passes,
+                                                                                          hist_all);
     for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
-        k_rs_hist<<<nb, kRsThreads, 0, st>>>(kin, S.n, shift, S.sort_hist, nb);
-        k_rs_offsets<<<1, kRsOffsetThreads, 0, st>>>(S.sort_hist, nb);
-        k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kin, vin, kout, vout, S.n, shift, S.sort_hist, nb);
+        k_rs_onesweep<<<nb, kRsThreads, 0, st>>>(kin, vin, kout, vout, S.n, p, hist_all, state + (size_t)p * nb * 256,
+                                                 tile_ctr, S.status);
         uint64_t *tk = kin;
         kin = kout;
         kout = tk;

@@ -9,10 +9,13 @@
 // one boundary: a warp per node finds the 8 starts once and keeps them).
 // Single-child chains never appear, so nodes < 2 * particles.  Children of a
 // node are stored contiguously and each depth is compacted with an exclusive
-// scan, so the layout, and every sum over it, is deterministic.
+// scan, so the layout, and every sum over it, is deterministic.  One launch
+// per depth does the octant search, the scan (decoupled look-back between
+// tiles taken in order) and the child writes.
 // Compared with the reference's pointer octree (bh_tree_iteration_v2.h:149-450:
 // one block, atomicCAS locks, a DFS sort that spins on its parent) there are
-// no locks and no waits.
+// no locks; the one wait, a tile reading its predecessors' published counts,
+// waits only on running blocks and is bounded.
 #include <algorithm>
 #include <cfloat>
 
@@ -32,7 +35,9 @@ __global__ void k_tree_roots(Tree T, Cloud *clouds, int ncloud, const uint64_t *
     if (c == 0) {
         T.depth_begin[0] = 0;
         T.depth_begin[1] = ncloud;
+        T.lvl[kLvlEpoch] += 1;  // a new tag for this build's look-back words
     }
+    if (c < kLvlEpoch) T.lvl[c] = 0;  // the per-depth tile counters
     if (c >= ncloud) return;
     Cloud &cl = clouds[c];
     int first = (int)cl.begin, count = (int)(cl.end - cl.begin);
@@ -44,181 +49,206 @@ __global__ void k_tree_roots(Tree T, Cloud *clouds, int ncloud, const uint64_t *
 }
 
 // Children of each node of depth d: one warp per node finds where each
-// 3-bit digit of the next level starts inside the node's sorted key run and
-// stores the 8 starts (-1 for an empty octant) in T.bounds; nchild_tmp gets
-// the number of non-empty octants (0 for a leaf).  Digits are non-decreasing
-// inside a run, so the start of digit g is the first index whose digit is
-// >= g.  Runs of up to 128 keys are read whole (4 coalesced loads per lane)
+// 3-bit digit of the next level starts inside the node's sorted key run (8
+// starts, -1 for an empty octant) and the number of non-empty octants (0 for
+// a leaf).  Digits are non-decreasing inside a run, so the start of digit g
+// is the first index whose digit is >= g.  Runs of up to 128 keys are read whole (4 coalesced loads per lane)
 // and each start is the run start plus a ballot count; longer runs are
 // searched 5-ary, 4 lanes per digit probing 4 points per round (about
 // log5(count) dependent rounds instead of log2).
 constexpr int kTreeScanMax = 128;  // runs up to this size are read whole
 
-__global__ void k_tree_count(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
-    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
+// The octant starts of node i (warp-collective): lane g < 8 gets the first
+// index of the node's run whose next 3-bit digit is g (-1 for an empty
+// octant); returns the number of non-empty octants, 0 for a node that stays
+// a leaf (at most leaf_size particles, or at the deepest level).
+__device__ __forceinline__ int node_octants(const Tree &T, const uint64_t *key, int i, int leaf_size, int max_level,
+                                            int &start) {
     const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarp = (gridDim.x * blockDim.x) >> 5;
-    for (int i = beg + warp; i < end; i += nwarp) {
-        const int2 r = T.range[i];
-        const int lvl = T.child[i].y >> 8;
-        if (!(r.y > leaf_size && lvl < max_level)) {
-            if (lane == 0) T.nchild_tmp[i - beg] = 0;
-            continue;
+    const int2 r = T.range[i];
+    const int lvl = T.child[i].y >> 8;
+    start = -1;
+    if (!(r.y > leaf_size && lvl < max_level)) return 0;
+    const int shift = 3 * (max_level - lvl - 1);
+    const int s = r.x, e = r.x + r.y;
+    int first;  // lanes 0..7: first index of the run with digit >= lane
+    if (r.y <= kTreeScanMax) {
+        int dg[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = s + 32 * q + lane;
+            dg[q] = k < e ? (int)((key[k] >> shift) & 7u) : 8;
         }
-        const int shift = 3 * (max_level - lvl - 1);
-        const int s = r.x, e = r.x + r.y;
-        int first;  // lanes 0..7: first index of the run with digit >= lane
-        if (r.y <= kTreeScanMax) {
-            int dg[4];
+        first = s;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int k = s + 32 * q + lane;
-                dg[q] = k < e ? (int)((key[k] >> shift) & 7u) : 8;
-            }
-            first = s;
+        for (int g = 1; g < 8; ++g) {
+            int below = 0;
 #pragma unroll
-            for (int g = 1; g < 8; ++g) {
-                int below = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) below += __popc(__ballot_sync(kFull, dg[q] < g));
-                if (lane == g) first = s + below;
-            }
-        } else {
-            const int g = lane >> 2, sub = lane & 3;
-            int a = s, b = e;  // the answer for digit g lies in [a, b]
-            while (__any_sync(kFull, a < b)) {
-                const int p = a + (int)((long long)(b - a) * (sub + 1) / 5);  // a <= p < b when a < b
-                const bool pred = a < b && (int)((key[p] >> shift) & 7u) < g;
-                const int t = __popc((__ballot_sync(kFull, pred) >> (4 * g)) & 0xFu);
-                const int pl = __shfl_sync(kFull, p, 4 * g + (t > 0 ? t - 1 : 0));
-                const int pr = __shfl_sync(kFull, p, 4 * g + (t < 4 ? t : 3));
-                if (a < b) {
-                    if (t > 0) a = pl + 1;
-                    if (t < 4) b = pr;
-                }
-            }
-            first = __shfl_sync(kFull, a, 4 * (lane & 7));
+            for (int q = 0; q < 4; ++q) below += __popc(__ballot_sync(kFull, dg[q] < g));
+            if (lane == g) first = s + below;
         }
-        const int nxt = __shfl_down_sync(kFull, first, 1);
-        const int stop = lane == 7 ? e : nxt;
-        const int v = lane < 8 && first < stop ? first : -1;
-        if (lane < 8) T.bounds[8 * (size_t)(i - beg) + lane] = v;
-        const int nch = __popc(__ballot_sync(kFull, v >= 0));
-        if (lane == 0) T.nchild_tmp[i - beg] = nch;
+    } else {
+        const int g = lane >> 2, sub = lane & 3;
+        int a = s, b = e;  // the answer for digit g lies in [a, b]
+        while (__any_sync(kFull, a < b)) {
+            const int p = a + (int)((long long)(b - a) * (sub + 1) / 5);  // a <= p < b when a < b
+            const bool pred = a < b && (int)((key[p] >> shift) & 7u) < g;
+            const int t = __popc((__ballot_sync(kFull, pred) >> (4 * g)) & 0xFu);
+            const int pl = __shfl_sync(kFull, p, 4 * g + (t > 0 ? t - 1 : 0));
+            const int pr = __shfl_sync(kFull, p, 4 * g + (t < 4 ? t : 3));
+            if (a < b) {
+                if (t > 0) a = pl + 1;
+                if (t < 4) b = pr;
+            }
+        }
+        first = __shfl_sync(kFull, a, 4 * (lane & 7));
+    }
+    const int nxt = __shfl_down_sync(kFull, first, 1);
+    const int stop = lane == 7 ? e : nxt;
+    start = lane < 8 && first < stop ? first : -1;
+    return __popc(__ballot_sync(kFull, start >= 0));
+}
+
+// Children of node i from its octant starts st[8] (-1: empty), written at
+// cf, cf + 1, ... (a thread per node; nch = 0 marks a leaf).
+__device__ __forceinline__ void emit_children(const Tree &T, const uint64_t *key, int i, int nch, const int *st,
+                                              int cf, int max_level) {
+    const int lvl = T.child[i].y >> 8;
+    if (nch == 0) {
+        T.child[i] = make_int2(-1, lvl << 8);
+        return;
+    }
+    const int2 r = T.range[i];
+    const int e = r.x + r.y;
+    // all 16 key loads before any store, so they are in flight together
+    int stops[8];
+    uint64_t kf[8], kl[8];
+#pragma unroll
+    for (int dg = 0; dg < 8; ++dg) {
+        int stop = e;
+#pragma unroll
+        for (int q = 7; q > dg; --q)
+            if (st[q] >= 0) stop = st[q];
+        stops[dg] = stop;
+        kf[dg] = st[dg] >= 0 ? __ldg(key + st[dg]) : 0;
+        kl[dg] = st[dg] >= 0 ? __ldg(key + stop - 1) : 0;
+    }
+    T.child[i] = make_int2(cf, nch | (lvl << 8));
+    int c = 0;
+#pragma unroll
+    for (int dg = 0; dg < 8; ++dg) {
+        if (st[dg] < 0) continue;
+        const int stop = stops[dg];
+        const int cl = common_level(kf[dg], kl[dg], max_level);
+        T.range[cf + c] = make_int2(st[dg], stop - st[dg]);
+        T.child[cf + c] = make_int2(-1, cl << 8);
+        T.parent[cf + c] = i;
+        ++c;
     }
 }
 
-// exclusive scan of the child counts of depth d; sets depth_begin[d + 2]
-__global__ void __launch_bounds__(1024) k_tree_scan(Tree T, int d, unsigned *status) {
-    // chunks of 16384 counts: 16 consecutive per thread (four 16-byte loads in
-    // flight), so a depth of ~10^5 nodes takes a handful of rounds
-    constexpr int kPer = 16, kChunk = 1024 * kPer;
-    __shared__ int warp_tot[32];
-    __shared__ int carry_s;
+// Decoupled look-back over the tiles of one depth (single thread): publishes
+// the tile's child count, adds up the predecessors' counts until one that
+// already knows its inclusive prefix, publishes the tile's own inclusive
+// prefix and returns the exclusive one.  Words are tagged with (build, depth),
+// so words of earlier passes read as "not yet published".  Tiles are taken in
+// order from an atomic counter by running blocks, so every predecessor is
+// running or done and each wait ends; the waits are bounded all the same and
+// raise SPH3_STATUS_TREE_CAPACITY if one ever ran out.
+constexpr unsigned kLbAgg = 1u, kLbIncl = 2u;
+constexpr int kLbMaxSpin = 1 << 22;
+
+__device__ __forceinline__ unsigned long long lb_word(unsigned tag, unsigned flag, int v) {
+    return ((unsigned long long)tag << 32) | ((unsigned long long)flag << 30) | (unsigned long long)(unsigned)v;
+}
+
+__device__ int tile_lookback(unsigned long long *state, int tile, int tot, unsigned tag, unsigned *status) {
+    if (tile == 0) {
+        atomicExch(state, lb_word(tag, kLbIncl, tot));
+        return 0;
+    }
+    atomicExch(state + tile, lb_word(tag, kLbAgg, tot));
+    int excl = 0, j = tile - 1, spins = 0;
+    while (j >= 0) {
+        const unsigned long long w = atomicAdd(state + j, 0ull);
+        const unsigned flag = (unsigned)(w >> 30) & 3u;
+        if ((unsigned)(w >> 32) != tag || flag == 0u) {
+            if (++spins > kLbMaxSpin) {
+                atomicOr(status, SPH3_STATUS_TREE_CAPACITY);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        excl += (int)(w & 0x3fffffffull);
+        if (flag == kLbIncl) break;
+        --j;
+    }
+    atomicExch(state + tile, lb_word(tag, kLbIncl, excl + tot));
+    return excl;
+}
+
+// One depth of the top-down build in one launch: blocks take tiles of
+// kTreeTile consecutive nodes of depth d in order; a warp per node finds its
+// octant starts (node_octants), the tile's child counts are scanned in the
+// block and offset by the look-back prefix over earlier tiles, and a thread
+// per node writes the children.  The children of the depth come out compacted
+// in node order -- the layout of a global exclusive scan -- so the tree is
+// deterministic.  The last tile sets depth_begin[d + 2].
+constexpr int kTreeTile = 64;
+
+__global__ void __launch_bounds__(256) k_tree_level(Tree T, const uint64_t *key, int d, int leaf_size, int max_level,
+                                                    unsigned *status) {
+    __shared__ int s_tile, s_base;
+    __shared__ int s_nch[kTreeTile], s_off[kTreeTile];
+    __shared__ int s_st[kTreeTile * 8];
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
     const int m = end - beg;
+    if (m <= 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) T.depth_begin[d + 2] = end;
+        return;
+    }
+    const int ntiles = (m + kTreeTile - 1) / kTreeTile;
+    const unsigned tag = (unsigned)T.lvl[kLvlEpoch] * 32u + (unsigned)d;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int carry = 0;
-    for (int base = 0; base < m; base += kChunk) {
-        const int idx = base + threadIdx.x * kPer;
-        const bool whole = idx + kPer <= m;
-        int v[kPer];
-        if (whole) {
-            const int4 *src = reinterpret_cast<const int4 *>(T.nchild_tmp + idx);
-#pragma unroll
-            for (int q = 0; q < kPer / 4; ++q) {
-                const int4 t = src[q];
-                v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) v[k] = idx + k < m ? T.nchild_tmp[idx + k] : 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(T.lvl + d, 1);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        const int t0 = tile * kTreeTile;
+        const int tn = min(kTreeTile, m - t0);
+        for (int q = w; q < tn; q += 8) {
+            int start;
+            const int nch = node_octants(T, key, beg + t0 + q, leaf_size, max_level, start);
+            if (lane < 8) s_st[q * 8 + lane] = start;
+            if (lane == 0) s_nch[q] = nch;
         }
-        int s = 0;
-#pragma unroll
-        for (int k = 0; k < kPer; ++k) s += v[k];
-        const int incl = warp_incl_scan(s);
-        if (lane == 31) warp_tot[w] = incl;
         __syncthreads();
         if (w == 0) {
-            const int t = warp_tot[lane];
-            warp_tot[lane] = warp_incl_scan(t) - t;
+            const int a = 2 * lane < tn ? s_nch[2 * lane] : 0;
+            const int b = 2 * lane + 1 < tn ? s_nch[2 * lane + 1] : 0;
+            const int incl = warp_incl_scan(a + b);
+            if (2 * lane < tn) s_off[2 * lane] = incl - a - b;
+            if (2 * lane + 1 < tn) s_off[2 * lane + 1] = incl - b;
+            const int tot = __shfl_sync(kFull, incl, 31);
+            if (lane == 0) {
+                int base = tile_lookback(T.lb, tile, tot, tag, status);
+                if (end + base + tot > T.cap) {  // cannot happen: nodes < 2n + clouds + 64
+                    atomicOr(status, SPH3_STATUS_TREE_CAPACITY);
+                    base = -1;
+                }
+                s_base = base;
+                if (tile == ntiles - 1) T.depth_begin[d + 2] = base >= 0 ? end + base + tot : end;
+            }
         }
         __syncthreads();
-        int run = carry + warp_tot[w] + incl - s;
-#pragma unroll
-        for (int k = 0; k < kPer; ++k) {
-            const int x = v[k];
-            v[k] = run;
-            run += x;
+        if (threadIdx.x < tn) {
+            const int q = threadIdx.x;
+            const int nch = s_base >= 0 ? s_nch[q] : 0;
+            emit_children(T, key, beg + t0 + q, nch, s_st + 8 * q, end + s_base + s_off[q], max_level);
         }
-        if (whole) {
-            int4 *dst = reinterpret_cast<int4 *>(T.scan_tmp + idx);
-#pragma unroll
-            for (int q = 0; q < kPer / 4; ++q) dst[q] = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-        } else {
-#pragma unroll
-            for (int k = 0; k < kPer; ++k)
-                if (idx + k < m) T.scan_tmp[idx + k] = v[k];
-        }
-        if (threadIdx.x == 1023) carry_s = run;
         __syncthreads();
-        carry = carry_s;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        int total = carry;
-        int next = end + total;
-        if (next > T.cap) {
-            atomicOr(status, SPH3_STATUS_TREE_CAPACITY);
-            next = end;  // emit nothing: the affected nodes stay leaves
-        }
-        T.depth_begin[d + 2] = next;
-    }
-}
-
-__global__ void k_tree_emit(Tree T, const uint64_t *key, int d, int leaf_size, int max_level) {
-    const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
-    const bool room = T.depth_begin[d + 2] > end || end == beg;
-    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        const int nch = T.nchild_tmp[i - beg];
-        int lvl = T.child[i].y >> 8;
-        if (nch == 0 || !room) {
-            T.child[i] = make_int2(-1, lvl << 8);
-            continue;
-        }
-        const int cf = end + T.scan_tmp[i - beg];
-        const int2 r = T.range[i];
-        const int e = r.x + r.y;
-        const int4 *bq = reinterpret_cast<const int4 *>(T.bounds + 8 * (size_t)(i - beg));
-        const int4 b0 = bq[0], b1 = bq[1];
-        const int st[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-        // all 16 key loads before any store, so they are in flight together
-        int stops[8];
-        uint64_t kf[8], kl[8];
-#pragma unroll
-        for (int dg = 0; dg < 8; ++dg) {
-            int stop = e;
-#pragma unroll
-            for (int q = 7; q > dg; --q)
-                if (st[q] >= 0) stop = st[q];
-            stops[dg] = stop;
-            kf[dg] = st[dg] >= 0 ? __ldg(key + st[dg]) : 0;
-            kl[dg] = st[dg] >= 0 ? __ldg(key + stop - 1) : 0;
-        }
-        T.child[i] = make_int2(cf, nch | (lvl << 8));
-        int c = 0;
-#pragma unroll
-        for (int dg = 0; dg < 8; ++dg) {
-            if (st[dg] < 0) continue;
-            const int stop = stops[dg];
-            const int cl = common_level(kf[dg], kl[dg], max_level);
-            T.range[cf + c] = make_int2(st[dg], stop - st[dg]);
-            T.child[cf + c] = make_int2(-1, cl << 8);
-            T.parent[cf + c] = i;
-            ++c;
-        }
     }
 }
 
@@ -618,11 +648,8 @@ void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
     const int maxd = S.max_level + 1;  // depths 0..max_level
     k_tree_roots<<<(S.ncloud + 127) / 128, 128, 0, st>>>(T, S.clouds, S.ncloud, S.key, S.max_level);
     const int blocks = S.num_sms * 4;
-    for (int d = 0; d < maxd; ++d) {
-        k_tree_count<<<blocks, 256, 0, st>>>(T, S.key, d, P.leaf_size, S.max_level);
-        k_tree_scan<<<1, 1024, 0, st>>>(T, d, S.status);
-        k_tree_emit<<<blocks, 256, 0, st>>>(T, S.key, d, P.leaf_size, S.max_level);
-    }
+    for (int d = 0; d < maxd; ++d)
+        k_tree_level<<<blocks, 256, 0, st>>>(T, S.key, d, P.leaf_size, S.max_level, S.status);
     MomArgs a;
     a.pos = S.pos; a.m = S.m; a.h = S.h; a.eps = S.eps; a.n = S.n;
     a.clouds = S.clouds; a.key = S.key; a.max_level = S.max_level;
