@@ -204,11 +204,6 @@ struct HArgs {
 
 constexpr int kHK = 16;  // thresholds per pass in the reference-step mode
 constexpr double kNewtonDelta = 0.08;
-// The Newton search's first pass also counts at 2h * kFirstShrink (inside
-// the same reach): a count just above the window -- the common case where
-// the density grows -- is often inside it at the smaller radius, which then
-// ends the search without a second walk (0.97^3 = 0.91: 70-75 -> 64-68).
-constexpr double kFirstShrink = 0.97;
 
 template <typename R, int MODE>
 __device__ __forceinline__ void h_search_body(const HArgs &A) {
@@ -268,7 +263,7 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                 // the first pass counts at 2h only (a smaller reach: most groups
                 // are already in the window with the previous step's h); later
                 // passes also count at 2h (1 + delta) for the measured slope
-                thr[1] = pass == 0 ? 2.0 * h * kFirstShrink : 2.0 * h * (1.0 + kNewtonDelta);
+                thr[1] = pass == 0 ? thr[0] : 2.0 * h * (1.0 + kNewtonDelta);
             }
             float reach = 0.f;
             if (!conv) {
@@ -388,11 +383,6 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                 ncount = n0;
                 if (n0 <= up && n0 >= low) {
                     conv = true;
-                } else if (pass == 0 && n1 <= up && n1 >= low) {
-                    // the first pass's second radius is inside the window
-                    h = h * kFirstShrink;
-                    ncount = n1;
-                    conv = true;
                 } else if (pass >= A.max_iter || (n0 < low && (int64_t)n0 >= ncl)) {
                     // out of iterations, or the whole system is inside 2h already
                     failed = true;
@@ -405,15 +395,6 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                         n_hb = n0;
                     } else if (n0 < low) {
                         lb = fmax(lb, h);
-                    }
-                    if (pass == 0) {  // the second radius of the first pass brackets too
-                        const double hs = h * kFirstShrink;
-                        if (n1 > up && hs < hb) {
-                            hb = hs;
-                            n_hb = n1;
-                        } else if (n1 < low) {
-                            lb = fmax(lb, hs);
-                        }
                     }
                 }
                 if (!conv && lb > 0.0 && hb < DBL_MAX && hb - lb <= 1e-6 * hb) {
@@ -429,9 +410,7 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                         hn = 2.0 * h;
                     } else {
                         // slope of ln N over ln h: measured, or 3 (uniform density) on the first pass
-                        double sl = 3.0;
-                        if (pass > 0 && n1 > n0) sl = log((double)n1 / (double)n0) / log1p(kNewtonDelta);
-                        else if (pass == 0 && n0 > n1 && n1 > 0) sl = log((double)n0 / (double)n1) / -log(kFirstShrink);
+                        double sl = pass > 0 && n1 > n0 ? log((double)n1 / (double)n0) / log1p(kNewtonDelta) : 3.0;
                         sl = fmin(fmax(sl, 1.0), 6.0);
                         hn = h * exp((log((double)A.n_ngb) - log((double)n0)) / sl);
                     }
