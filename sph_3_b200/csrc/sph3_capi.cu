@@ -16,6 +16,9 @@ void launch_balsara(State &S, cudaStream_t st);
 }
 
 // ------------------------------------------------------------ context
+// row chunks of the host-buffer step's first inputs and last outputs
+constexpr int kIoChunks = 8;
+
 struct sph3_ctx {
     sph3_config cfg{};
     Params P{};
@@ -60,6 +63,9 @@ struct sph3_ctx {
     int64_t io_in_cap = 0, io_out_cap = 0;  // doubles
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t io_ev[10] = {};
+    // row chunks of the position/velocity/acceleration inputs and of the
+    // end-of-step outputs, so that copies and kernels overlap chunk by chunk
+    cudaEvent_t io_chunk_ev[2][kIoChunks] = {};
 };
 
 namespace {
@@ -360,6 +366,16 @@ __global__ void k_scatter_in(const double *src, double *dst, const int64_t *orig
     }
 }
 
+// rows [b, e) of a row-major (n, ncomp) caller-order array -> component-major
+// sorted field (sorted index inv[r])
+__global__ void k_scatter_rows(const double *src, double *dst, const int64_t *inv, int64_t n, int ncomp, int64_t b,
+                               int64_t e) {
+    for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = inv[r];
+        for (int c = 0; c < ncomp; ++c) dst[c * n + k] = src[r * ncomp + c];
+    }
+}
+
 // rows [b, e) of a component-major sorted field -> row-major caller order
 __global__ void k_gather_out(const double *src, double *dst, const int64_t *inv, int64_t n, int ncomp,
                              int64_t b, int64_t e) {
@@ -528,9 +544,12 @@ void record(sph3_ctx *c, int k, cudaStream_t st) {
 // Points inside one step where the host-buffer step moves its inputs in and
 // its outputs out, each called on the compute stream: after the gather that
 // follows the sort (new order in place, packs not yet built), after the h
-// search, before the kick that updates u, and at the end.
+// search, before the kick that updates u, and at the end.  second_kick, if
+// set, may run the serial order's closing kick itself (returning true), e.g.
+// chunk by chunk with each chunk's outputs handed to a copy.
 struct StepHooks {
     std::function<void(cudaStream_t)> after_gather, after_h, before_kick, after_u, at_end;
+    std::function<bool(cudaStream_t)> second_kick;
 };
 
 // One timestep, enqueued on st.  Switches the carried block half way (the
@@ -586,7 +605,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
         record(c, 8, st);
         if (P.gravity) launch_gravity(S, P, st, phi);
         record(c, 9, st);
-        launch_kick_update(S, P, dt, false, true, st);
+        if (!(hk && hk->second_kick && hk->second_kick(st))) launch_kick_update(S, P, dt, false, true, st);
     } else {
         if (P.gravity) launch_gravity(S, P, st, phi);
         record(c, 7, st);
@@ -613,6 +632,8 @@ int ensure_io(sph3_ctx *c, int64_t in_tot, int64_t out_tot) {
         CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
         for (auto &e : c->io_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto &row : c->io_chunk_ev)
+            for (auto &e : row) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     if (in_tot > c->io_in_cap) {
         if (c->io_in) cudaFree(c->io_in);
@@ -810,6 +831,9 @@ int sph3_ctx_destroy(sph3_ctx *c) {
     if (c->d2h) cudaStreamSynchronize(c->d2h);
     for (auto &e : c->io_ev)
         if (e) cudaEventDestroy(e);
+    for (auto &row : c->io_chunk_ev)
+        for (auto &e : row)
+            if (e) cudaEventDestroy(e);
     if (c->io_in) cudaFree(c->io_in);
     if (c->io_out) cudaFree(c->io_out);
     if (c->h2d) cudaStreamDestroy(c->h2d);
@@ -1219,10 +1243,28 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
     if (rc) return rc;
     if ((rc = sync_packs(c, st, true))) return rc;
     if (!c->P.gravity) CK(cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st));
-    // inputs: host -> staging on the copy stream, ordered by when the step needs them
+    // Inputs: host -> staging on the copy stream, ordered by when the step
+    // needs them.  The first group (positions, velocities, accelerations:
+    // everything the opening kick reads) goes in row chunks, each scattered
+    // into the state as soon as it has landed, so the scatter kernels overlap
+    // the rest of the copy.
+    const int nchunk = n >= (int64_t)kIoChunks * 8192 ? kIoChunks : 1;
+    auto chunk_rows = [&](int ch, int64_t &b, int64_t &e) {
+        b = n * ch / nchunk;
+        e = n * (ch + 1) / nchunk;
+    };
     CK(cudaEventRecord(c->io_ev[9], st));
     CK(cudaStreamWaitEvent(c->h2d, c->io_ev[9], 0));
-    for (int stage = 0; stage < 4; ++stage) {
+    for (int ch = 0; ch < nchunk; ++ch) {
+        int64_t b, e;
+        chunk_rows(ch, b, e);
+        for (int k = 0; k < nin; ++k)
+            if (io_stage_in(in_fields[k]) == 0)
+                CK(cudaMemcpyAsync(c->io_in + in_off[k] + b * in_nc[k], in[k] + b * in_nc[k],
+                                   sizeof(double) * in_nc[k] * (e - b), cudaMemcpyHostToDevice, c->h2d));
+        CK(cudaEventRecord(c->io_chunk_ev[0][ch], c->h2d));
+    }
+    for (int stage = 1; stage < 4; ++stage) {
         for (int k = 0; k < nin; ++k)
             if (io_stage_in(in_fields[k]) == stage)
                 CK(cudaMemcpyAsync(c->io_in + in_off[k], in[k], sizeof(double) * in_nc[k] * n,
@@ -1258,7 +1300,35 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
         }
         cudaEventRecord(c->io_ev[4 + stage], s);
     };
-    scatter(0, st);
+    // the first group by rows, through the inverse of the current order
+    k_invert<<<blocks_for(c, n), 256, 0, st>>>(S.orig, c->inv, n);
+    for (int ch = 0; ch < nchunk; ++ch) {
+        int64_t b, e;
+        chunk_rows(ch, b, e);
+        CK(cudaStreamWaitEvent(st, c->io_chunk_ev[0][ch], 0));
+        for (int k = 0; k < nin; ++k) {
+            if (io_stage_in(in_fields[k]) != 0) continue;
+            int nc = 1;
+            double *dst = field_ptr(c, in_fields[k], &nc);
+            k_scatter_rows<<<blocks_for(c, e - b), 256, 0, st>>>(c->io_in + in_off[k], dst, c->inv, n, nc, b, e);
+        }
+    }
+    // The closing outputs (velocities, accelerations and whatever else is
+    // final only at the end) by rows as well: in the serial order the closing
+    // kick runs chunk by chunk in caller order, each chunk gathered into the
+    // staging and copied out while the next is kicked.
+    bool tail_chunked = false;
+    for (int k = 0; k < nout; ++k) tail_chunked |= io_stage_out(out_fields[k]) == 3;
+    tail_chunked &= c->P.step_order == SPH3_ORDER_SERIAL;
+    auto gather_rows = [&](int64_t b, int64_t e, cudaStream_t s) {
+        for (int k = 0; k < nout; ++k) {
+            if (io_stage_out(out_fields[k]) != 3) continue;
+            int nc = 1;
+            const double *src = field_ptr(c, out_fields[k], &nc);
+            k_gather_out<<<blocks_for(c, e - b), 256, 0, s>>>(src, c->io_out + out_off[k] + b * nc, c->inv, n, nc,
+                                                              b, e);
+        }
+    };
     for (int step = 0; step < nsteps; ++step) {
         const bool first = step == 0, last = step == nsteps - 1;
         StepHooks hk;
@@ -1280,13 +1350,37 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
             if (last) gather(2, s);
         };
         hk.at_end = [&](cudaStream_t s) {
-            if (last) gather(3, s);
+            if (last && !tail_chunked) gather(3, s);
         };
+        if (last && tail_chunked)
+            hk.second_kick = [&](cudaStream_t s) {
+                for (int ch = 0; ch < nchunk; ++ch) {
+                    int64_t b, e;
+                    chunk_rows(ch, b, e);
+                    launch_kick_rows(S, dt, c->inv, b, e, s);
+                    gather_rows(b, e, s);
+                    cudaEventRecord(c->io_chunk_ev[1][ch], s);
+                }
+                return true;
+            };
         enqueue_step(c, dt, st, &hk);
         if ((rc = check_launch())) return rc;
     }
-    // staging -> host on the other copy stream, each group as soon as it is final
+    // staging -> host on the other copy stream, each group as soon as it is
+    // final (the closing group chunk by chunk when the kick ran by rows)
     for (int stage = 0; stage < 4; ++stage) {
+        if (stage == 3 && tail_chunked) {
+            for (int ch = 0; ch < nchunk; ++ch) {
+                int64_t b, e;
+                chunk_rows(ch, b, e);
+                CK(cudaStreamWaitEvent(c->d2h, c->io_chunk_ev[1][ch], 0));
+                for (int k = 0; k < nout; ++k)
+                    if (io_stage_out(out_fields[k]) == 3)
+                        CK(cudaMemcpyAsync(out[k] + b * out_nc[k], c->io_out + out_off[k] + b * out_nc[k],
+                                           sizeof(double) * out_nc[k] * (e - b), cudaMemcpyDeviceToHost, c->d2h));
+            }
+            continue;
+        }
         CK(cudaStreamWaitEvent(c->d2h, c->io_ev[4 + stage], 0));
         for (int k = 0; k < nout; ++k)
             if (io_stage_out(out_fields[k]) == stage)

@@ -43,6 +43,21 @@ void launch_kick_drift(State &S, const Params &P, double dt, cudaStream_t st) {
     k_kick_drift<<<grid_for(S, S.n), 256, 0, st>>>(S.n, dt, S.pos, S.vel, S.acc, P.box[0], P.box[1], P.box[2]);
 }
 
+// the second kick (v += a dt / 2, a = a_g + a_sph) of sorted particle i
+__device__ __forceinline__ void second_kick_one(int64_t n, int64_t i, double dt, double *acc, const double *acc_g,
+                                                const double *acc_sph, double *vel, float4 *pk_vel) {
+    float v3[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double a = acc_g[d * n + i] + acc_sph[d * n + i];
+        acc[d * n + i] = a;
+        const double v = __dadd_rn(vel[d * n + i], __dmul_rn(__dmul_rn(a, dt), 0.5));
+        vel[d * n + i] = v;
+        v3[d] = (float)v;
+    }
+    pk_vel[i] = make_float4(v3[0], v3[1], v3[2], 0.f);
+}
+
 __global__ void k_kick_update(int64_t n, double dt, int update_u, int second_kick, double *u,
                               double *u_prev, const double *dudt, double *dudt_prev, double *acc,
                               const double *acc_g, const double *acc_sph, double *vel, float4 *pk_vel) {
@@ -54,18 +69,7 @@ __global__ void k_kick_update(int64_t n, double dt, int update_u, int second_kic
             u_prev[i] = un;
             dudt_prev[i] = ut;
         }
-        if (second_kick) {
-            float v3[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double a = acc_g[d * n + i] + acc_sph[d * n + i];
-                acc[d * n + i] = a;
-                const double v = __dadd_rn(vel[d * n + i], __dmul_rn(__dmul_rn(a, dt), 0.5));
-                vel[d * n + i] = v;
-                v3[d] = (float)v;
-            }
-            pk_vel[i] = make_float4(v3[0], v3[1], v3[2], 0.f);
-        }
+        if (second_kick) second_kick_one(n, i, dt, acc, acc_g, acc_sph, vel, pk_vel);
     }
 }
 
@@ -75,6 +79,20 @@ void launch_kick_update(State &S, const Params &P, double dt, bool update_u, boo
     if (S.n == 0) return;
     k_kick_update<<<grid_for(S, S.n), 256, 0, st>>>(S.n, dt, update_u, second_kick, S.u, S.u_prev, S.dudt,
                                                    S.dudt_prev, S.acc, S.acc_g, S.acc_sph, S.vel, S.pk_vel);
+}
+
+// The second kick for the particles of caller rows [b, e) (the same
+// arithmetic as k_kick_update's), so that a step can finish its particles
+// chunk by chunk and hand each chunk to a copy as soon as it is done.
+__global__ void k_kick_rows(int64_t n, double dt, const int64_t *inv, int64_t b, int64_t e, double *acc,
+                            const double *acc_g, const double *acc_sph, double *vel, float4 *pk_vel) {
+    for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x)
+        second_kick_one(n, inv[r], dt, acc, acc_g, acc_sph, vel, pk_vel);
+}
+
+void launch_kick_rows(State &S, double dt, const int64_t *inv, int64_t b, int64_t e, cudaStream_t st) {
+    if (e <= b) return;
+    k_kick_rows<<<grid_for(S, e - b), 256, 0, st>>>(S.n, dt, inv, b, e, S.acc, S.acc_g, S.acc_sph, S.vel, S.pk_vel);
 }
 
 void launch_u_update(State &S, const Params &P, double dt, cudaStream_t st) {

@@ -310,6 +310,8 @@ void launch_kick_update(State &S, const Params &P, double dt, bool update_u, boo
                         cudaStream_t st);
 void launch_u_update(State &S, const Params &P, double dt, cudaStream_t st);
 void launch_first_u(State &S, const Params &P, double dt, cudaStream_t st);
+// the second kick of the particles of caller rows [b, e) (sorted index inv[r])
+void launch_kick_rows(State &S, double dt, const int64_t *inv, int64_t b, int64_t e, cudaStream_t st);
 void launch_sum_acc(State &S, cudaStream_t st);
 void launch_energy(State &S, const Params &P, cudaStream_t st);
 void launch_check_finite(State &S, cudaStream_t st);

@@ -3,7 +3,8 @@ u, ut_previous) in host memory, moved in and out in the same call with the
 transfers overlapping the step.  It must give, bit for bit, what the
 field-by-field path gives (sph3_set_field x6 -> sph3_step -> sph3_get_field
 x6) on a context with the same history, for both precisions and step
-orders, with page-locked and pageable host buffers."""
+orders, with page-locked and pageable host buffers, and at a size where the
+first inputs and the closing outputs move in row chunks (ragged last chunk)."""
 import numpy as np
 import pytest
 
@@ -22,14 +23,15 @@ def _ctx(cfg, ic):
     return ctx
 
 
-@pytest.mark.parametrize("prec,order,pinned", [("mixed", "serial", True), ("fp64", "serial", False),
-                                               ("mixed", "mpi4", True)])
-def test_step_io_matches_field_by_field(prec, order, pinned):
+@pytest.mark.parametrize("prec,order,pinned,n", [("mixed", "serial", True, 30000), ("fp64", "serial", False, 30000),
+                                                 ("mixed", "mpi4", True, 30000), ("mixed", "serial", True, 70001),
+                                                 ("fp64", "serial", True, 70001), ("mixed", "mpi4", False, 70001)])
+def test_step_io_matches_field_by_field(prec, order, pinned, n):
     import torch
     from sph_3_b200 import Config
     from sph_3_b200.ic import evrard
-    ic = evrard(30000, seed=13)
-    ic["vel"] = np.random.default_rng(13).normal(scale=0.05, size=(30000, 3))
+    ic = evrard(n, seed=13)
+    ic["vel"] = np.random.default_rng(13).normal(scale=0.05, size=(n, 3))
     cfg = Config(precision=prec, step_order=order, visc="balsara" if order == "mpi4" else "signal")
     a, b = _ctx(cfg, ic), _ctx(cfg, ic)
     state = {f: a.get_field(f) for f in FIELDS}
