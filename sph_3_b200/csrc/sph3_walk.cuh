@@ -24,16 +24,13 @@ namespace sph3 {
 struct WarpMem {
     int *stack;
     int *leafq;
-    int *lfirst;  // [32]
-    int *lpre;    // [32]
     void *tile;
 };
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 __host__ __device__ inline size_t warp_mem_bytes(int stack_cap, size_t tile_bytes) {
-    return align16(sizeof(int) * stack_cap) + align16(sizeof(int) * kLeafQ) +
-           align16(sizeof(int) * 64) + align16(tile_bytes);
+    return align16(sizeof(int) * stack_cap) + align16(sizeof(int) * kLeafQ) + align16(tile_bytes);
 }
 
 __device__ inline WarpMem carve_warp_mem(unsigned char *base, int stack_cap, size_t tile_bytes) {
@@ -44,9 +41,6 @@ __device__ inline WarpMem carve_warp_mem(unsigned char *base, int stack_cap, siz
     p += align16(sizeof(int) * stack_cap);
     m.leafq = reinterpret_cast<int *>(p);
     p += align16(sizeof(int) * kLeafQ);
-    m.lfirst = reinterpret_cast<int *>(p);
-    m.lpre = m.lfirst + 32;
-    p += align16(sizeof(int) * 64);
     m.tile = p;
     return m;
 }
@@ -142,14 +136,30 @@ struct alignas(4 * sizeof(R)) V4 {
     R x, y, z, w;
 };
 
+// Source particle of slot c0 + lane of a flush batch whose leaves are held
+// one per lane (first particle fst, exclusive prefix pre of the counts).
+// Every queued leaf holds at least one particle (the walks never take an
+// empty node), so the prefixes strictly increase: the leaf holding slot c0 is
+// the last lane starting at or before it, and each leaf starting inside the
+// chunk moves the later slots on by one leaf -- a ballot and an OR-reduction
+// instead of a dependent binary search through shared memory per slot.
+__device__ __forceinline__ int leaf_source(int c0, int pre, int fst, bool is_leaf) {
+    const int lane = lane_id();
+    const unsigned at_or_before = __ballot_sync(kFull, is_leaf && pre <= c0);
+    const int l0 = 31 - __clz((int)at_or_before);
+    const unsigned starts =
+        __reduce_or_sync(kFull, (is_leaf && pre > c0 && pre - c0 < 32) ? 1u << (pre - c0) : 0u);
+    const int leaf = l0 + __popc(starts & (0xffffffffu >> (31 - lane)));
+    return __shfl_sync(kFull, fst, leaf) + (c0 + lane - __shfl_sync(kFull, pre, leaf));
+}
+
 // Streams every particle of the queued leaves through a double-buffered
 // 32-entry tile (tile[0..63]): the loads of the next 32 candidates are in
 // flight while the lanes run the current ones.  load(j) returns the tile
 // entry of sorted particle j (global loads + conversion to the group frame);
 // interact(tile, ne) runs every lane's target against ne staged entries.
 template <class E, class Load, class Interact>
-__device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq, int nleaf,
-                                             int *lfirst, int *lpre, E *tile, Load &load,
+__device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq, int nleaf, E *tile, Load &load,
                                              Interact &interact) {
     const int lane = lane_id();
     for (int base = 0; base < nleaf; base += 32) {
@@ -161,21 +171,13 @@ __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq
         }
         const int incl = warp_incl_scan(cnt);
         const int tot = __shfl_sync(kFull, incl, 31);
-        __syncwarp();
-        lfirst[lane] = fst;
-        lpre[lane] = incl - cnt;
-        __syncwarp();
-        const int nl = min(32, nleaf - base);
+        const int pre = incl - cnt;
+        const bool is_leaf = base + lane < nleaf;
         auto fetch = [&](int c0, E &out) -> bool {
             const int t = c0 + lane;
+            const int j = leaf_source(c0, pre, fst, is_leaf);
             if (t >= tot) return false;
-            int lo = 0, hi = nl - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (lpre[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
-            out = load(lfirst[lo] + (t - lpre[lo]));
+            out = load(j);
             return true;
         };
         E cur;
@@ -199,8 +201,8 @@ __device__ __forceinline__ void flush_leaves(const int2 *range, const int *leafq
 // first ne entries of buffer buf.  Padded slots let the interaction run
 // whole pairs of entries without bounds checks.
 template <class E, class Load, class Store, class Interact>
-__device__ __forceinline__ void flush_leaves_st(const int2 *range, const int *leafq, int nleaf, int *lfirst,
-                                                int *lpre, Load &load, Store &store, Interact &interact) {
+__device__ __forceinline__ void flush_leaves_st(const int2 *range, const int *leafq, int nleaf, Load &load,
+                                                Store &store, Interact &interact) {
     const int lane = lane_id();
     for (int base = 0; base < nleaf; base += 32) {
         int cnt = 0, fst = 0;
@@ -211,21 +213,13 @@ __device__ __forceinline__ void flush_leaves_st(const int2 *range, const int *le
         }
         const int incl = warp_incl_scan(cnt);
         const int tot = __shfl_sync(kFull, incl, 31);
-        __syncwarp();
-        lfirst[lane] = fst;
-        lpre[lane] = incl - cnt;
-        __syncwarp();
-        const int nl = min(32, nleaf - base);
+        const int pre = incl - cnt;
+        const bool is_leaf = base + lane < nleaf;
         auto fetch = [&](int c0, E &out) -> bool {
             const int t = c0 + lane;
+            const int j = leaf_source(c0, pre, fst, is_leaf);
             if (t >= tot) return false;
-            int lo = 0, hi = nl - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (lpre[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
-            out = load(lfirst[lo] + (t - lpre[lo]));
+            out = load(j);
             return true;
         };
         E cur{};
@@ -248,9 +242,8 @@ __device__ __forceinline__ void flush_leaves_st(const int2 *range, const int *le
 // sees a full tile of 32.  The tile holds 64 entries: up to 31 left over
 // plus one freshly loaded chunk.
 template <class E, class Load, class Interact>
-__device__ __forceinline__ void flush_leaves_compact(const int2 *range, const int *leafq, int nleaf,
-                                                     int *lfirst, int *lpre, E *tile, Load &load,
-                                                     Interact &interact) {
+__device__ __forceinline__ void flush_leaves_compact(const int2 *range, const int *leafq, int nleaf, E *tile,
+                                                     Load &load, Interact &interact) {
     const int lane = lane_id();
     int fill = 0;
     for (int base = 0; base < nleaf; base += 32) {
@@ -262,22 +255,14 @@ __device__ __forceinline__ void flush_leaves_compact(const int2 *range, const in
         }
         const int incl = warp_incl_scan(cnt);
         const int tot = __shfl_sync(kFull, incl, 31);
-        __syncwarp();
-        lfirst[lane] = fst;
-        lpre[lane] = incl - cnt;
-        __syncwarp();
-        const int nl = min(32, nleaf - base);
+        const int pre = incl - cnt;
+        const bool is_leaf = base + lane < nleaf;
         auto fetch = [&](int c0, E &out) -> bool {
             const int t = c0 + lane;
+            const int j = leaf_source(c0, pre, fst, is_leaf);
             if (t >= tot) return false;
-            int lo = 0, hi = nl - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (lpre[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
             bool keep = true;
-            out = load(lfirst[lo] + (t - lpre[lo]), keep);
+            out = load(j, keep);
             return keep;
         };
         E cur;
@@ -320,9 +305,8 @@ struct SoaV {
 // set to pad[f], so the entries can be run in pairs, two consecutive entries
 // loading as one float2 per field: a ready packed FP32 operand.
 template <int NF, class Load, class Interact>
-__device__ __forceinline__ void flush_leaves_compact_soa(const int2 *range, const int *leafq, int nleaf, int *lfirst,
-                                                         int *lpre, float *tile, const SoaV<NF> &pad, Load &load,
-                                                         Interact &interact) {
+__device__ __forceinline__ void flush_leaves_compact_soa(const int2 *range, const int *leafq, int nleaf, float *tile,
+                                                         const SoaV<NF> &pad, Load &load, Interact &interact) {
     const int lane = lane_id();
     int fill = 0;
     for (int base = 0; base < nleaf; base += 32) {
@@ -334,22 +318,14 @@ __device__ __forceinline__ void flush_leaves_compact_soa(const int2 *range, cons
         }
         const int incl = warp_incl_scan(cnt);
         const int tot = __shfl_sync(kFull, incl, 31);
-        __syncwarp();
-        lfirst[lane] = fst;
-        lpre[lane] = incl - cnt;
-        __syncwarp();
-        const int nl = min(32, nleaf - base);
+        const int pre = incl - cnt;
+        const bool is_leaf = base + lane < nleaf;
         auto fetch = [&](int c0, SoaV<NF> &out) -> bool {
             const int t = c0 + lane;
+            const int j = leaf_source(c0, pre, fst, is_leaf);
             if (t >= tot) return false;
-            int lo = 0, hi = nl - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (lpre[mid] <= t) lo = mid;
-                else hi = mid - 1;
-            }
             bool keep = true;
-            out = load(lfirst[lo] + (t - lpre[lo]), keep);
+            out = load(j, keep);
             return keep;
         };
         SoaV<NF> cur;

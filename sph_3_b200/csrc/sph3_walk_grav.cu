@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
             }
         };
         auto flush_leaves_fn = [&](int nl) {
-            flush_leaves(A.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile.pt, load_part, part_interact);
+            flush_leaves(A.range, wm.leafq, nl, tile.pt, load_part, part_interact);
         };
         unsigned long long visits = 0;
         const int guard = grav_walk(A, wm, tile.nodeq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn, visits);
@@ -397,11 +397,13 @@ __device__ __forceinline__ void spline_near2(float2 r2, float2 r, float2 rinv, f
     }
 }
 
-// 24 resident warps per SM (at most 85 registers): the walk part is latency-bound
-constexpr int kGravMinWarpsPerSM = 24;
+// At most 72 registers: 28 resident warps per SM (registers are granted in
+// steps of 8 per thread, so 73 would already cost a block of four warps).
+// The walk part is latency-bound and wants the residency.
+constexpr int kGravMaxRegs = 72;
 
 template <bool QUAD, bool PHI>
-__global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWarps) k_gravity_f32(GArgs A) {
+__global__ void __maxnreg__(kGravMaxRegs) k_gravity_f32(GArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpMem wm = carve_warp_mem(smem, A.stack_cap, sizeof(GTileF));
     GTileF &tile = *reinterpret_cast<GTileF *>(wm.tile);
@@ -560,7 +562,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kGravMinWarpsPerSM / kWalkWar
             }
         };
         auto flush_leaves_fn = [&](int nl) {
-            flush_leaves_st<PartF>(A.range, wm.leafq, nl, wm.lfirst, wm.lpre, load_part, store_part,
+            flush_leaves_st<PartF>(A.range, wm.leafq, nl, load_part, store_part,
                                    part_interact);
         };
         unsigned long long visits = 0;

@@ -339,10 +339,10 @@ __device__ __forceinline__ void h_search_body(const HArgs &A) {
                 };
                 auto flush = [&](int nl) {
                     if constexpr (sizeof(R) == 4)
-                        flush_leaves_compact_soa<3>(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, xs,
+                        flush_leaves_compact_soa<3>(a.range, wm.leafq, nl, xs,
                                                     SoaV<3>{{1e18f, 1e18f, 1e18f}}, load_xyz, interact_xyz);
                     else
-                        flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                        flush_leaves_compact(a.range, wm.leafq, nl, tile, load, interact);
                 };
                 collect_leaves(a, wm, gi.root, gb, reach, false, s, flush);
             }
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_boot_h(Boot
                     }
                 };
                 auto flush = [&](int nl) {
-                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                    flush_leaves(a.range, wm.leafq, nl, tile, load, interact);
                 };
                 collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
             }
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_boot_h(Boot
                     }
                 };
                 auto flush = [&](int nl) {
-                    flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                    flush_leaves(a.range, wm.leafq, nl, tile, load, interact);
                 };
                 collect_leaves(a, wm, gi.root, gb, (float)Rg * 1.0001f, false, s, flush);
             }
@@ -878,11 +878,11 @@ __device__ __forceinline__ void density_body(const DArgs &A) {
             };
             auto flush = [&](int nl) {
                 if constexpr (sizeof(R) == 4 && !DC)
-                    flush_leaves_compact_soa<6>(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, sx,
+                    flush_leaves_compact_soa<6>(a.range, wm.leafq, nl, sx,
                                                 SoaV<6>{{1e18f, 1e18f, 1e18f, 0.f, 0.f, 0.f}}, load_soa,
                                                 interact_bal);
                 else
-                    flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                    flush_leaves_compact(a.range, wm.leafq, nl, tile, load, interact);
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
@@ -1124,7 +1124,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
                 }
             };
             auto flush = [&](int nl) {
-                flush_leaves_compact(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                flush_leaves_compact(a.range, wm.leafq, nl, tile, load, interact);
             };
             collect_leaves(a, wm, gi.root, gb, hmax_g, true, s, flush);
         }
@@ -1391,7 +1391,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_neighbours(
                 (void)ne;
             };
             auto flush = [&](int nl) {
-                flush_leaves(a.range, wm.leafq, nl, wm.lfirst, wm.lpre, tile, load, interact);
+                flush_leaves(a.range, wm.leafq, nl, tile, load, interact);
             };
             collect_leaves(a, wm, cl.root, gb, (float)th, true, s, flush);
         }
