@@ -87,7 +87,7 @@ struct Tree {
     float *quad1;       // {yz}
     // walk records (one contiguous record per node; child.y = -1 marks an empty node)
     float4 *gw;         // [cap][2] gravity: {com_c}, {r_open, r_soft, first child, nch | level << 8}
-    float4 *sw;         // [cap][3] SPH: {box_c}, {box_h}, {first child, nch | level << 8, 0, 0}
+    float4 *sw;         // [cap][3] SPH: {box_c}, {box_h}, {first child, nch | level << 8, count, 0}
     int cap;
     int *depth_begin;   // [max_depth + 2] node id where each depth starts
     int *meta;          // [128] depth_begin (first 96) and the scratch counters `total`

@@ -396,7 +396,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         T.gw[2 * i + 1] = make_float4((float)r_open, (float)r_soft, __int_as_float(ch.x), __int_as_float(chy));
         T.sw[3 * i] = T.box_c[i];
         T.sw[3 * i + 1] = T.box_h[i];
-        T.sw[3 * i + 2] = make_float4(__int_as_float(ch.x), __int_as_float(chy), 0.f, 0.f);
+        T.sw[3 * i + 2] = make_float4(__int_as_float(ch.x), __int_as_float(chy), __int_as_float(r.y), 0.f);
     }
 }
 

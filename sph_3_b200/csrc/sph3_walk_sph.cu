@@ -64,6 +64,11 @@ __device__ __forceinline__ double exact_dist(double dx, double dy, double dz) {
     return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
 }
 
+// The SPH walks take a node with at most kSphLeaf particles whole, as if it
+// were a leaf: below that size descending costs more walk steps than the
+// extra candidates it saves (the gravity walk keeps the tree's own leaves).
+constexpr int kSphLeaf = 32;
+
 // Walk the tree for one group, calling flush(nleaf) on full leaf queues.
 // A node is kept if the gap between its bbox and the group bbox is at most
 // reach = Rg + (node_h ? hmax_node : 0) (times a 4e-5 safety margin; the
@@ -106,7 +111,7 @@ __device__ void collect_leaves(const WalkArgs &a, const WarpMem &wm, int root, c
             const float g2 = box_gap2(gb, c, make_float3(bh.x, bh.y, bh.z));
             if (chy >= 0 && g2 <= reach * reach) {
                 const int k = chy & 255;
-                if (k == 0) {
+                if (k == 0 || __float_as_int(w2.z) <= kSphLeaf) {
                     take = true;
                 } else {
                     nch = k;
