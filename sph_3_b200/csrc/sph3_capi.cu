@@ -66,6 +66,10 @@ struct sph3_ctx {
     // row chunks of the position/velocity/acceleration inputs and of the
     // end-of-step outputs, so that copies and kernels overlap chunk by chunk
     cudaEvent_t io_chunk_ev[2][kIoChunks] = {};
+    // the host-buffer step captured as a graph per carried-block parity, with
+    // the call it was captured for (buffers, fields, dt, steps)
+    cudaGraphExec_t io_graph[2] = {nullptr, nullptr};
+    std::vector<uint64_t> io_key[2];
 };
 
 namespace {
@@ -230,6 +234,9 @@ void drop_graphs(sph3_ctx *c) {
     for (int k = 0; k < 2; ++k) {
         if (c->graph[k]) cudaGraphExecDestroy(c->graph[k]);
         c->graph[k] = nullptr;
+        if (c->io_graph[k]) cudaGraphExecDestroy(c->io_graph[k]);
+        c->io_graph[k] = nullptr;
+        c->io_key[k].clear();
     }
     c->warm_steps = 0;
 }
@@ -1243,151 +1250,215 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
     if (rc) return rc;
     if ((rc = sync_packs(c, st, true))) return rc;
     if (!c->P.gravity) CK(cudaMemsetAsync(S.acc_g, 0, sizeof(double) * 3 * c->cap_n, st));
-    // Inputs: host -> staging on the copy stream, ordered by when the step
-    // needs them.  The first group (positions, velocities, accelerations:
-    // everything the opening kick reads) goes in row chunks, each scattered
-    // into the state as soon as it has landed, so the scatter kernels overlap
-    // the rest of the copy.
-    const int nchunk = n >= (int64_t)kIoChunks * 8192 ? kIoChunks : 1;
-    auto chunk_rows = [&](int ch, int64_t &b, int64_t &e) {
-        b = n * ch / nchunk;
-        e = n * (ch + 1) / nchunk;
-    };
-    CK(cudaEventRecord(c->io_ev[9], st));
-    CK(cudaStreamWaitEvent(c->h2d, c->io_ev[9], 0));
-    for (int ch = 0; ch < nchunk; ++ch) {
-        int64_t b, e;
-        chunk_rows(ch, b, e);
-        for (int k = 0; k < nin; ++k)
-            if (io_stage_in(in_fields[k]) == 0)
-                CK(cudaMemcpyAsync(c->io_in + in_off[k] + b * in_nc[k], in[k] + b * in_nc[k],
-                                   sizeof(double) * in_nc[k] * (e - b), cudaMemcpyHostToDevice, c->h2d));
-        CK(cudaEventRecord(c->io_chunk_ev[0][ch], c->h2d));
-    }
-    for (int stage = 1; stage < 4; ++stage) {
-        for (int k = 0; k < nin; ++k)
-            if (io_stage_in(in_fields[k]) == stage)
-                CK(cudaMemcpyAsync(c->io_in + in_off[k], in[k], sizeof(double) * in_nc[k] * n,
-                                   cudaMemcpyHostToDevice, c->h2d));
-        CK(cudaEventRecord(c->io_ev[stage], c->h2d));
-    }
-    // staging -> state in the current order (field pointers looked up when the
-    // hook runs: the carried block switches inside the step)
-    auto scatter = [&](int stage, cudaStream_t s) {
-        cudaStreamWaitEvent(s, c->io_ev[stage], 0);
-        for (int k = 0; k < nin; ++k) {
-            if (io_stage_in(in_fields[k]) != stage) continue;
-            int nc = 1;
-            double *dst = field_ptr(c, in_fields[k], &nc);
-            k_scatter_in<<<blocks_for(c, n), 256, 0, s>>>(c->io_in + in_off[k], dst, S.orig, n, nc);
+    // everything below, up to the join of the copy streams, is one enqueue:
+    // run directly or captured once and replayed as a graph
+    auto enqueue_io = [&]() -> int {
+        // Inputs: host -> staging on the copy stream, ordered by when the step
+        // needs them.  The first group (positions, velocities, accelerations:
+        // everything the opening kick reads) goes in row chunks, each scattered
+        // into the state as soon as it has landed, so the scatter kernels overlap
+        // the rest of the copy.
+        const int nchunk = n >= (int64_t)kIoChunks * 8192 ? kIoChunks : 1;
+        auto chunk_rows = [&](int ch, int64_t &b, int64_t &e) {
+            b = n * ch / nchunk;
+            e = n * (ch + 1) / nchunk;
+        };
+        CK(cudaEventRecord(c->io_ev[9], st));
+        CK(cudaStreamWaitEvent(c->h2d, c->io_ev[9], 0));
+        for (int ch = 0; ch < nchunk; ++ch) {
+            int64_t b, e;
+            chunk_rows(ch, b, e);
+            for (int k = 0; k < nin; ++k)
+                if (io_stage_in(in_fields[k]) == 0)
+                    CK(cudaMemcpyAsync(c->io_in + in_off[k] + b * in_nc[k], in[k] + b * in_nc[k],
+                                       sizeof(double) * in_nc[k] * (e - b), cudaMemcpyHostToDevice, c->h2d));
+            CK(cudaEventRecord(c->io_chunk_ev[0][ch], c->h2d));
         }
-        // the reference's loop keeps u_previous = u between iterations
-        // (sph_serial.py:181-182): an input u alone sets both
-        if (stage == 3 && has_u && !has_uprev)
-            cudaMemcpyAsync(S.u_prev, S.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
-    };
-    // outputs: state -> staging in the caller's order as soon as each is final
-    auto gather = [&](int stage, cudaStream_t s) {
-        for (int k = 0; k < nout; ++k) {
-            if (io_stage_out(out_fields[k]) != stage) continue;
-            if (out_fields[k] == SPH3_FIELD_NNGB) {
-                k_gather_out_int<<<blocks_for(c, n), 256, 0, s>>>(S.nngb, c->io_out + out_off[k], c->inv, 0, n);
-            } else {
+        for (int stage = 1; stage < 4; ++stage) {
+            for (int k = 0; k < nin; ++k)
+                if (io_stage_in(in_fields[k]) == stage)
+                    CK(cudaMemcpyAsync(c->io_in + in_off[k], in[k], sizeof(double) * in_nc[k] * n,
+                                       cudaMemcpyHostToDevice, c->h2d));
+            CK(cudaEventRecord(c->io_ev[stage], c->h2d));
+        }
+        // staging -> state in the current order (field pointers looked up when the
+        // hook runs: the carried block switches inside the step)
+        auto scatter = [&](int stage, cudaStream_t s) {
+            cudaStreamWaitEvent(s, c->io_ev[stage], 0);
+            for (int k = 0; k < nin; ++k) {
+                if (io_stage_in(in_fields[k]) != stage) continue;
+                int nc = 1;
+                double *dst = field_ptr(c, in_fields[k], &nc);
+                k_scatter_in<<<blocks_for(c, n), 256, 0, s>>>(c->io_in + in_off[k], dst, S.orig, n, nc);
+            }
+            // the reference's loop keeps u_previous = u between iterations
+            // (sph_serial.py:181-182): an input u alone sets both
+            if (stage == 3 && has_u && !has_uprev)
+                cudaMemcpyAsync(S.u_prev, S.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+        };
+        // outputs: state -> staging in the caller's order as soon as each is final
+        auto gather = [&](int stage, cudaStream_t s) {
+            for (int k = 0; k < nout; ++k) {
+                if (io_stage_out(out_fields[k]) != stage) continue;
+                if (out_fields[k] == SPH3_FIELD_NNGB) {
+                    k_gather_out_int<<<blocks_for(c, n), 256, 0, s>>>(S.nngb, c->io_out + out_off[k], c->inv, 0, n);
+                } else {
+                    int nc = 1;
+                    const double *src = field_ptr(c, out_fields[k], &nc);
+                    k_gather_out<<<blocks_for(c, n), 256, 0, s>>>(src, c->io_out + out_off[k], c->inv, n, nc, 0, n);
+                }
+            }
+            cudaEventRecord(c->io_ev[4 + stage], s);
+        };
+        // the first group by rows, through the inverse of the current order
+        k_invert<<<blocks_for(c, n), 256, 0, st>>>(S.orig, c->inv, n);
+        for (int ch = 0; ch < nchunk; ++ch) {
+            int64_t b, e;
+            chunk_rows(ch, b, e);
+            CK(cudaStreamWaitEvent(st, c->io_chunk_ev[0][ch], 0));
+            for (int k = 0; k < nin; ++k) {
+                if (io_stage_in(in_fields[k]) != 0) continue;
+                int nc = 1;
+                double *dst = field_ptr(c, in_fields[k], &nc);
+                k_scatter_rows<<<blocks_for(c, e - b), 256, 0, st>>>(c->io_in + in_off[k], dst, c->inv, n, nc, b, e);
+            }
+        }
+        // The closing outputs (velocities, accelerations and whatever else is
+        // final only at the end) by rows as well: in the serial order the closing
+        // kick runs chunk by chunk in caller order, each chunk gathered into the
+        // staging and copied out while the next is kicked.
+        bool tail_chunked = false;
+        for (int k = 0; k < nout; ++k) tail_chunked |= io_stage_out(out_fields[k]) == 3;
+        tail_chunked &= c->P.step_order == SPH3_ORDER_SERIAL;
+        auto gather_rows = [&](int64_t b, int64_t e, cudaStream_t s) {
+            for (int k = 0; k < nout; ++k) {
+                if (io_stage_out(out_fields[k]) != 3) continue;
                 int nc = 1;
                 const double *src = field_ptr(c, out_fields[k], &nc);
-                k_gather_out<<<blocks_for(c, n), 256, 0, s>>>(src, c->io_out + out_off[k], c->inv, n, nc, 0, n);
-            }
-        }
-        cudaEventRecord(c->io_ev[4 + stage], s);
-    };
-    // the first group by rows, through the inverse of the current order
-    k_invert<<<blocks_for(c, n), 256, 0, st>>>(S.orig, c->inv, n);
-    for (int ch = 0; ch < nchunk; ++ch) {
-        int64_t b, e;
-        chunk_rows(ch, b, e);
-        CK(cudaStreamWaitEvent(st, c->io_chunk_ev[0][ch], 0));
-        for (int k = 0; k < nin; ++k) {
-            if (io_stage_in(in_fields[k]) != 0) continue;
-            int nc = 1;
-            double *dst = field_ptr(c, in_fields[k], &nc);
-            k_scatter_rows<<<blocks_for(c, e - b), 256, 0, st>>>(c->io_in + in_off[k], dst, c->inv, n, nc, b, e);
-        }
-    }
-    // The closing outputs (velocities, accelerations and whatever else is
-    // final only at the end) by rows as well: in the serial order the closing
-    // kick runs chunk by chunk in caller order, each chunk gathered into the
-    // staging and copied out while the next is kicked.
-    bool tail_chunked = false;
-    for (int k = 0; k < nout; ++k) tail_chunked |= io_stage_out(out_fields[k]) == 3;
-    tail_chunked &= c->P.step_order == SPH3_ORDER_SERIAL;
-    auto gather_rows = [&](int64_t b, int64_t e, cudaStream_t s) {
-        for (int k = 0; k < nout; ++k) {
-            if (io_stage_out(out_fields[k]) != 3) continue;
-            int nc = 1;
-            const double *src = field_ptr(c, out_fields[k], &nc);
-            k_gather_out<<<blocks_for(c, e - b), 256, 0, s>>>(src, c->io_out + out_off[k] + b * nc, c->inv, n, nc,
-                                                              b, e);
-        }
-    };
-    for (int step = 0; step < nsteps; ++step) {
-        const bool first = step == 0, last = step == nsteps - 1;
-        StepHooks hk;
-        hk.after_gather = [&](cudaStream_t s) {
-            if (first) scatter(1, s);
-            if (last) {
-                k_invert<<<blocks_for(c, n), 256, 0, s>>>(S.orig, c->inv, n);
-                gather(0, s);
+                k_gather_out<<<blocks_for(c, e - b), 256, 0, s>>>(src, c->io_out + out_off[k] + b * nc, c->inv, n, nc,
+                                                                  b, e);
             }
         };
-        hk.after_h = [&](cudaStream_t s) {
-            if (first) scatter(2, s);
-            if (last) gather(1, s);
-        };
-        hk.before_kick = [&](cudaStream_t s) {
-            if (first) scatter(3, s);
-        };
-        hk.after_u = [&](cudaStream_t s) {
-            if (last) gather(2, s);
-        };
-        hk.at_end = [&](cudaStream_t s) {
-            if (last && !tail_chunked) gather(3, s);
-        };
-        if (last && tail_chunked)
-            hk.second_kick = [&](cudaStream_t s) {
+        for (int step = 0; step < nsteps; ++step) {
+            const bool first = step == 0, last = step == nsteps - 1;
+            StepHooks hk;
+            hk.after_gather = [&](cudaStream_t s) {
+                if (first) scatter(1, s);
+                if (last) {
+                    k_invert<<<blocks_for(c, n), 256, 0, s>>>(S.orig, c->inv, n);
+                    gather(0, s);
+                }
+            };
+            hk.after_h = [&](cudaStream_t s) {
+                if (first) scatter(2, s);
+                if (last) gather(1, s);
+            };
+            hk.before_kick = [&](cudaStream_t s) {
+                if (first) scatter(3, s);
+            };
+            hk.after_u = [&](cudaStream_t s) {
+                if (last) gather(2, s);
+            };
+            hk.at_end = [&](cudaStream_t s) {
+                if (last && !tail_chunked) gather(3, s);
+            };
+            if (last && tail_chunked)
+                hk.second_kick = [&](cudaStream_t s) {
+                    for (int ch = 0; ch < nchunk; ++ch) {
+                        int64_t b, e;
+                        chunk_rows(ch, b, e);
+                        launch_kick_rows(S, dt, c->inv, b, e, s);
+                        gather_rows(b, e, s);
+                        cudaEventRecord(c->io_chunk_ev[1][ch], s);
+                    }
+                    return true;
+                };
+            enqueue_step(c, dt, st, &hk);
+            if ((rc = check_launch())) return rc;
+        }
+        // staging -> host on the other copy stream, each group as soon as it is
+        // final (the closing group chunk by chunk when the kick ran by rows)
+        for (int stage = 0; stage < 4; ++stage) {
+            if (stage == 3 && tail_chunked) {
                 for (int ch = 0; ch < nchunk; ++ch) {
                     int64_t b, e;
                     chunk_rows(ch, b, e);
-                    launch_kick_rows(S, dt, c->inv, b, e, s);
-                    gather_rows(b, e, s);
-                    cudaEventRecord(c->io_chunk_ev[1][ch], s);
+                    CK(cudaStreamWaitEvent(c->d2h, c->io_chunk_ev[1][ch], 0));
+                    for (int k = 0; k < nout; ++k)
+                        if (io_stage_out(out_fields[k]) == 3)
+                            CK(cudaMemcpyAsync(out[k] + b * out_nc[k], c->io_out + out_off[k] + b * out_nc[k],
+                                               sizeof(double) * out_nc[k] * (e - b), cudaMemcpyDeviceToHost, c->d2h));
                 }
-                return true;
-            };
-        enqueue_step(c, dt, st, &hk);
-        if ((rc = check_launch())) return rc;
-    }
-    // staging -> host on the other copy stream, each group as soon as it is
-    // final (the closing group chunk by chunk when the kick ran by rows)
-    for (int stage = 0; stage < 4; ++stage) {
-        if (stage == 3 && tail_chunked) {
-            for (int ch = 0; ch < nchunk; ++ch) {
-                int64_t b, e;
-                chunk_rows(ch, b, e);
-                CK(cudaStreamWaitEvent(c->d2h, c->io_chunk_ev[1][ch], 0));
-                for (int k = 0; k < nout; ++k)
-                    if (io_stage_out(out_fields[k]) == 3)
-                        CK(cudaMemcpyAsync(out[k] + b * out_nc[k], c->io_out + out_off[k] + b * out_nc[k],
-                                           sizeof(double) * out_nc[k] * (e - b), cudaMemcpyDeviceToHost, c->d2h));
+                continue;
             }
-            continue;
+            CK(cudaStreamWaitEvent(c->d2h, c->io_ev[4 + stage], 0));
+            for (int k = 0; k < nout; ++k)
+                if (io_stage_out(out_fields[k]) == stage)
+                    CK(cudaMemcpyAsync(out[k], c->io_out + out_off[k], sizeof(double) * out_nc[k] * n,
+                                       cudaMemcpyDeviceToHost, c->d2h));
         }
-        CK(cudaStreamWaitEvent(c->d2h, c->io_ev[4 + stage], 0));
-        for (int k = 0; k < nout; ++k)
-            if (io_stage_out(out_fields[k]) == stage)
-                CK(cudaMemcpyAsync(out[k], c->io_out + out_off[k], sizeof(double) * out_nc[k] * n,
-                                   cudaMemcpyDeviceToHost, c->d2h));
+        // the copy-out stream joins the step's stream
+        CK(cudaEventRecord(c->io_ev[8], c->d2h));
+        CK(cudaStreamWaitEvent(st, c->io_ev[8], 0));
+        return SPH3_OK;
+    };
+    // Replay a graph when this call repeats an earlier one (same buffers,
+    // fields, dt and step count, every host buffer page-locked: a captured copy
+    // from pageable memory is not allowed); the first such call captures it.
+    bool pinned = true;
+    auto is_pinned = [](const void *ptr) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    for (int k = 0; k < nin; ++k) pinned = pinned && is_pinned(in[k]);
+    for (int k = 0; k < nout; ++k) pinned = pinned && is_pinned(out[k]);
+    const bool graph_ok = pinned && c->cfg.use_graph && !c->cfg.timing && c->warm_steps >= 2;
+    if (!graph_ok) {
+        if ((rc = enqueue_io())) return rc;
+        c->warm_steps += nsteps;
+    } else {
+        std::vector<uint64_t> key;
+        uint64_t dtb;
+        std::memcpy(&dtb, &dt, sizeof(dtb));
+        key.push_back(dtb);
+        key.push_back((uint64_t)nsteps);
+        key.push_back((uint64_t)n);
+        key.push_back((uint64_t)nin);
+        for (int k = 0; k < nin; ++k) {
+            key.push_back((uint64_t)in_fields[k]);
+            key.push_back((uint64_t)(uintptr_t)in[k]);
+        }
+        key.push_back((uint64_t)nout);
+        for (int k = 0; k < nout; ++k) {
+            key.push_back((uint64_t)out_fields[k]);
+            key.push_back((uint64_t)(uintptr_t)out[k]);
+        }
+        const int par = c->cur;
+        if (!c->io_graph[par] || c->io_key[par] != key) {
+            if (c->io_graph[par]) cudaGraphExecDestroy(c->io_graph[par]);
+            c->io_graph[par] = nullptr;
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_io();
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            // capture switched the carried block without running: restore it
+            c->cur = par;
+            point_carried(c);
+            if (rc) return rc;
+            if (e != cudaSuccess) return SPH3_ERR_CUDA;
+            e = cudaGraphInstantiate(&c->io_graph[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return SPH3_ERR_CUDA;
+            c->io_key[par] = key;
+        }
+        CK(cudaGraphLaunch(c->io_graph[par], st));
+        c->cur = par ^ (nsteps & 1);
+        point_carried(c);
     }
-    CK(cudaStreamSynchronize(c->d2h));
     CK(cudaStreamSynchronize(st));
     c->inv_valid = true;
     return SPH3_OK;
