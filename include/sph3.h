@@ -255,9 +255,15 @@ int sph3_step(sph3_ctx *ctx, double dt, int32_t nsteps, void *stream);
  * vsig after the u update -- which the serial order runs before the gravity
  * walk -- the rest at the end).  An input u without u_prev also
  * sets u_prev (the reference's loop keeps u_previous = u between
- * iterations).  Page-locked host buffers are needed for the overlap
- * (pageable ones work, serialised).  The steps run without the captured
- * graph; the call synchronises before it returns. */
+ * iterations).  The positions, velocities and accelerations (what the
+ * opening kick reads) move in row chunks, each scattered as soon as it lands;
+ * in the serial order the closing kick runs by row chunks too, each chunk's
+ * outputs copied out while the next is kicked.  Page-locked host buffers are
+ * needed for the overlap (pageable ones work, serialised).  With page-locked
+ * buffers (and use_graph, timing off, after two warm-up steps) the whole call
+ * -- copies, scatters, steps, gathers -- is captured as a CUDA graph and
+ * replayed by later calls with the same buffers, fields, dt and nsteps (a
+ * different call captures again).  The call synchronises before it returns. */
 int sph3_step_io(sph3_ctx *ctx, double dt, int32_t nsteps, int32_t nin, const int32_t *in_fields,
                  const double *const *in, int32_t nout, const int32_t *out_fields, double *const *out,
                  void *stream);
