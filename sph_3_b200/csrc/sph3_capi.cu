@@ -345,8 +345,8 @@ int alloc_for(sph3_ctx *c, int64_t n, int ncloud, int ngroups) {
     T.total = T.meta + 96;
     CK(dalloc(&T.lvl, kLvlEpoch + 1));
     CK(cudaMemset(T.lvl, 0, sizeof(int) * (kLvlEpoch + 1)));
-    // a depth holds at most n + clouds + 64 nodes: tiles of 64 nodes of the level pass
-    const size_t ntiles = (size_t)(nn + ncloud + 64) / 64 + 2;
+    // a depth holds at most n + clouds + 64 nodes: tiles of at least 8 nodes of the level pass
+    const size_t ntiles = (size_t)(nn + ncloud + 64) / 8 + 2;
     CK(dalloc(&T.lb, ntiles));
     CK(cudaMemset(T.lb, 0, sizeof(unsigned long long) * ntiles));
     c->cap_groups = std::max(ngroups, 1);

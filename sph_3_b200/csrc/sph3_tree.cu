@@ -189,13 +189,17 @@ __device__ int tile_lookback(unsigned long long *state, int tile, int tot, unsig
 }
 
 // One depth of the top-down build in one launch: blocks take tiles of
-// kTreeTile consecutive nodes of depth d in order; a warp per node finds its
+// consecutive nodes of depth d in order; a warp per node finds its
 // octant starts (node_octants), the tile's child counts are scanned in the
 // block and offset by the look-back prefix over earlier tiles, and a thread
 // per node writes the children.  The children of the depth come out compacted
 // in node order -- the layout of a global exclusive scan -- so the tree is
-// deterministic.  The last tile sets depth_begin[d + 2].
+// deterministic.  The last tile sets depth_begin[d + 2].  Tiles hold up to
+// kTreeTile nodes, fewer (down to one per warp) at the shallow depths, whose
+// few nodes have long key runs to search: there the depth's nodes spread
+// over all blocks instead of queueing eight deep behind one block's warps.
 constexpr int kTreeTile = 64;
+constexpr int kTreeTileMin = 8;
 
 __global__ void __launch_bounds__(256) k_tree_level(Tree T, const uint64_t *key, int d, int leaf_size, int max_level,
                                                     unsigned *status) {
@@ -208,7 +212,9 @@ __global__ void __launch_bounds__(256) k_tree_level(Tree T, const uint64_t *key,
         if (blockIdx.x == 0 && threadIdx.x == 0) T.depth_begin[d + 2] = end;
         return;
     }
-    const int ntiles = (m + kTreeTile - 1) / kTreeTile;
+    const int per_block = (m + gridDim.x - 1) / gridDim.x;
+    const int ts = min(kTreeTile, max(kTreeTileMin, (per_block + 7) & ~7));  // nodes per tile
+    const int ntiles = (m + ts - 1) / ts;
     const unsigned tag = (unsigned)T.lvl[kLvlEpoch] * 32u + (unsigned)d;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (;;) {
@@ -216,8 +222,8 @@ __global__ void __launch_bounds__(256) k_tree_level(Tree T, const uint64_t *key,
         __syncthreads();
         const int tile = s_tile;
         if (tile >= ntiles) break;
-        const int t0 = tile * kTreeTile;
-        const int tn = min(kTreeTile, m - t0);
+        const int t0 = tile * ts;
+        const int tn = min(ts, m - t0);
         for (int q = w; q < tn; q += 8) {
             int start;
             const int nch = node_octants(T, key, beg + t0 + q, leaf_size, max_level, start);
