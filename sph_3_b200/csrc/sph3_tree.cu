@@ -213,7 +213,9 @@ __global__ void __launch_bounds__(256) k_tree_level(Tree T, const uint64_t *key,
         return;
     }
     const int per_block = (m + gridDim.x - 1) / gridDim.x;
-    const int ts = min(kTreeTile, max(kTreeTileMin, (per_block + 7) & ~7));  // nodes per tile
+    // nodes per tile: 64, or down to 8 when the depth is too small to give
+    // every block a tile of 16
+    const int ts = per_block <= 16 ? max(kTreeTileMin, (per_block + 7) & ~7) : kTreeTile;
     const int ntiles = (m + ts - 1) / ts;
     const unsigned tag = (unsigned)T.lvl[kLvlEpoch] * 32u + (unsigned)d;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

@@ -68,6 +68,7 @@ struct GTile {
     GN<R> nd[64];
     GP<R> pt[64];
     int nodeq[kNodeQ];
+    int farq[kLeafQ];
 };
 
 __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
@@ -110,17 +111,22 @@ __device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R eps
 // The walk of one group, shared by both precisions.  Pops up to 32 nodes per
 // iteration, accepts a node as a multipole when the group's bbox lies outside
 // both its opening radius and its softening reach, queues accepted nodes
-// (nodeq) and opened leaves (wm.leafq), and hands full queues to
-// flush_nodes(count) / flush_leaves(count).  Returns the iteration count.
-template <class FlushNodes, class FlushLeaves>
-__device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int *nodeq, const Cloud &cl, int ref,
-                                         const GroupBox &gb, float eps_g, FlushNodes &flush_nodes,
-                                         FlushLeaves &flush_leaves_fn, unsigned long long &visits) {
+// (nodeq) and opened leaves, and hands full queues to flush_nodes(count) /
+// flush_leaves(count) / flush_far(count).  An opened leaf that still passes
+// the softening test (it fails only the opening radius) goes to its own
+// queue (farq): every pair it gives lies outside the softened kernel
+// (r >= eps_i + eps_j), so its flush needs no spline.  Others go to
+// wm.leafq.  Returns the iteration count.
+template <class FlushNodes, class FlushLeaves, class FlushFar>
+__device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int *nodeq, int *farq, const Cloud &cl,
+                                         int ref, const GroupBox &gb, float eps_g, FlushNodes &flush_nodes,
+                                         FlushLeaves &flush_leaves_fn, FlushFar &flush_far,
+                                         unsigned long long &visits) {
     const int lane = lane_id();
     int top = 1;
     if (lane == 0) wm.stack[0] = cl.root;
     __syncwarp();
-    int nleaf = 0, nnode = 0;
+    int nleaf = 0, nnode = 0, nfar = 0;
     int guard = 0;
     // each node is popped at most once; the bound only trips on a corrupted tree
     for (; top > 0; ++guard) {
@@ -134,7 +140,7 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
         if (lane < p) node = wm.stack[top - 1 - lane];
         __syncwarp();
         top -= p;
-        bool take_leaf = false, take_node = false;
+        bool take_leaf = false, take_node = false, take_far = false;
         int nch = 0, cf = 0;
         if (node >= 0) {
             const float4 w0 = A.gw[2 * node], w1 = A.gw[2 * node + 1];  // one record, one round trip
@@ -147,8 +153,10 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
                     take_node = true;
                 } else {
                     const int k = chy & 255;
-                    if (k == 0) take_leaf = true;
-                    else {
+                    if (k == 0) {
+                        if (d2 > rs * rs) take_far = true;
+                        else take_leaf = true;
+                    } else {
                         nch = k;
                         cf = __float_as_int(w1.z);
                     }
@@ -161,6 +169,9 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
         const unsigned lb = __ballot_sync(kFull, take_leaf);
         if (take_leaf) wm.leafq[nleaf + __popc(lb & lanemask_lt())] = node;
         nleaf += __popc(lb);
+        const unsigned fb = __ballot_sync(kFull, take_far);
+        if (take_far) farq[nfar + __popc(fb & lanemask_lt())] = node;
+        nfar += __popc(fb);
         top = push_children(wm.stack, top, A.stack_cap, nch, cf, A.status);
         __syncwarp();
         if (nnode > kNodeQ - 32) {
@@ -171,10 +182,15 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
             flush_leaves_fn(nleaf);
             nleaf = 0;
         }
+        if (nfar > kLeafQ - 32) {
+            flush_far(nfar);
+            nfar = 0;
+        }
     }
     __syncwarp();
     if (nnode > 0) flush_nodes(nnode);
     if (nleaf > 0) flush_leaves_fn(nleaf);
+    if (nfar > 0) flush_far(nfar);
     return guard;
 }
 
@@ -286,8 +302,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
         auto flush_leaves_fn = [&](int nl) {
             flush_leaves(A.range, wm.leafq, nl, tile.pt, load_part, part_interact);
         };
+        auto flush_far = [&](int nl) { flush_leaves(A.range, tile.farq, nl, tile.pt, load_part, part_interact); };
         unsigned long long visits = 0;
-        const int guard = grav_walk(A, wm, tile.nodeq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn, visits);
+        const int guard = grav_walk(A, wm, tile.nodeq, tile.farq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn,
+                                    flush_far, visits);
         if (lane == 0) {  // walk statistics
             atomicAdd(&A.counters[kCntVisitsGravity], visits);
             atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
@@ -326,10 +344,17 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
 // lanes per target, each lane over every 2nd (4th) entry pair, and the
 // copies are summed with shuffles, so fewer lanes idle.
 struct GTileF {
-    float4 na[2][16], nb[2][16], nc[2][16], nd[2][16], ne[2][16];  // node pairs, two buffers
-    float4 pa[2][16], pb[2][16];                                    // particle pairs
-    float2 pe[2][16];
+    union {  // the node and particle flushes never overlap
+        struct {
+            float4 na[2][16], nb[2][16], nc[2][16], nd[2][16], ne[2][16];  // node pairs, two buffers
+        };
+        struct {
+            float4 pa[2][16], pb[2][16];  // particle pairs
+            float2 pe[2][16];
+        };
+    };
     int nodeq[kNodeQ];
+    int farq[kLeafQ];  // opened leaves outside every softening kernel
 };
 
 struct NodeF {
@@ -565,8 +590,35 @@ __global__ void __maxnreg__(kGravMaxRegs) k_gravity_f32(GArgs A) {
             flush_leaves_st<PartF>(A.range, wm.leafq, nl, load_part, store_part,
                                    part_interact);
         };
+        // leaves outside every softening kernel: the plain 1/r^2 law, the
+        // same operations as part_interact's far branch (identical results)
+        auto part_interact_far = [&](int buf, int ne) {
+            if (lead) n_part += ne;
+            const int np = (ne + 1) >> 1;
+            for (int pb = 0; pb < np; pb += split) {
+                const int p = pb + cp;
+                const float4 a4 = tile.pa[buf][p], b4 = tile.pb[buf][p];
+                const float2 dx = __fadd2_rn(lo2(a4), ntx), dy = __fadd2_rn(hi2(a4), nty),
+                             dz = __fadd2_rn(lo2(b4), ntz);
+                const float2 m = hi2(b4);
+                float2 r2 = __fmul2_rn(dx, dx);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                const float2 fk = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
+                const float2 mf = __fmul2_rn(m, fk);
+                ax = __ffma2_rn(mf, dx, ax);
+                ay = __ffma2_rn(mf, dy, ay);
+                az = __ffma2_rn(mf, dz, az);
+                if (PHI) pp = __ffma2_rn(m, rinv, pp);
+            }
+        };
+        auto flush_far = [&](int nl) {
+            flush_leaves_st<PartF>(A.range, tile.farq, nl, load_part, store_part, part_interact_far);
+        };
         unsigned long long visits = 0;
-        const int guard = grav_walk(A, wm, tile.nodeq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn, visits);
+        const int guard = grav_walk(A, wm, tile.nodeq, tile.farq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn,
+                                    flush_far, visits);
         if (lane == 0) {  // walk statistics
             atomicAdd(&A.counters[kCntVisitsGravity], visits);
             atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
