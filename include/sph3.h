@@ -232,6 +232,16 @@ int sph3_get_field(sph3_ctx *ctx, int field, double *dst, int64_t row_begin, int
 /* Runs the passes named by `what` (SPH3_DO_* bits) on the loaded state. */
 int sph3_compute(sph3_ctx *ctx, uint32_t what, void *stream);
 
+/* As sph3_compute, but the walks run only for the particles of caller rows
+ * [row_begin, row_end) (the walk groups that hold them): the *_mpi forms of
+ * sph_code/libsx.py (getDensity_mpi :50-86, h_smooth_fast_mpi :852-902,
+ * getAcc_sph_mpi / get_dU_mpi, getAcc_g_smth_mpi), where each rank of
+ * sph_mpi4_v4.py asks for its own slice.  The rows' results equal those of
+ * sph3_compute bit for bit (a group's results depend only on the group);
+ * other rows' pair results are left undefined, and the neighbour lists and
+ * the potential are marked stale. */
+int sph3_compute_rows(sph3_ctx *ctx, uint32_t what, int64_t row_begin, int64_t row_end, void *stream);
+
 /* The reference's start-up: h (bootstrap if h is all zero, then the h search),
  * rho, gravity, P, c, hydro acceleration, du/dt, then u += du/dt * dt,
  * u_prev = u, dudt_prev = du/dt (sph_serial.py:85-134). */

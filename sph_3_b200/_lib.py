@@ -94,6 +94,7 @@ SIGNATURES = {
     "sph3_set_field": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, P]),
     "sph3_get_field": (ctypes.c_int, [P, ctypes.c_int, P, I64, I64, ctypes.c_int, P]),
     "sph3_compute": (ctypes.c_int, [P, U32, P]),
+    "sph3_compute_rows": (ctypes.c_int, [P, U32, I64, I64, P]),
     "sph3_first_step": (ctypes.c_int, [P, D, P]),
     "sph3_step": (ctypes.c_int, [P, D, I32, P]),
     "sph3_energy": (ctypes.c_int, [P, P, P]),

@@ -235,11 +235,18 @@ class Context:
         return out
 
     # ------------------------------------------------------------ passes
-    def compute(self, *what):
+    def compute(self, *what, rows=None):
+        """Run the named passes; rows=(begin, end) runs the walks only for
+        those rows in the caller's order (sph3_compute_rows: the other rows'
+        pair results are left undefined)."""
         mask = 0
         for w in what:
             mask |= DO[w] if isinstance(w, str) else int(w)
-        check(self.lib.sph3_compute(self._ptr, mask, None), "compute")
+        if rows is None:
+            check(self.lib.sph3_compute(self._ptr, mask, None), "compute")
+        else:
+            b, e = int(rows[0]), int(rows[1])
+            check(self.lib.sph3_compute_rows(self._ptr, mask, b, e, None), "compute_rows")
 
     def first_step(self, dt):
         check(self.lib.sph3_first_step(self._ptr, float(dt), None), "first_step")

@@ -70,6 +70,12 @@ struct sph3_ctx {
     // the call it was captured for (buffers, fields, dt, steps)
     cudaGraphExec_t io_graph[2] = {nullptr, nullptr};
     std::vector<uint64_t> io_key[2];
+    // row-restricted compute (sph3_compute_rows): the groups holding the
+    // requested rows, and a per-particle mark
+    int2 *sub_groups = nullptr;
+    int *sub_cloud = nullptr, *sub_n = nullptr;
+    unsigned char *row_flag = nullptr;
+    int64_t sub_cap = 0;
 };
 
 namespace {
@@ -200,9 +206,14 @@ void free_buffers(sph3_ctx *c) {
                     S.tree.bmin, S.tree.bmax, S.tree.hmax, S.tree.epsmax, S.tree.quad, S.tree.box_c,
                     S.tree.box_h, S.tree.com_c, S.tree.mono, S.tree.quad4, S.tree.quad1,
                     S.tree.meta, S.tree.parent, S.tree.arrive, S.tree.lvl, S.tree.lb, S.tree.gw, S.tree.sw, S.list, S.nlist, S.hrec, S.ovf, S.groups, S.group_cloud, S.ngroups_dev, S.clouds, S.box_items,
-                    S.box_item_begin, S.box_part};
+                    S.box_item_begin, S.box_part, c->sub_groups, c->sub_cloud, c->sub_n, c->row_flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    c->sub_groups = nullptr;
+    c->sub_cloud = nullptr;
+    c->sub_n = nullptr;
+    c->row_flag = nullptr;
+    c->sub_cap = 0;
     c->carried[0] = c->carried[1] = nullptr;
     c->orig_blk[0] = c->orig_blk[1] = nullptr;
     c->fixed = c->tmp = c->staging = nullptr;
@@ -395,6 +406,29 @@ __global__ void k_gather_out(const double *src, double *dst, const int64_t *inv,
 __global__ void k_gather_out_int(const int *src, double *dst, const int64_t *inv, int64_t b, int64_t e) {
     for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x)
         dst[r - b] = (double)src[inv[r]];
+}
+
+// mark the particles of caller rows [b, e) (sorted index inv[r])
+__global__ void k_mark_rows(const int64_t *inv, int64_t b, int64_t e, unsigned char *flag) {
+    for (int64_t r = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < e; r += (int64_t)gridDim.x * blockDim.x)
+        flag[inv[r]] = 1;
+}
+
+// the walk groups holding at least one marked particle (order does not
+// matter: a group's results depend only on the group)
+__global__ void k_select_groups(const int2 *groups, const int *gcl, const int *ng, const unsigned char *flag,
+                                int2 *gsub, int *csub, int *nsub) {
+    const int n = *ng;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int2 gr = groups[g];
+        bool any = false;
+        for (int k = gr.x; k < gr.x + gr.y && !any; ++k) any = flag[k] != 0;
+        if (any) {
+            const int s = atomicAdd(nsub, 1);
+            gsub[s] = gr;
+            csub[s] = gcl[g];
+        }
+    }
 }
 
 __global__ void k_invert(const int64_t *orig, int64_t *inv, int64_t n) {
@@ -1071,15 +1105,11 @@ int sph3_get_field(sph3_ctx *c, int field, double *dst, int64_t row_begin, int64
     return SPH3_OK;
 }
 
-int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
-    if (!c) return SPH3_ERR_INVALID_ARG;
-    if (!c->have) return SPH3_ERR_STATE;
-    CK(cudaSetDevice(c->device));
-    cudaStream_t st = pick(c, stream);
+namespace {
+// the body of sph3_compute over whatever group table S holds
+int compute_impl(sph3_ctx *c, uint32_t what, cudaStream_t st) {
     State &S = c->S;
     const Params &P = c->P;
-    if (S.n == 0) return SPH3_OK;
-    if ((what & SPH3_DO_GRAVITY) && P.periodic) return SPH3_ERR_UNSUPPORTED;
     int rc = sync_packs(c, st);
     if (rc) return rc;
     if (what & SPH3_DO_BOOT_H) {
@@ -1113,7 +1143,69 @@ int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
     }
     if (what & (SPH3_DO_ACC_SPH | SPH3_DO_DUDT))
         launch_hydro(S, P, (what & SPH3_DO_ACC_SPH) != 0, (what & SPH3_DO_DUDT) != 0, st);
-    rc = check_launch();
+    return check_launch();
+}
+}  // namespace
+
+int sph3_compute(sph3_ctx *c, uint32_t what, void *stream) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (c->S.n == 0) return SPH3_OK;
+    if ((what & SPH3_DO_GRAVITY) && c->P.periodic) return SPH3_ERR_UNSUPPORTED;
+    const int rc = compute_impl(c, what, st);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_compute_rows(sph3_ctx *c, uint32_t what, int64_t row_begin, int64_t row_end, void *stream) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    State &S = c->S;
+    if (row_begin < 0 || row_end > S.n || row_begin > row_end) return SPH3_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    if (S.n == 0 || row_begin == row_end) return SPH3_OK;
+    if ((what & SPH3_DO_GRAVITY) && c->P.periodic) return SPH3_ERR_UNSUPPORTED;
+    int rc = sync_packs(c, st);  // order, tree and groups as the full call would see them
+    if (rc) return rc;
+    if (c->sub_cap < (int64_t)c->cap_groups || !c->row_flag) {
+        if (c->sub_groups) cudaFree(c->sub_groups);
+        if (c->sub_cloud) cudaFree(c->sub_cloud);
+        if (c->sub_n) cudaFree(c->sub_n);
+        if (c->row_flag) cudaFree(c->row_flag);
+        c->sub_groups = nullptr;
+        c->sub_cloud = nullptr;
+        c->sub_n = nullptr;
+        c->row_flag = nullptr;
+        c->sub_cap = 0;
+        CK(dalloc(&c->sub_groups, c->cap_groups));
+        CK(dalloc(&c->sub_cloud, c->cap_groups));
+        CK(dalloc(&c->sub_n, 1));
+        CK(dalloc(&c->row_flag, c->cap_n));
+        c->sub_cap = c->cap_groups;
+    }
+    const int64_t n = S.n;
+    k_invert<<<blocks_for(c, n), 256, 0, st>>>(S.orig, c->inv, n);
+    CK(cudaMemsetAsync(c->row_flag, 0, (size_t)n, st));
+    CK(cudaMemsetAsync(c->sub_n, 0, sizeof(int), st));
+    k_mark_rows<<<blocks_for(c, row_end - row_begin), 256, 0, st>>>(c->inv, row_begin, row_end, c->row_flag);
+    k_select_groups<<<c->S.num_sms * 4, 256, 0, st>>>(S.groups, S.group_cloud, S.ngroups_dev, c->row_flag,
+                                                      c->sub_groups, c->sub_cloud, c->sub_n);
+    // the walks run over the selected groups only
+    std::swap(S.groups, c->sub_groups);
+    std::swap(S.group_cloud, c->sub_cloud);
+    std::swap(S.ngroups_dev, c->sub_n);
+    rc = compute_impl(c, what, st);
+    std::swap(S.groups, c->sub_groups);
+    std::swap(S.group_cloud, c->sub_cloud);
+    std::swap(S.ngroups_dev, c->sub_n);
+    // lists, potentials and div/curl exist for these rows only
+    S.list_valid = false;
+    c->phi_valid = false;
+    c->inv_valid = true;
     if (rc) return rc;
     CK(cudaStreamSynchronize(st));
     return SPH3_OK;

@@ -68,7 +68,6 @@ struct GTile {
     GN<R> nd[64];
     GP<R> pt[64];
     int nodeq[kNodeQ];
-    int farq[kLeafQ];
 };
 
 __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
@@ -116,8 +115,9 @@ __device__ __forceinline__ void spline_force(R r2, R dx, R dy, R dz, R mj, R eps
 // the softening test (it fails only the opening radius) goes to its own
 // queue (farq): every pair it gives lies outside the softened kernel
 // (r >= eps_i + eps_j), so its flush needs no spline.  Others go to
-// wm.leafq.  Returns the iteration count.
-template <class FlushNodes, class FlushLeaves, class FlushFar>
+// wm.leafq.  Without FAR_QUEUE every opened leaf goes to wm.leafq.  Returns
+// the iteration count.
+template <bool FAR_QUEUE, class FlushNodes, class FlushLeaves, class FlushFar>
 __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int *nodeq, int *farq, const Cloud &cl,
                                          int ref, const GroupBox &gb, float eps_g, FlushNodes &flush_nodes,
                                          FlushLeaves &flush_leaves_fn, FlushFar &flush_far,
@@ -154,7 +154,7 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
                 } else {
                     const int k = chy & 255;
                     if (k == 0) {
-                        if (d2 > rs * rs) take_far = true;
+                        if (FAR_QUEUE && d2 > rs * rs) take_far = true;
                         else take_leaf = true;
                     } else {
                         nch = k;
@@ -169,9 +169,11 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
         const unsigned lb = __ballot_sync(kFull, take_leaf);
         if (take_leaf) wm.leafq[nleaf + __popc(lb & lanemask_lt())] = node;
         nleaf += __popc(lb);
-        const unsigned fb = __ballot_sync(kFull, take_far);
-        if (take_far) farq[nfar + __popc(fb & lanemask_lt())] = node;
-        nfar += __popc(fb);
+        if (FAR_QUEUE) {
+            const unsigned fb = __ballot_sync(kFull, take_far);
+            if (take_far) farq[nfar + __popc(fb & lanemask_lt())] = node;
+            nfar += __popc(fb);
+        }
         top = push_children(wm.stack, top, A.stack_cap, nch, cf, A.status);
         __syncwarp();
         if (nnode > kNodeQ - 32) {
@@ -182,7 +184,7 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
             flush_leaves_fn(nleaf);
             nleaf = 0;
         }
-        if (nfar > kLeafQ - 32) {
+        if (FAR_QUEUE && nfar > kLeafQ - 32) {
             flush_far(nfar);
             nfar = 0;
         }
@@ -190,7 +192,7 @@ __device__ __forceinline__ int grav_walk(const GArgs &A, const WarpMem &wm, int 
     __syncwarp();
     if (nnode > 0) flush_nodes(nnode);
     if (nleaf > 0) flush_leaves_fn(nleaf);
-    if (nfar > 0) flush_far(nfar);
+    if (FAR_QUEUE && nfar > 0) flush_far(nfar);
     return guard;
 }
 
@@ -302,10 +304,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_gravity_f64
         auto flush_leaves_fn = [&](int nl) {
             flush_leaves(A.range, wm.leafq, nl, tile.pt, load_part, part_interact);
         };
-        auto flush_far = [&](int nl) { flush_leaves(A.range, tile.farq, nl, tile.pt, load_part, part_interact); };
         unsigned long long visits = 0;
-        const int guard = grav_walk(A, wm, tile.nodeq, tile.farq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn,
-                                    flush_far, visits);
+        // one leaf queue: the FP64 pair loop has no separate spline branch to skip
+        const int guard = grav_walk<false>(A, wm, tile.nodeq, nullptr, cl, ref, gb, eps_g, flush_nodes,
+                                           flush_leaves_fn, flush_leaves_fn, visits);
         if (lane == 0) {  // walk statistics
             atomicAdd(&A.counters[kCntVisitsGravity], visits);
             atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);
@@ -617,8 +619,8 @@ __global__ void __maxnreg__(kGravMaxRegs) k_gravity_f32(GArgs A) {
             flush_leaves_st<PartF>(A.range, tile.farq, nl, load_part, store_part, part_interact_far);
         };
         unsigned long long visits = 0;
-        const int guard = grav_walk(A, wm, tile.nodeq, tile.farq, cl, ref, gb, eps_g, flush_nodes, flush_leaves_fn,
-                                    flush_far, visits);
+        const int guard = grav_walk<true>(A, wm, tile.nodeq, tile.farq, cl, ref, gb, eps_g, flush_nodes,
+                                          flush_leaves_fn, flush_far, visits);
         if (lane == 0) {  // walk statistics
             atomicAdd(&A.counters[kCntVisitsGravity], visits);
             atomicMax(&A.counters[kCntWalkMaxIter], (unsigned long long)guard);

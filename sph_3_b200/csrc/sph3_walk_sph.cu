@@ -1250,7 +1250,7 @@ __global__ void __launch_bounds__(128, 7) k_hydro_list(LArgs A) {
             }
             const float d2 = dx * dx + dy * dy + dz * dz;
             const float hs = th + hj;
-            const float rr = sqrtf(d2);
+            const float rr = d2 > 0.f ? d2 * rsqrtf(d2) : 0.f;  // as the density pass computes |r|
             const float hij = 0.5f * hs;
             const float q = rr * __fdividef(1.0f, hij);
             const V4<float> sv{r1.x, r1.y, r1.z, mj};

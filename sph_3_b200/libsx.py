@@ -100,7 +100,7 @@ def getDensity_mpi(nbeg, nend, pos, m, h):
     """Rows [nbeg, nend) of getDensity (libsx.py:50-86)."""
     ctx = _context()
     ctx.set_particles(pos, m, h=h)
-    ctx.compute("density")
+    ctx.compute("density", rows=(nbeg, nend))
     return _ret(None, pos, ctx, "rho", rows=(nbeg, nend))
 
 
@@ -121,7 +121,7 @@ def h_smooth_fast_mpi(nbeg, nend, pos, h):
     """Rows [nbeg, nend) of h_smooth_fast (libsx.py:852-902)."""
     ctx = _context()
     ctx.set_particles(pos, _ones(pos), h=h)
-    ctx.compute("h")
+    ctx.compute("h", rows=(nbeg, nend))
     return _ret(None, pos, ctx, "h", rows=(nbeg, nend))
 
 
@@ -130,7 +130,7 @@ def smoothing_length_mpi(nbeg, nend, pos):
     (libsx.py:779-800)."""
     ctx = _context()
     ctx.set_particles(pos, _ones(pos))
-    ctx.compute("boot_h")
+    ctx.compute("boot_h", rows=(nbeg, nend))
     return _ret(None, pos, ctx, "h", rows=(nbeg, nend))
 
 
@@ -163,7 +163,7 @@ def _hydro(pos, v, rho, P, c, h, m, want, visc, alpha, beta=2.0, eta=0.1, divV=N
     if divV is not None:
         ctx.set_field("divV", divV)
         ctx.set_field("curlV", curlV)
-    ctx.compute("acc_sph" if want == "acc_sph" else "dudt")
+    ctx.compute("acc_sph" if want == "acc_sph" else "dudt", rows=rows)
     return _ret(None, pos, ctx, want, rows=rows)
 
 
@@ -204,11 +204,11 @@ def _eps_array(epsilon, pos):
     return epsilon
 
 
-def _gravity(pos, mass, G, epsilon, tree=True):
+def _gravity(pos, mass, G, epsilon, tree=True, rows=None):
     ctx = _context(G=float(G))
     ctx.set_particles(pos, mass, eps=_eps_array(epsilon, pos))
     if tree:
-        ctx.compute("gravity")
+        ctx.compute("gravity", rows=rows)
     return ctx
 
 
@@ -217,7 +217,8 @@ def _grav_rows(pos, mass, G, epsilon, nbeg, nend, form="rows"):
     if _grav_method == "direct":
         ctx = _gravity(pos, mass, G, epsilon, tree=False)
         return ctx.gravity_pairsum(form, nbeg, nend, device=dev)
-    ctx = _gravity(pos, mass, G, epsilon)
+    whole = nbeg == 0 and nend == _n(pos)
+    ctx = _gravity(pos, mass, G, epsilon, rows=None if whole else (nbeg, nend))
     return _ret(None, pos, ctx, "acc_g", rows=(nbeg, nend))
 
 
