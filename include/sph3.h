@@ -367,7 +367,7 @@ int sph3_counters(sph3_ctx *ctx, int64_t out[16], int clear);
 
 /* Per-phase device times in ms accumulated while cfg.timing = 1:
  * [0] kick+drift+keys, [1] sort, [2] gather, [3] tree, [4] h search,
- * [5] density, [6] gravity, [7] hydro, [8] kick+u+energy.  Clears if `clear`. */
+ * [5] density, [6] gravity, [7] hydro, [8] kick+u.  Clears if `clear`. */
 int sph3_phase_times(sph3_ctx *ctx, double out[9], int clear);
 
 /* Per-particle time step, the reference's dt_array_indiv_dt

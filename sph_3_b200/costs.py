@@ -34,6 +34,7 @@ BYTES = {
     "density": 40,
     "gravity": 40,
     "hydro": 72,
-    # u update + second kick + energy sums
-    "kick_u": 200,
+    # u update (u, u_prev, dudt, dudt_prev read; u, u_prev, dudt_prev written)
+    # + second kick (a_g, a_sph, v read; a, v, packed v written)
+    "kick_u": 56 + 136,
 }
