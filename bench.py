@@ -241,7 +241,7 @@ def cpu_baseline(n, target_s=12.0):
 # DRAM bytes per particle of one gravity launch, from an ncu capture of the
 # step's gravity walk at N=524288 (dram__bytes_read.sum + dram__bytes_write.sum
 # = 31.12 + 1.79 MB)
-GRAV_DRAM_BYTES_PER_PARTICLE = 31.32e6 / 524288
+GRAV_DRAM_BYTES_PER_PARTICLE = 32.78e6 / 524288
 
 
 def make_ic(n, seed, clouds=0):
@@ -493,7 +493,7 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "TFLOP/s", "frac": ach / fp32_peak,
                 "traffic": GRAV_DRAM_BYTES_PER_PARTICLE * n,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one N=524288 launch "
-                                  "(31.32 MB), scaled per particle to this N",
+                                  "(32.78 MB), scaled per particle to this N",
                 "peak_source": fp32_src + "; MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                 "work": "%.3g node + %.3g particle interactions per launch" % (cnt.get("grav_node", 0),
                                                                                cnt.get("grav_part", 0))}
