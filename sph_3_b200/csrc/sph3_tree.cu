@@ -271,11 +271,31 @@ struct MomArgs {
     int mac_offset;    // add the com offset to the opening radius
 };
 
+// Four threads per node: a leaf's particles and an internal node's children
+// are shared out round-robin and the partial sums (FP64), minima and maxima
+// are combined with two shuffles, so a warp reads eight nodes' particle runs
+// four consecutive entries at a time.  The combination order is fixed, so the
+// moments are deterministic.
 __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
     const int beg = T.depth_begin[d], end = T.depth_begin[d + 1];
     const int cap = T.cap;
     const int64_t n = a.n;
-    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    const int qt = threadIdx.x & 3;
+    const unsigned qmask = 0xFu << (threadIdx.x & 28);
+    auto qsum = [&](double v) {
+        v += __shfl_xor_sync(qmask, v, 1);
+        return v + __shfl_xor_sync(qmask, v, 2);
+    };
+    auto qmin = [&](double v) {
+        v = fmin(v, __shfl_xor_sync(qmask, v, 1));
+        return fmin(v, __shfl_xor_sync(qmask, v, 2));
+    };
+    auto qmax = [&](double v) {
+        v = fmax(v, __shfl_xor_sync(qmask, v, 1));
+        return fmax(v, __shfl_xor_sync(qmask, v, 2));
+    };
+    for (int i = beg + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 2); i < end;
+         i += (int)((gridDim.x * blockDim.x) >> 2)) {
         const int2 r = T.range[i];
         const int2 ch = T.child[i];
         const int nch = ch.y & 255;
@@ -284,7 +304,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         double hm = 0, em = 0;
         if (nch == 0) {
 #pragma unroll 4
-            for (int k = r.x; k < r.x + r.y; ++k) {
+            for (int k = r.x + qt; k < r.x + r.y; k += 4) {
                 const double mk = a.m[k];
                 const double x = a.pos[k], y = a.pos[n + k], z = a.pos[2 * n + k];
                 M += mk;
@@ -301,7 +321,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
             // fixed trip count with a guard: the loads of all children are
             // issued together (a node has at most 8), same summation order
 #pragma unroll
-            for (int q8 = 0; q8 < 8; ++q8) {
+            for (int q8 = qt; q8 < 8; q8 += 4) {
                 if (q8 >= nch) continue;
                 const int c = ch.x + q8;
                 const double mc = T.mass[c];
@@ -317,6 +337,16 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
                 em = fmax(em, T.epsmax[c]);
             }
         }
+        M = qsum(M);
+        sx = qsum(sx);
+        sy = qsum(sy);
+        sz = qsum(sz);
+        for (int q = 0; q < 3; ++q) {
+            lo[q] = qmin(lo[q]);
+            hi[q] = qmax(hi[q]);
+        }
+        hm = qmax(hm);
+        em = qmax(em);
         if (r.y == 0) {
             lo[0] = lo[1] = lo[2] = 0.0;
             hi[0] = hi[1] = hi[2] = 0.0;
@@ -327,19 +357,21 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
         } else {
             cx = 0.5 * (lo[0] + hi[0]); cy = 0.5 * (lo[1] + hi[1]); cz = 0.5 * (lo[2] + hi[2]);
         }
-        T.mass[i] = M;
-        T.com[i] = cx; T.com[cap + i] = cy; T.com[2 * cap + i] = cz;
-        for (int q = 0; q < 3; ++q) {
-            T.bmin[q * cap + i] = lo[q];
-            T.bmax[q * cap + i] = hi[q];
+        if (qt == 0) {
+            T.mass[i] = M;
+            T.com[i] = cx; T.com[cap + i] = cy; T.com[2 * cap + i] = cz;
+            for (int q = 0; q < 3; ++q) {
+                T.bmin[q * cap + i] = lo[q];
+                T.bmax[q * cap + i] = hi[q];
+            }
+            T.hmax[i] = hm;
+            T.epsmax[i] = em;
         }
-        T.hmax[i] = hm;
-        T.epsmax[i] = em;
         double Q[6] = {0, 0, 0, 0, 0, 0};
         if (quad) {
             if (nch == 0) {
 #pragma unroll 4
-                for (int k = r.x; k < r.x + r.y; ++k) {
+                for (int k = r.x + qt; k < r.x + r.y; k += 4) {
                     const double mk = a.m[k];
                     const double dx = a.pos[k] - cx, dy = a.pos[n + k] - cy, dz = a.pos[2 * n + k] - cz;
                     const double d2 = dx * dx + dy * dy + dz * dz;
@@ -352,7 +384,7 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
                 }
             } else {
 #pragma unroll
-                for (int q8 = 0; q8 < 8; ++q8) {
+                for (int q8 = qt; q8 < 8; q8 += 4) {
                     if (q8 >= nch) continue;
                     const int c = ch.x + q8;
                     const double mc = T.mass[c];
@@ -367,6 +399,8 @@ __global__ void k_tree_moments(Tree T, MomArgs a, int d, int quad) {
                 }
             }
         }
+        for (int q = 0; q < 6; ++q) Q[q] = qsum(Q[q]);
+        if (qt != 0) continue;  // one thread of the four writes the node
         for (int q = 0; q < 6; ++q) T.quad[q * cap + i] = Q[q];
 
         // FP32 packs for the walks
@@ -663,7 +697,7 @@ void launch_tree_build(State &S, const Params &P, cudaStream_t st) {
     a.clouds = S.clouds; a.key = S.key; a.max_level = S.max_level;
     a.inv_theta = P.theta > 0 ? 1.0 / P.theta : __builtin_inf();
     a.mac_offset = P.mac == SPH3_MAC_BH_OFFSET;
-    for (int d = maxd; d >= 0; --d) k_tree_moments<<<blocks, 128, 0, st>>>(T, a, d, P.quadrupole);
+    for (int d = maxd; d >= 0; --d) k_tree_moments<<<blocks * 4, 128, 0, st>>>(T, a, d, P.quadrupole);
     k_tree_totals<<<blocks, 256, 0, st>>>(T, maxd + 1, S.counters);
     launch_groups(S, st);
 }
