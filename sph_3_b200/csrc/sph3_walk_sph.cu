@@ -66,8 +66,9 @@ __device__ __forceinline__ double exact_dist(double dx, double dy, double dz) {
 
 // The SPH walks take a node with at most kSphLeaf particles whole, as if it
 // were a leaf: below that size descending costs more walk steps than the
-// extra candidates it saves (the gravity walk keeps the tree's own leaves).
-constexpr int kSphLeaf = 32;
+// extra candidates it saves (the per-candidate reach test still drops them;
+// the gravity walk keeps the tree's own leaves).
+constexpr int kSphLeaf = 64;
 
 // Walk the tree for one group, calling flush(nleaf) on full leaf queues.
 // A node is kept if the gap between its bbox and the group bbox is at most
@@ -1119,7 +1120,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_hydro(YArgs
                         const R d2 = dx * dx + dy * dy + dz * dz;
                         const R hs = th + en.p.w;
                         in = d2 <= hs * hs;
-                        rr = (R)sqrtf((float)d2);
+                        rr = d2 > (R)0 ? (R)((float)d2 * rsqrtf((float)d2)) : (R)0;  // as the list pass
                         hij = (R)0.5 * hs;
                         q = (R)((float)rr * __fdividef(1.0f, (float)hij));
                     }
