@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-errors", action="store_true")
     p.add_argument("--no-ensemble", action="store_true")
+    p.add_argument("--no-cooling", action="store_true")
     p.add_argument("--leaf", type=int, default=0)
     p.add_argument("--clouds", type=int, default=0,
                    help="batched ensemble instead of one cloud: this many independent Evrard clouds, N "
@@ -316,6 +317,50 @@ def run_ensemble(args, local_rank, timed, world, ncloud=256):
     return out
 
 
+def run_cooling(local_rank, n=4194304, k=20):
+    """The heating/cooling step (hcoolingZ) on n float particles resident on
+    the GPU (inputs of 76 B per particle, 319 MB at the default n: larger than
+    L2), with a seeded table of the reference's layout: ms per launch and the
+    algorithmic bytes per particle (typ, u, rho, x, y, z read; u and N_M ion
+    fractions written) against the HBM peak."""
+    import torch
+    from sph_3_b200 import cooling
+    dev = torch.device("cuda", local_rank)
+    tab = cooling.seeded_table(seed=0)
+    t = cooling.CoolTable(tab, device=local_rank)
+    units = cooling.Units(unit_density_cgs=1e-24, unit_time_s=3e13, unit_u_cgs=1e12, unit_length_cm=3.086e21)
+    g = torch.Generator(device=dev).manual_seed(1)
+    xyz = tuple(torch.rand(n, device=dev, generator=g) * 4 - 2 for _ in range(3))
+    rho = 10.0 ** (torch.rand(n, device=dev, generator=g) * 8 - 4)
+    u0 = 10.0 ** (torch.rand(n, device=dev, generator=g) * 6 - 3)
+    typ = torch.zeros(n, dtype=torch.int32, device=dev)
+    u = u0.clone()
+    for _ in range(3):
+        u.copy_(u0)
+        cooling.hcooling(t, units, DT, u, rho, xyz, typ=typ)
+    torch.cuda.synchronize()
+    # each launch cools fresh energies (the copy is outside the timed events)
+    ms = 0.0
+    st = torch.cuda.current_stream()
+    for _ in range(k):
+        u.copy_(u0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        cooling.hcooling(t, units, DT, u, rho, xyz, typ=typ)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= k
+    nm = int(tab["dims"][4])
+    per = 4 * 6 + 4 + 4 * nm
+    t.close()
+    return {"workload": "hcoolingZ over %d gas particles (float), seeded table dims %s (N_kpc, N_T, N_nH, N_Z, "
+                        "N_M, N_t)" % (n, list(int(d) for d in tab["dims"])),
+            "ms_per_launch": ms, "particles_per_s": n / (ms / 1e3),
+            "algorithmic_bytes_per_particle": per, "algorithmic_GBps": per * n / (ms / 1e3) / 1e9}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from sph_3_b200 import Config, Context, costs
@@ -460,6 +505,11 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_ensemble and not args.clouds:
         ensemble = run_ensemble(args, local_rank, timed, world)
 
+    # ---- the heating/cooling step on its own (not part of the Evrard step)
+    cool = None
+    if not args.no_cooling and not args.clouds:
+        cool = run_cooling(local_rank)
+
     # ---- roofline of the dominant kernel
     g_flops = (cnt.get("grav_node", 0) * costs.GRAV_NODE_QUAD + cnt.get("grav_part", 0) * costs.GRAV_PART)
     kernels = {}
@@ -471,6 +521,8 @@ def run_ours(args, rank, world, local_rank):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+    if cool is not None:
+        cool["frac_of_hbm_peak"] = cool["algorithmic_GBps"] / hbm_peak
     sm_mhz = ck.get("sm_mhz") or 1965.0
     fp32_nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     try:  # measured on this GPU: packed-FP32 FMA chains on every SM
@@ -535,6 +587,7 @@ def run_ours(args, rank, world, local_rank):
                                       if fp64 else None),
         "errors": errors,
         "ensemble": ensemble,
+        "cooling": cool,
         "energy_drift_timed_region": drift,
         "status": status,
         "e2e": e2e,

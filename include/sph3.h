@@ -42,6 +42,11 @@
  *   sph3_step_io                          the same loop body with its arrays in host
  *        memory (sph_serial.py:142-193 keeps r, v, acc, h, u, ut_previous as NumPy arrays)
  *   sph3_energy                           getKE / getPE (libsx.py:569-620)
+ *   sph3_cool_table_create                the cooling table read from coolHeatGridJan2024.bin
+ *        (Main_Code/hfvGpuSphBHtree_newCool_v8.cu:40-80, 122-199)
+ *   sph3_hcooling / sph3_set_cooling      hcoolingZ after u_updater
+ *        (Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:1433-1623; launched at
+ *         Main_Code/hfvGpuSphBHtree_newCool_v8.cu:1552)
  *
  * Buffers: every pointer argument names memory of the kind its `on_device`
  * flag says (0: host memory, pageable or pinned; 1: device memory of the
@@ -85,6 +90,7 @@ extern "C" {
 #define SPH3_STATUS_LIST_OVERFLOW 0x20u   /* neighbour export capacity exceeded */
 #define SPH3_STATUS_SORT 0x40u            /* radix-sort bookkeeping mismatch */
 #define SPH3_STATUS_BOX_TOO_SMALL 0x80u   /* 2h above half a periodic box length: no unique minimum image */
+#define SPH3_STATUS_COOL_NEGATIVE_U 0x100u /* the cooling table gave a negative u (the reference prints it) */
 
 /* ----------------------------------------------------------------- enums */
 #define SPH3_PREC_MIXED 0 /* FP32 cell-relative pair arithmetic, FP64 state/accumulators/sums */
@@ -419,6 +425,67 @@ int sph3_probe_fp32_rate(int device, double *tflops, void *stream);
  * on entry (the caller's own; it is left unread). */
 int sph3_morton_sort_noalloc(const double *pos, int64_t n, int32_t max_level, int64_t *order,
                              uint64_t *keys, unsigned *status, void *stream);
+
+
+/* ------------------------------------------------------ heating / cooling */
+/* A heating/cooling table in the layout of the reference's
+ * coolHeatGridJan2024.bin (Particles_in_BH_Tree_III/Main_Code/
+ * hfvGpuSphBHtree_newCool_v8.cu:40-80 reads it; :122-199 uploads it).  dims
+ * in the file header's order: N_kpc, N_T, N_nH, N_Z, N_M, N_t.  Host float
+ * arrays: kpc[N_kpc], nh[N_nH], t[N_t] (elapsed seconds), uevol (u after t,
+ * cgs) [N_kpc][N_T][N_nH][N_Z][N_t], metalz (species fractions)
+ * [N_kpc][N_T][N_nH][N_Z][N_M][N_t], uarr (u at t = 0) [N_kpc][N_T][N_nH][N_Z].
+ * The file's Z, T and mu arrays are not used by the step.  Copied to device
+ * `device`; the caller's arrays may be freed after the call. */
+typedef struct sph3_cool_table sph3_cool_table;
+int sph3_cool_table_create(int device, const int32_t dims[6], const float *kpc, const float *nh, const float *t,
+                           const float *uevol, const float *metalz, const float *uarr, sph3_cool_table **out);
+int sph3_cool_table_destroy(sph3_cool_table *table);
+/* dims as given to create; monotone (may be NULL): whether the kpc, nH and t
+ * grids and every T column of uarr are non-decreasing (searched by bisection;
+ * otherwise by the reference's linear scan -- the same index either way). */
+int sph3_cool_table_dims(const sph3_cool_table *table, int32_t dims[6], int32_t monotone[4]);
+
+/* Unit conversions of the reference's params.txt (readParams,
+ * Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:24-53), in float as there. */
+typedef struct sph3_cool_units {
+    float unit_density_cgs; /* UnitDensity_in_cgs */
+    float unit_time_s;      /* unitTime_in_s */
+    float unit_u_cgs;       /* Unit_u_in_cgs */
+    float unit_length_cm;   /* unitLength_in_cm */
+    float kpc_cm;           /* kpc_in_cm (the reference: 3.086e21) */
+    int32_t z_index;        /* metallicity row of the table (the reference fixes 1: [Z/H] = -1) */
+} sph3_cool_units;
+
+/* hcoolingZ (Particles_in_BH_Tree_III/Evrard_Collapse_2024/
+ * hfvCLibs_v7_hfv_v8.1.h:1433-1623) on the reference's float device arrays:
+ * for every particle with typ[i] == 0 (typ NULL: all), u[i] (code units) is
+ * replaced by the table's evolved u after dt at the nearest kpc, nH and t grid
+ * points, interpolated linearly in u along T, and ionfrac[i * N_M + k] (may be
+ * NULL) receives the species fractions.  FP32 as the reference, with the
+ * reference kernel's results bit for bit.  status (one device word, may be NULL): SPH3_STATUS_COOL_NEGATIVE_U
+ * when a particle's new u is negative.  Device pointers on the table's GPU;
+ * stream-ordered, does not synchronise. */
+int sph3_hcooling(const sph3_cool_table *table, const sph3_cool_units *units, float dt, int64_t n,
+                  const int32_t *typ, float *u, const float *rho, const float *x, const float *y, const float *z,
+                  float *ionfrac, uint32_t *status, void *stream);
+
+/* Makes every sph3_step / sph3_step_io of the context apply the table to u
+ * right after the u update, as the production driver calls hcoolingZ after
+ * u_updater (Main_Code/hfvGpuSphBHtree_newCool_v8.cu:1546-1556); every
+ * particle is gas.  The state is rounded to float for the lookups and u is
+ * written back from the float result.  The table must live on the context's
+ * GPU and outlive the setting; table NULL turns cooling off.  The context
+ * keeps the ion fractions of the last step (sph3_get_ionfrac). */
+int sph3_set_cooling(sph3_ctx *ctx, const sph3_cool_table *table, const sph3_cool_units *units);
+
+/* Applies the context's cooling table once to the current state (dt in code
+ * units), outside a step. */
+int sph3_cool_now(sph3_ctx *ctx, double dt, void *stream);
+
+/* Ion fractions of the last cooled step, (n, N_M) float in the caller's
+ * particle order, into a host buffer.  SPH3_ERR_STATE when none exist. */
+int sph3_get_ionfrac(sph3_ctx *ctx, float *out, int64_t n_species);
 
 #ifdef __cplusplus
 }

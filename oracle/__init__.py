@@ -59,12 +59,13 @@ def build(force: bool = False) -> str:
 
 
 def build_ref(ref_root=None):
-    """Compile oracle/_ref/ref_timestep (the reference's own GPU time-step
-    kernel behind a small driver, oracle/build_ref.sh) where the reference is
-    checked out; returns the binary's path, or None when it is not."""
+    """Compile oracle/_ref/ref_timestep and oracle/_ref/ref_cooling (the
+    reference's own GPU time-step and heating/cooling kernels behind small
+    drivers, oracle/build_ref.sh) where the reference is checked out; returns
+    the binaries' paths, or None when it is not."""
     cmd = ["sh", os.path.join(_HERE, "build_ref.sh")] + ([ref_root] if ref_root else [])
     r = subprocess.run(cmd, capture_output=True, text=True)
-    return r.stdout.strip() if r.returncode == 0 else None
+    return r.stdout.split() if r.returncode == 0 else None
 
 
 def _load():
@@ -92,6 +93,7 @@ def _load():
         "orc_pe": [I, P, P, D, P],
         "orc_ke": [I, P, P],
         "orc_timestep": [I, P, P, P, P, P, P, P, P, D, D, C, P, I, P, P],
+        "orc_hcooling": [I, P, P, P, P, P, P, P, ctypes.c_float, P, P, P, P, P, P, P, P, ctypes.c_int32],
         "orc_set_threads": [C],
         "orc_num_threads": [],
     }
@@ -389,3 +391,25 @@ def timestep_rows(pos, v, acc_tot, acc_g, h, c, divV, eps, c_cfl, alpha, neighbo
     _load().orc_timestep(n, _ptr(pos), _ptr(v), _ptr(at), _ptr(ag), _ptr(h), _ptr(c), _ptr(dv), _ptr(eps),
                          float(c_cfl), float(alpha), 1 if neighbours else 0, _ptr(r), r.shape[0], _ptr(dt), _ptr(dh))
     return dt, dh
+
+
+def hcooling(table, units, dt, u, rho, pos, typ=None, z_index=1, ionfrac=True):
+    """hcoolingZ restated in FP32 (orc_hcooling): returns (u_new, ionfrac or
+    None).  `table` holds the arrays of the reference's cooling-table file
+    (dims, kpc, nH, t, uEvol, metalz, uArr); `units` = (unit density cgs,
+    unit time s, unit u cgs, unit length cm, kpc cm)."""
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    pos = f32(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    x, y, z = f32(pos[:, 0]), f32(pos[:, 1]), f32(pos[:, 2])
+    un = f32(u).copy()
+    rh = f32(rho)
+    dims = np.ascontiguousarray(table["dims"], dtype=np.int32)
+    arrs = [f32(table[k]) for k in ("kpc", "nH", "t", "uEvol", "metalz", "uArr")]
+    uv = f32(units)
+    ty = None if typ is None else np.ascontiguousarray(typ, dtype=np.int32)
+    ion = np.zeros((n, int(dims[4])), np.float32) if ionfrac else None
+    vp = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _load().orc_hcooling(n, vp(ty), vp(un), vp(rh), vp(x), vp(y), vp(z), vp(ion), float(dt), vp(dims),
+                         *[vp(a) for a in arrs], vp(uv), int(z_index))
+    return un, ion

@@ -591,3 +591,81 @@ void orc_timestep(int64_t n, const double *pos, const double *v, const double *a
         dhdt[r] = 1.0 / 3.0 * h[i] * divV[i];
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Table-driven heating/cooling: hcoolingZ
+ * (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:1433-1623),
+ * restated in FP32 with the reference's linear scans and nearest-point rule.
+ * Table layout of coolHeatGridJan2024.bin (Main_Code/hfvGpuSphBHtree_newCool_v8.cu:40-80):
+ * uevol [kpc][T][nH][Z][t], metalz [kpc][T][nH][Z][M][t], uarr [kpc][T][nH][Z].
+ * dims: N_kpc, N_T, N_nH, N_Z, N_M, N_t.  units: unit density (cgs), unit time
+ * (s), unit u (cgs), unit length (cm), kpc (cm).  Particles with typ != 0 are
+ * left alone (typ NULL: all gas).  No contraction (-ffp-contract=off) except
+ * the explicit fmaf of the interpolation. */
+static int orc_nearest(const float *g, int n, float x) {
+    int k = -1;
+    for (int j = 0; j < n; ++j)
+        if (k == -1 && x <= g[j]) k = j;
+    if (k > 0) {
+        const float d1 = fabsf(g[k] - x);
+        const float d2 = fabsf(g[k - 1] - x);
+        if (d2 < d1) k -= 1;
+    }
+    if (k == -1) k = n - 1;
+    return k;
+}
+
+void orc_hcooling(int64_t n, const int32_t *typ, float *u, const float *rho, const float *x, const float *y,
+                  const float *z, float *ionfrac, float dt, const int32_t *dims, const float *kpc, const float *nhg,
+                  const float *tg, const float *uevol, const float *metalz, const float *uarr, const float *units,
+                  int32_t z_index) {
+    const int NK = dims[0], NT = dims[1], NH = dims[2], NZ = dims[3], NM = dims[4], Nt = dims[5];
+    const float ud = units[0], ut = units[1], uu = units[2], ul = units[3], kpc_cm = units[4];
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        if (typ && typ[i] != 0) continue;
+        const float dt_sec = dt * ut;
+        float r = sqrtf(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        r = r * ul / kpc_cm;
+        const int ik = orc_nearest(kpc, NK, r);
+        const float mH = 1.6726e-24f, XH = 0.70f;
+        const float rho_cgs = rho[i] * ud;
+        const float nH = rho_cgs * XH / mH;
+        const int ih = orc_nearest(nhg, NH, nH);
+        const int iz = z_index;
+        const int it = orc_nearest(tg, Nt, dt_sec);
+        /* uarr strides */
+        const int64_t sZ0 = 1, sH0 = NZ * sZ0, sT0 = (int64_t)NH * sH0, sK0 = (int64_t)NT * sT0;
+        const float u_i = u[i] * uu;
+        int iu = -1;
+        for (int j = 0; j < NT; ++j) {
+            const int64_t idx = ik * sK0 + j * sT0 + ih * sH0 + iz;
+            if (iu == -1 && u_i <= uarr[idx]) iu = j;
+        }
+        if (iu == -1) iu = NT - 1;
+        /* uevol strides */
+        const int64_t st = 1, sZ = Nt * st, sH = NZ * sZ, sT = (int64_t)NH * sH, sK = (int64_t)NT * sT;
+        const int64_t ndx = ik * sK + iu * sT + ih * sH + iz * sZ + it;
+        float uEv;
+        if (iu > 0) {
+            const float e1 = uevol[ndx - sT], e2 = uevol[ndx];
+            const int64_t iU = ik * sK0 + iu * sT0 + ih * sH0 + iz;
+            const int64_t iUm = ik * sK0 + (iu - 1) * sT0 + ih * sH0 + iz;
+            const float diff = uarr[iU] - uarr[iUm];
+            const float fhi = (u_i - uarr[iUm]) / diff;
+            const float flow = 1.0f - fhi;
+            /* one fused multiply-add: the reference kernel's compiled form
+               (its outputs on the golden vectors equal this bit for bit) */
+            uEv = fmaf(fhi, e2, flow * e1);
+        } else {
+            uEv = uevol[ndx];
+        }
+        u[i] = uEv / uu;
+        if (ionfrac) {
+            const int64_t mt = 1, mM = Nt * mt, mZ = (int64_t)NM * mM, mH = (int64_t)NZ * mZ, mT = (int64_t)NH * mH,
+                          mK = (int64_t)NT * mT;
+            for (int k = 0; k < NM; ++k)
+                ionfrac[i * NM + k] = metalz[ik * mK + iu * mT + ih * mH + iz * mZ + k * mM + it];
+        }
+    }
+}

@@ -74,6 +74,17 @@ class Config(ctypes.Structure):
     ]
 
 
+class CoolUnits(ctypes.Structure):
+    _fields_ = [
+        ("unit_density_cgs", ctypes.c_float),
+        ("unit_time_s", ctypes.c_float),
+        ("unit_u_cgs", ctypes.c_float),
+        ("unit_length_cm", ctypes.c_float),
+        ("kpc_cm", ctypes.c_float),
+        ("z_index", ctypes.c_int32),
+    ]
+
+
 # every exported function with its ctypes signature
 P = ctypes.c_void_p
 I64 = ctypes.c_int64
@@ -113,6 +124,13 @@ SIGNATURES = {
     "sph3_potential_pairsum": (ctypes.c_int, [P, P, P]),
     "sph3_kth_distance": (ctypes.c_int, [P, P, I64, I32, P, ctypes.c_int, P]),
     "sph3_step_io": (ctypes.c_int, [P, D, I32, I32, P, P, I32, P, P, P]),
+    "sph3_cool_table_create": (ctypes.c_int, [ctypes.c_int, P, P, P, P, P, P, P, P]),
+    "sph3_cool_table_destroy": (ctypes.c_int, [P]),
+    "sph3_cool_table_dims": (ctypes.c_int, [P, P, P]),
+    "sph3_hcooling": (ctypes.c_int, [P, P, ctypes.c_float, I64, P, P, P, P, P, P, P, P, P]),
+    "sph3_set_cooling": (ctypes.c_int, [P, P, P]),
+    "sph3_cool_now": (ctypes.c_int, [P, D, P]),
+    "sph3_get_ionfrac": (ctypes.c_int, [P, P, I64]),
 }
 
 _lib = None

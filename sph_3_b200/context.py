@@ -331,6 +331,33 @@ class Context:
               "timestep")
         return self.get_field("dt"), float(v.value)
 
+    def set_cooling(self, table=None, units=None):
+        """Every later step applies the cooling table to u right after the u
+        update (hcoolingZ after u_updater in the production driver); None
+        turns it off.  `table` is a :class:`sph_3_b200.cooling.CoolTable` on
+        this context's GPU, `units` a :class:`sph_3_b200.cooling.Units`."""
+        if table is None:
+            check(self.lib.sph3_set_cooling(self._ptr, None, None), "set_cooling")
+            self._cool = None
+            return
+        cu = units.to_c()
+        check(self.lib.sph3_set_cooling(self._ptr, table.handle, ctypes.byref(cu)), "set_cooling")
+        self._cool = table  # the context uses the table until cooling is turned off
+
+    def cool_now(self, dt):
+        """Applies the cooling table set by :meth:`set_cooling` once to the current state."""
+        check(self.lib.sph3_cool_now(self._ptr, float(dt), None), "cool_now")
+
+    def ionfrac(self):
+        """Species fractions of the last cooled step, (n, N_M) float32, caller's order."""
+        tab = getattr(self, "_cool", None)
+        if tab is None:
+            raise RuntimeError("no cooling table is set")
+        out = np.empty((self.n, tab.n_species), np.float32)
+        check(self.lib.sph3_get_ionfrac(self._ptr, out.ctypes.data_as(ctypes.c_void_p), tab.n_species),
+              "get_ionfrac")
+        return out
+
     def kernels_per_step(self):
         """Kernel launches per step of the captured step graph (-1 before capture)."""
         v = ctypes.c_int64()

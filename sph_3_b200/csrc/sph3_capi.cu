@@ -76,6 +76,14 @@ struct sph3_ctx {
     int *sub_cloud = nullptr, *sub_n = nullptr;
     unsigned char *row_flag = nullptr;
     int64_t sub_cap = 0;
+    // heating / cooling after the u update (sph3_set_cooling): the caller's
+    // table and units, and the last cooled step's ion fractions, (n, N_M)
+    // float in the caller's particle order
+    const sph3_cool_table *cool = nullptr;
+    sph3_cool_units cool_units{};
+    float *ionfrac = nullptr;
+    int64_t ionfrac_cap = 0;  // floats
+    bool ionfrac_valid = false;
 };
 
 namespace {
@@ -255,6 +263,22 @@ void drop_graphs(sph3_ctx *c) {
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
     return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+}
+
+// the ion-fraction buffer of a context with cooling, (n, N_M) floats; any
+// earlier fractions become invalid
+int ensure_ionfrac(sph3_ctx *c) {
+    c->ionfrac_valid = false;
+    if (!c->cool) return SPH3_OK;
+    const int64_t want = std::max<int64_t>(c->S.n, 1) * cool_table_species(c->cool);
+    if (want > c->ionfrac_cap) {
+        if (c->ionfrac) cudaFree(c->ionfrac);
+        c->ionfrac = nullptr;
+        c->ionfrac_cap = 0;
+        if (dalloc(&c->ionfrac, (size_t)want) != cudaSuccess) return SPH3_ERR_OUT_OF_MEMORY;
+        c->ionfrac_cap = want;
+    }
+    return SPH3_OK;
 }
 
 // a temporary device buffer freed on every return path
@@ -642,6 +666,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
         record(c, 7, st);
         if (hk && hk->before_kick) hk->before_kick(st);
         launch_kick_update(S, P, dt, true, false, st);
+        if (c->cool) launch_cooling_state(S, c->cool, &c->cool_units, dt, c->ionfrac, st);
         if (hk && hk->after_u) hk->after_u(st);
         record(c, 8, st);
         if (P.gravity) launch_gravity(S, P, st, phi);
@@ -658,6 +683,7 @@ void enqueue_step(sph3_ctx *c, double dt, cudaStream_t st, const StepHooks *hk =
         launch_hydro(S, P, false, true, st);
         record(c, 10, st);
         launch_u_update(S, P, dt, st);
+        if (c->cool) launch_cooling_state(S, c->cool, &c->cool_units, dt, c->ionfrac, st);
         if (hk && hk->after_u) hk->after_u(st);
     }
     // (no energy sums here: the reference's loop takes none per step, and
@@ -878,6 +904,7 @@ int sph3_ctx_destroy(sph3_ctx *c) {
             if (e) cudaEventDestroy(e);
     if (c->io_in) cudaFree(c->io_in);
     if (c->io_out) cudaFree(c->io_out);
+    if (c->ionfrac) cudaFree(c->ionfrac);
     if (c->h2d) cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamDestroy(c->d2h);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1023,6 +1050,8 @@ int sph3_set_particles(sph3_ctx *c, int64_t n, const double *pos, const double *
     }
     c->have = true;
     c->phi_valid = false;
+    rc = ensure_ionfrac(c);
+    if (rc) return rc;
     rc = resort_all(c, st);
     if (rc) return rc;
     CK(cudaStreamSynchronize(st));
@@ -1303,6 +1332,7 @@ int sph3_step(sph3_ctx *c, double dt, int32_t nsteps, void *stream) {
         point_carried(c);
         c->inv_valid = false;
     }
+    if (c->cool && nsteps > 0) c->ionfrac_valid = true;
     return SPH3_OK;
 }
 
@@ -1554,6 +1584,7 @@ int sph3_step_io(sph3_ctx *c, double dt, int32_t nsteps, int32_t nin, const int3
     }
     CK(cudaStreamSynchronize(st));
     c->inv_valid = true;
+    if (c->cool) c->ionfrac_valid = true;
     return SPH3_OK;
 }
 
@@ -1838,6 +1869,45 @@ int sph3_kth_distance(sph3_ctx *c, const double *qpos, int64_t m, int32_t k, dou
     if (rc) return rc;
     CK(cudaMemcpyAsync(out, dout.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    return SPH3_OK;
+}
+
+int sph3_set_cooling(sph3_ctx *c, const sph3_cool_table *table, const sph3_cool_units *units) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (table) {
+        if (!units || !cool_units_valid(table, units)) return SPH3_ERR_INVALID_ARG;
+        if (cool_table_device(table) != c->device) return SPH3_ERR_INVALID_ARG;
+    }
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // the step graphs change
+    c->cool = table;
+    if (table) c->cool_units = *units;
+    return ensure_ionfrac(c);
+}
+
+int sph3_cool_now(sph3_ctx *c, double dt, void *stream) {
+    if (!c) return SPH3_ERR_INVALID_ARG;
+    if (!c->have) return SPH3_ERR_STATE;
+    if (!c->cool) return SPH3_ERR_STATE;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = pick(c, stream);
+    launch_cooling_state(c->S, c->cool, &c->cool_units, dt, c->ionfrac, st);
+    int rc = check_launch();
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    c->ionfrac_valid = true;
+    return SPH3_OK;
+}
+
+int sph3_get_ionfrac(sph3_ctx *c, float *out, int64_t n_species) {
+    if (!c || !out) return SPH3_ERR_INVALID_ARG;
+    if (!c->cool || !c->ionfrac_valid) return SPH3_ERR_STATE;
+    if (n_species != cool_table_species(c->cool)) return SPH3_ERR_INVALID_ARG;
+    if (c->S.n == 0) return SPH3_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(out, c->ionfrac, sizeof(float) * c->S.n * n_species, cudaMemcpyDeviceToHost));
     return SPH3_OK;
 }
 

@@ -1,0 +1,360 @@
+// Table-driven heating/cooling of the gas (the production runs' step after
+// the u update): the reference kernel hcoolingZ
+// (Particles_in_BH_Tree_III/Evrard_Collapse_2024/hfvCLibs_v7_hfv_v8.1.h:1433-1623,
+// launched right after u_updater at Main_Code/hfvGpuSphBHtree_newCool_v8.cu:1552)
+// over a table in the layout of the reference's coolHeatGridJan2024.bin
+// (Main_Code/hfvGpuSphBHtree_newCool_v8.cu:40-80).
+//
+// Per gas particle, in FP32 as the reference computes it:
+//   r  = |x| in kpc           -> nearest kpc grid point       (ndx_kpc)
+//   nH = rho XH / mH (cgs)    -> nearest nH grid point        (ndx_nH)
+//   dt in s                   -> nearest elapsed-time point   (ndx_t)
+//   u  (cgs)                  -> first T row whose u(T) >= u  (ndx_u)
+//   u_new = linear interpolation in u between rows ndx_u - 1 and ndx_u of the
+//           evolved-u table at (kpc, nH, Z, t)  (row 0, or u beyond the last
+//           row: no interpolation below, extrapolation above, as the reference)
+//   ionFrac[i][k] = table species fractions at (kpc, T = ndx_u, nH, Z, k, t)
+//
+// "First grid point with x <= g[j]" is the reference's linear scan; here it
+// is a binary search when the grid (or, for u, every T column of the table)
+// is non-decreasing -- checked once when the table is made -- and the same
+// linear scan otherwise, so both give the reference's index for every table.
+// Products, sums and quotients are written with explicit round-to-nearest
+// intrinsics, so the results do not depend on the compiler's FMA choices;
+// the one fused operation is the interpolation, fhi * e2 + (flo * e1) with a
+// single rounding, which reproduces the reference kernel's outputs bit for
+// bit (tested against them).
+//
+// A particle's ion fractions are one row of N_M floats; the warp writes its
+// particles' rows one after the other, lane k writing species k, so the
+// stores coalesce instead of striding by N_M per thread.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "sph3_internal.cuh"
+
+struct sph3_cool_table {
+    int device = 0;
+    int nkpc = 0, nT = 0, nnH = 0, nZ = 0, nM = 0, nt = 0;
+    float *kpc = nullptr, *nH = nullptr, *t = nullptr;  // device grids
+    float *uevol = nullptr;                               // [kpc][T][nH][Z][t]
+    float *metalz = nullptr;                              // [kpc][T][nH][Z][M][t]
+    float *uarr = nullptr;                                // [kpc][T][nH][Z]
+    int mono_kpc = 0, mono_nH = 0, mono_t = 0, mono_u = 0;
+};
+
+namespace sph3 {
+
+namespace {
+
+constexpr float kMassH = 1.6726e-24f;  // g (the reference's mH)
+constexpr float kXH = 0.70f;           // hydrogen mass fraction (the reference's XH)
+
+// First j in [0, n) with x <= g[j * stride], or -1 (x above every entry, or
+// NaN).  Binary search when the entries are non-decreasing (the predicate is
+// then false...false true...true), the reference's linear scan otherwise.
+__device__ __forceinline__ int first_at_or_above(const float *g, int n, int64_t stride, float x, int mono) {
+    if (mono) {
+        int lo = 0, hi = n;  // answer in [lo, hi]; hi == n: none
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (x <= g[mid * stride]) hi = mid;
+            else lo = mid + 1;
+        }
+        return lo < n ? lo : -1;
+    }
+    for (int j = 0; j < n; ++j)
+        if (x <= g[j * stride]) return j;
+    return -1;
+}
+
+// The reference's nearest grid point: the first point at or above x, moved
+// one down when the point below is strictly closer; the last point when x is
+// above the grid (or NaN).
+__device__ __forceinline__ int nearest_point(const float *g, int n, float x, int mono) {
+    int k = first_at_or_above(g, n, 1, x, mono);
+    if (k > 0) {
+        const float d1 = fabsf(__fsub_rn(g[k], x));
+        const float d2 = fabsf(__fsub_rn(g[k - 1], x));
+        if (d2 < d1) k -= 1;
+    }
+    return k < 0 ? n - 1 : k;
+}
+
+struct CoolArgs {
+    const float *kpc, *nH, *t, *uevol, *metalz, *uarr;
+    int nkpc, nT, nnH, nZ, nM, nt;
+    int mono_kpc, mono_nH, mono_t, mono_u;
+    int z_index;
+    float dt;
+    float unit_density, unit_time, unit_u, unit_length, kpc_cm;
+};
+
+// One particle's table lookups.  Returns the new u (code units) and the base
+// offset of its ion fractions in the species table (species k at base + k N_t).
+__device__ __forceinline__ float cool_one(const CoolArgs &A, float x, float y, float z, float rho, float u,
+                                          int64_t &ion_base, bool &negative) {
+    const float dt_sec = __fmul_rn(A.dt, A.unit_time);
+    // distance from the origin in kpc
+    float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+    r = __fdiv_rn(__fmul_rn(r, A.unit_length), A.kpc_cm);
+    const int ik = nearest_point(A.kpc, A.nkpc, r, A.mono_kpc);
+    // hydrogen number density
+    const float rho_cgs = __fmul_rn(rho, A.unit_density);
+    const float nh = __fdiv_rn(__fmul_rn(rho_cgs, kXH), kMassH);
+    const int ih = nearest_point(A.nH, A.nnH, nh, A.mono_nH);
+    const int iz = A.z_index;
+    const int it = nearest_point(A.t, A.nt, dt_sec, A.mono_t);
+    // T row from u: strides of uArr [kpc][T][nH][Z]
+    const int64_t sT0 = (int64_t)A.nnH * A.nZ;
+    const int64_t sK0 = (int64_t)A.nT * sT0;
+    const float u_cgs = __fmul_rn(u, A.unit_u);
+    const float *col = A.uarr + ik * sK0 + (int64_t)ih * A.nZ + iz;
+    int iu = first_at_or_above(col, A.nT, sT0, u_cgs, A.mono_u);
+    if (iu < 0) iu = A.nT - 1;
+    // evolved u: strides of uEvol [kpc][T][nH][Z][t]
+    const int64_t sZ = A.nt, sH = (int64_t)A.nZ * sZ, sT = (int64_t)A.nnH * sH, sK = (int64_t)A.nT * sT;
+    const int64_t at = ik * sK + (int64_t)iu * sT + (int64_t)ih * sH + (int64_t)iz * sZ + it;
+    float uev;
+    if (iu > 0) {
+        const float e1 = A.uevol[at - sT], e2 = A.uevol[at];
+        const float lo = col[(int64_t)(iu - 1) * sT0], hi = col[(int64_t)iu * sT0];
+        const float fhi = __fdiv_rn(__fsub_rn(u_cgs, lo), __fsub_rn(hi, lo));
+        const float flo = __fsub_rn(1.0f, fhi);
+        // fused as fhi * e2 + (flo * e1): the form whose results equal the
+        // reference kernel's outputs bit for bit on the golden vectors
+        uev = __fmaf_rn(fhi, e2, __fmul_rn(flo, e1));
+    } else {
+        uev = A.uevol[at];
+    }
+    negative = uev < 0.0f;
+    // species fractions: metalz [kpc][T][nH][Z][M][t]
+    const int64_t mM = A.nt, mZ = (int64_t)A.nM * mM, mH = (int64_t)A.nZ * mZ, mT = (int64_t)A.nnH * mH,
+                  mK = (int64_t)A.nT * mT;
+    ion_base = ik * mK + (int64_t)iu * mT + (int64_t)ih * mH + (int64_t)iz * mZ + it;
+    return __fdiv_rn(uev, A.unit_u);
+}
+
+// Ion fractions of the warp's particles: the lanes with `mine` set hand
+// their output row and species base around; for each, the 32 lanes write the
+// row's N_M species (species k from metalz[base + k N_t]) to consecutive
+// addresses.
+__device__ __forceinline__ void write_ionfrac(const CoolArgs &A, float *ionfrac, bool mine, int64_t row,
+                                              int64_t base) {
+    const int lane = threadIdx.x & 31;
+    const unsigned todo = __ballot_sync(0xffffffffu, mine);
+    for (unsigned m = todo; m; m &= m - 1) {
+        const int p = __ffs(m) - 1;
+        const int64_t b = __shfl_sync(0xffffffffu, base, p);
+        const int64_t r = __shfl_sync(0xffffffffu, row, p);
+        for (int k = lane; k < A.nM; k += 32) ionfrac[r * A.nM + k] = A.metalz[b + (int64_t)k * A.nt];
+    }
+}
+
+// Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).
+// Whole warps stay in the loop so the cooperative ion-fraction write has
+// every lane.
+__global__ void __launch_bounds__(256) k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u,
+                                                  const float *rho, const float *x, const float *y,
+                                                  const float *z, float *ionfrac, unsigned *status) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+        const int64_t i = i0 + (threadIdx.x & 31);
+        const bool gas = i < n && (typ == nullptr || typ[i] == 0);
+        int64_t base = 0;
+        bool neg = false;
+        if (gas) {
+            u[i] = cool_one(A, x[i], y[i], z[i], rho[i], u[i], base, neg);
+            if (neg && status) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
+        }
+        if (ionfrac) write_ionfrac(A, ionfrac, gas, i, base);
+    }
+}
+
+// The context's FP64 state (component-major positions, sorted order; every
+// particle is gas): the inputs are rounded to FP32 as the reference's arrays
+// are, and u is written back from the FP32 result.  Ion fractions go to the
+// particle's row in the caller's order (orig: sorted -> caller index), so they
+// stay valid whatever the context's order later becomes.
+__global__ void __launch_bounds__(256) k_hcooling_state(CoolArgs A, int64_t n, const double *pos,
+                                                        const double *rho, double *u, const int64_t *orig,
+                                                        float *ionfrac, unsigned *status) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+        const int64_t i = i0 + (threadIdx.x & 31);
+        const bool mine = i < n;
+        int64_t base = 0;
+        bool neg = false;
+        if (mine) {
+            const float un = cool_one(A, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
+                                      (float)u[i], base, neg);
+            u[i] = (double)un;
+            if (neg) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
+        }
+        if (ionfrac) write_ionfrac(A, ionfrac, mine, mine ? orig[i] : 0, base);
+    }
+}
+
+CoolArgs make_args(const sph3_cool_table *T, const sph3_cool_units *U, float dt) {
+    CoolArgs A;
+    A.kpc = T->kpc;
+    A.nH = T->nH;
+    A.t = T->t;
+    A.uevol = T->uevol;
+    A.metalz = T->metalz;
+    A.uarr = T->uarr;
+    A.nkpc = T->nkpc;
+    A.nT = T->nT;
+    A.nnH = T->nnH;
+    A.nZ = T->nZ;
+    A.nM = T->nM;
+    A.nt = T->nt;
+    A.mono_kpc = T->mono_kpc;
+    A.mono_nH = T->mono_nH;
+    A.mono_t = T->mono_t;
+    A.mono_u = T->mono_u;
+    A.z_index = U->z_index;
+    A.dt = dt;
+    A.unit_density = U->unit_density_cgs;
+    A.unit_time = U->unit_time_s;
+    A.unit_u = U->unit_u_cgs;
+    A.unit_length = U->unit_length_cm;
+    A.kpc_cm = U->kpc_cm;
+    return A;
+}
+
+int cool_grid(int64_t n, int dev) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+}
+
+bool nondecreasing(const float *g, int64_t n, int64_t stride) {
+    for (int64_t j = 1; j < n; ++j)
+        if (!(g[(j - 1) * stride] <= g[j * stride])) return false;
+    return true;
+}
+
+template <typename T>
+int upload(T **dst, const T *src, size_t count) {
+    if (cudaMalloc(dst, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) return SPH3_ERR_OUT_OF_MEMORY;
+    if (cudaMemcpy(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice) != cudaSuccess) return SPH3_ERR_CUDA;
+    return SPH3_OK;
+}
+
+}  // namespace
+
+int cool_units_valid(const sph3_cool_table *T, const sph3_cool_units *U) {
+    if (!T || !U) return 0;
+    return U->z_index >= 0 && U->z_index < T->nZ;
+}
+
+int cool_table_device(const sph3_cool_table *T) { return T ? T->device : -1; }
+int cool_table_species(const sph3_cool_table *T) { return T ? T->nM : 0; }
+
+void launch_cooling_state(const State &S, const sph3_cool_table *T, const sph3_cool_units *U, double dt,
+                          float *ionfrac, cudaStream_t st) {
+    if (S.n == 0) return;
+    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), 256, 0, st>>>(
+        make_args(T, U, (float)dt), S.n, S.pos, S.rho, S.u, S.orig, ionfrac, S.status);
+}
+
+}  // namespace sph3
+
+using namespace sph3;
+
+extern "C" {
+
+int sph3_cool_table_create(int device, const int32_t dims[6], const float *kpc, const float *nh, const float *t,
+                           const float *uevol, const float *metalz, const float *uarr, sph3_cool_table **out) {
+    if (!out || !dims || !kpc || !nh || !t || !uevol || !metalz || !uarr) return SPH3_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (int k = 0; k < 6; ++k)
+        if (dims[k] <= 0) return SPH3_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SPH3_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return SPH3_ERR_INVALID_ARG;
+    // dims in the order of the file header: N_kpc, N_T, N_nH, N_Z, N_M, N_t
+    const int64_t nk = dims[0], nT = dims[1], nh_ = dims[2], nZ = dims[3], nM = dims[4], nt = dims[5];
+    const int64_t n_u = nk * nT * nh_ * nZ, n_ev = n_u * nt, n_mz = n_ev * nM;
+    if (n_mz > (int64_t(1) << 40)) return SPH3_ERR_INVALID_ARG;
+    auto *T = new (std::nothrow) sph3_cool_table;
+    if (!T) return SPH3_ERR_OUT_OF_MEMORY;
+    T->device = device;
+    T->nkpc = (int)nk;
+    T->nT = (int)nT;
+    T->nnH = (int)nh_;
+    T->nZ = (int)nZ;
+    T->nM = (int)nM;
+    T->nt = (int)nt;
+    T->mono_kpc = nondecreasing(kpc, nk, 1);
+    T->mono_nH = nondecreasing(nh, nh_, 1);
+    T->mono_t = nondecreasing(t, nt, 1);
+    bool mono = true;
+    for (int64_t c = 0; c < nk && mono; ++c)
+        for (int64_t r = 0; r < nh_ * nZ && mono; ++r) mono = nondecreasing(uarr + c * nT * nh_ * nZ + r, nT, nh_ * nZ);
+    T->mono_u = mono;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    int rc = cudaSetDevice(device) == cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA;
+    if (!rc) rc = upload(&T->kpc, kpc, nk);
+    if (!rc) rc = upload(&T->nH, nh, nh_);
+    if (!rc) rc = upload(&T->t, t, nt);
+    if (!rc) rc = upload(&T->uarr, uarr, n_u);
+    if (!rc) rc = upload(&T->uevol, uevol, n_ev);
+    if (!rc) rc = upload(&T->metalz, metalz, n_mz);
+    cudaSetDevice(prev);
+    if (rc) {
+        sph3_cool_table_destroy(T);
+        return rc;
+    }
+    *out = T;
+    return SPH3_OK;
+}
+
+int sph3_cool_table_destroy(sph3_cool_table *T) {
+    if (!T) return SPH3_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(T->device);
+    for (float *p : {T->kpc, T->nH, T->t, T->uevol, T->metalz, T->uarr})
+        if (p) cudaFree(p);
+    cudaSetDevice(prev);
+    delete T;
+    return SPH3_OK;
+}
+
+int sph3_cool_table_dims(const sph3_cool_table *T, int32_t dims[6], int32_t monotone[4]) {
+    if (!T || !dims) return SPH3_ERR_INVALID_ARG;
+    const int32_t d[6] = {T->nkpc, T->nT, T->nnH, T->nZ, T->nM, T->nt};
+    for (int k = 0; k < 6; ++k) dims[k] = d[k];
+    if (monotone) {
+        monotone[0] = T->mono_kpc;
+        monotone[1] = T->mono_nH;
+        monotone[2] = T->mono_t;
+        monotone[3] = T->mono_u;
+    }
+    return SPH3_OK;
+}
+
+int sph3_hcooling(const sph3_cool_table *T, const sph3_cool_units *U, float dt, int64_t n, const int32_t *typ,
+                  float *u, const float *rho, const float *x, const float *y, const float *z, float *ionfrac,
+                  uint32_t *status, void *stream) {
+    if (!T || !U || n < 0) return SPH3_ERR_INVALID_ARG;
+    if (!cool_units_valid(T, U)) return SPH3_ERR_INVALID_ARG;
+    if (n == 0) return SPH3_OK;
+    if (!u || !rho || !x || !y || !z) return SPH3_ERR_INVALID_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return SPH3_ERR_CUDA;
+    if (prev != T->device && cudaSetDevice(T->device) != cudaSuccess) return SPH3_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_hcooling<<<cool_grid(n, T->device), 256, 0, st>>>(make_args(T, U, dt), n, typ, u, rho, x, y, z, ionfrac,
+                                                        status);
+    const cudaError_t e = cudaGetLastError();
+    if (prev != T->device) cudaSetDevice(prev);
+    return e == cudaSuccess ? SPH3_OK : SPH3_ERR_CUDA;
+}
+
+}  // extern "C"

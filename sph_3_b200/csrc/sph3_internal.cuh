@@ -318,6 +318,13 @@ void launch_check_finite(State &S, cudaStream_t st);
 void launch_timestep(State &S, const Params &P, double c_cfl, bool all_pairs, double *dt_min_dev,
                      cudaStream_t st);
 
+// cooling.cu (table-driven heating/cooling of u, hcoolingZ)
+int cool_units_valid(const sph3_cool_table *T, const sph3_cool_units *U);
+int cool_table_device(const sph3_cool_table *T);
+int cool_table_species(const sph3_cool_table *T);
+void launch_cooling_state(const State &S, const sph3_cool_table *T, const sph3_cool_units *U, double dt,
+                          float *ionfrac, cudaStream_t st);
+
 // pack selectors for launch_pack
 constexpr unsigned kPackPos = 1, kPackHme = 2, kPackVel = 4, kPackThm = 8;
 
