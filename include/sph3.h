@@ -473,7 +473,8 @@ int sph3_hcooling(const sph3_cool_table *table, const sph3_cool_units *units, fl
 /* Makes every sph3_step / sph3_step_io of the context apply the table to u
  * right after the u update, as the production driver calls hcoolingZ after
  * u_updater (Main_Code/hfvGpuSphBHtree_newCool_v8.cu:1546-1556); every
- * particle is gas.  The state is rounded to float for the lookups and u is
+ * particle is gas.  sph3_first_step does not cool, as the driver's first
+ * step before its loop does not (:1033).  The state is rounded to float for the lookups and u is
  * written back from the float result.  The table must live on the context's
  * GPU and outlive the setting; table NULL turns cooling off.  The context
  * keeps the ion fractions of the last step (sph3_get_ionfrac). */

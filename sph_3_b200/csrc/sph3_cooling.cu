@@ -25,9 +25,10 @@
 // single rounding, which reproduces the reference kernel's outputs bit for
 // bit (tested against them).
 //
-// A particle's ion fractions are one row of N_M floats; the warp writes its
-// particles' rows one after the other, lane k writing species k, so the
-// stores coalesce instead of striding by N_M per thread.
+// A particle's ion fractions are one row of N_M floats.  On the raw arrays a
+// warp's rows are one contiguous block: the lanes gather their species into
+// shared memory and the warp writes the block with consecutive lanes on
+// consecutive addresses, instead of 32 stores strided by N_M floats.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -137,31 +138,35 @@ __device__ __forceinline__ float cool_one(const CoolArgs &A, float x, float y, f
     return __fdiv_rn(uev, A.unit_u);
 }
 
-// Ion fractions of the warp's particles: the lanes with `mine` set hand
-// their output row and species base around; for each, the 32 lanes write the
-// row's N_M species (species k from metalz[base + k N_t]) to consecutive
-// addresses.
-__device__ __forceinline__ void write_ionfrac(const CoolArgs &A, float *ionfrac, bool mine, int64_t row,
-                                              int64_t base) {
-    const int lane = threadIdx.x & 31;
-    const unsigned todo = __ballot_sync(0xffffffffu, mine);
-    for (unsigned m = todo; m; m &= m - 1) {
-        const int p = __ffs(m) - 1;
-        const int64_t b = __shfl_sync(0xffffffffu, base, p);
-        const int64_t r = __shfl_sync(0xffffffffu, row, p);
-        for (int k = lane; k < A.nM; k += 32) ionfrac[r * A.nM + k] = A.metalz[b + (int64_t)k * A.nt];
-    }
+// One particle's N_M species fractions (species k at metalz[base + k N_t])
+// into its output row, thread by thread.
+__device__ __forceinline__ void ionfrac_row(const CoolArgs &A, float *dst, int64_t base) {
+    for (int k = 0; k < A.nM; ++k) dst[k] = A.metalz[base + (int64_t)k * A.nt];
 }
 
-// Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).
-// Whole warps stay in the loop so the cooperative ion-fraction write has
-// every lane.
-__global__ void __launch_bounds__(256) k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u,
-                                                  const float *rho, const float *x, const float *y,
-                                                  const float *z, float *ionfrac, unsigned *status) {
+constexpr int kCoolThreads = 256;
+constexpr int kIonStage = 32;  // species staged per particle (rows of 32 floats, padded to 33)
+
+// Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).  A
+// warp's 32 particles own the contiguous rows [i0, i0 + 32) of ionfrac.  With
+// N_M <= 32 each lane gathers its species into a padded shared-memory row and
+// the warp then writes the whole block of 32 * N_M floats with consecutive
+// lanes on consecutive addresses (rows of non-gas particles are skipped, so
+// they keep their contents); with more species each thread writes its row.
+// Whole warps stay in the loop.
+__global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u,
+                                                          const float *rho, const float *x, const float *y,
+                                                          const float *z, float *ionfrac, unsigned *status) {
+    __shared__ float stage[kCoolThreads / 32][32][kIonStage + 1];
+    const int lane = threadIdx.x & 31;
+    float(*buf)[kIonStage + 1] = stage[threadIdx.x >> 5];
+    const bool staged = A.nM <= kIonStage;
+    // position in the warp block of this lane's first element: row p, species k
+    const int p0 = staged ? lane / A.nM : 0, k0 = staged ? lane - p0 * A.nM : 0;
+    const int dp = staged ? 32 / A.nM : 0, dk = staged ? 32 - dp * A.nM : 0;  // per 32 elements
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
-        const int64_t i = i0 + (threadIdx.x & 31);
+        const int64_t i = i0 + lane;
         const bool gas = i < n && (typ == nullptr || typ[i] == 0);
         int64_t base = 0;
         bool neg = false;
@@ -169,7 +174,29 @@ __global__ void __launch_bounds__(256) k_hcooling(CoolArgs A, int64_t n, const i
             u[i] = cool_one(A, x[i], y[i], z[i], rho[i], u[i], base, neg);
             if (neg && status) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
         }
-        if (ionfrac) write_ionfrac(A, ionfrac, gas, i, base);
+        if (!ionfrac) continue;
+        if (!staged) {
+            if (gas) ionfrac_row(A, ionfrac + i * A.nM, base);
+            continue;
+        }
+        if (gas)
+            for (int k = 0; k < A.nM; ++k) buf[lane][k] = A.metalz[base + (int64_t)k * A.nt];
+        const unsigned gm = __ballot_sync(0xffffffffu, gas);
+        __syncwarp();
+        const int rows = n - i0 < 32 ? (int)(n - i0) : 32;
+        const int total = rows * A.nM;
+        float *out = ionfrac + i0 * A.nM;
+        int p = p0, k = k0;
+        for (int e = lane; e < total; e += 32) {
+            if ((gm >> p) & 1u) out[e] = buf[p][k];
+            p += dp;
+            k += dk;
+            if (k >= A.nM) {
+                k -= A.nM;
+                ++p;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -177,23 +204,21 @@ __global__ void __launch_bounds__(256) k_hcooling(CoolArgs A, int64_t n, const i
 // particle is gas): the inputs are rounded to FP32 as the reference's arrays
 // are, and u is written back from the FP32 result.  Ion fractions go to the
 // particle's row in the caller's order (orig: sorted -> caller index), so they
-// stay valid whatever the context's order later becomes.
-__global__ void __launch_bounds__(256) k_hcooling_state(CoolArgs A, int64_t n, const double *pos,
-                                                        const double *rho, double *u, const int64_t *orig,
-                                                        float *ionfrac, unsigned *status) {
+// stay valid whatever the context's order later becomes; those rows are
+// scattered, so each thread writes its own.
+__global__ void __launch_bounds__(kCoolThreads) k_hcooling_state(CoolArgs A, int64_t n, const double *pos,
+                                                                const double *rho, double *u,
+                                                                const int64_t *orig, float *ionfrac,
+                                                                unsigned *status) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
-        const int64_t i = i0 + (threadIdx.x & 31);
-        const bool mine = i < n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int64_t base = 0;
         bool neg = false;
-        if (mine) {
-            const float un = cool_one(A, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
-                                      (float)u[i], base, neg);
-            u[i] = (double)un;
-            if (neg) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
-        }
-        if (ionfrac) write_ionfrac(A, ionfrac, mine, mine ? orig[i] : 0, base);
+        const float un = cool_one(A, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
+                                  (float)u[i], base, neg);
+        u[i] = (double)un;
+        if (neg) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
+        if (ionfrac) ionfrac_row(A, ionfrac + orig[i] * A.nM, base);
     }
 }
 
@@ -257,7 +282,7 @@ int cool_table_species(const sph3_cool_table *T) { return T ? T->nM : 0; }
 void launch_cooling_state(const State &S, const sph3_cool_table *T, const sph3_cool_units *U, double dt,
                           float *ionfrac, cudaStream_t st) {
     if (S.n == 0) return;
-    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), 256, 0, st>>>(
+    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), kCoolThreads, 0, st>>>(
         make_args(T, U, (float)dt), S.n, S.pos, S.rho, S.u, S.orig, ionfrac, S.status);
 }
 
@@ -350,7 +375,7 @@ int sph3_hcooling(const sph3_cool_table *T, const sph3_cool_units *U, float dt, 
     if (cudaGetDevice(&prev) != cudaSuccess) return SPH3_ERR_CUDA;
     if (prev != T->device && cudaSetDevice(T->device) != cudaSuccess) return SPH3_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    k_hcooling<<<cool_grid(n, T->device), 256, 0, st>>>(make_args(T, U, dt), n, typ, u, rho, x, y, z, ionfrac,
+    k_hcooling<<<cool_grid(n, T->device), kCoolThreads, 0, st>>>(make_args(T, U, dt), n, typ, u, rho, x, y, z, ionfrac,
                                                         status);
     const cudaError_t e = cudaGetLastError();
     if (prev != T->device) cudaSetDevice(prev);

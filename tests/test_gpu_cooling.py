@@ -170,3 +170,41 @@ def test_context_cooling_in_the_step_graph_matches_eager():
     a.close()
     b.close()
     t.close()
+
+
+@pytest.mark.parametrize("n_species,n", [(5, 19987), (32, 33), (33, 1001), (40, 4099)])
+def test_ion_fraction_block_writes(oc, n_species, n):
+    """Ragged warp blocks, species counts either side of the staged limit and
+    non-gas rows, through the C ABI: gas rows equal the oracle's, non-gas rows
+    keep the caller's contents."""
+    import ctypes
+    import torch
+    from sph_3_b200 import _lib, cooling
+    rng = np.random.default_rng(n_species * 1000 + n)
+    tab = cooling.seeded_table(seed=n_species, dims=(5, 12, 9, 3, n_species, 7))
+    t = cooling.CoolTable(tab, device=0)
+    units = cooling.Units(unit_density_cgs=1e-24, unit_time_s=3e13, unit_u_cgs=1e12, unit_length_cm=3.086e21)
+    pos = rng.uniform(-2.0, 2.0, (n, 3)).astype(np.float32)
+    rho = (10.0 ** rng.uniform(-4, 4, n)).astype(np.float32)
+    u = (10.0 ** rng.uniform(-3, 4, n)).astype(np.float32)
+    typ = np.where(rng.random(n) < 0.2, 2, 0).astype(np.int32)
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
+    ud, rd, td = T(u), T(rho), T(typ)
+    xs = [T(np.ascontiguousarray(pos[:, k])) for k in range(3)]
+    ion = torch.full((n, n_species), -7.0, dtype=torch.float32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    cu = units.to_c()
+    P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+    lib = _lib.load()
+    rc = lib.sph3_hcooling(t.handle, ctypes.byref(cu), ctypes.c_float(2e-3), n, P(td), P(ud), P(rd), P(xs[0]),
+                           P(xs[1]), P(xs[2]), P(ion), P(status), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    uo, io = oc.hcooling(tab, units.as_tuple(), 2e-3, u, rho, pos, typ=typ)
+    gas = typ == 0
+    got = ion.cpu().numpy()
+    assert np.array_equal(ud.cpu().numpy(), uo)
+    assert np.array_equal(got[gas], io[gas])
+    assert np.all(got[~gas] == -7.0)
+    t.close()
