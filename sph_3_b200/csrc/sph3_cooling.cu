@@ -93,21 +93,48 @@ struct CoolArgs {
     float unit_density, unit_time, unit_u, unit_length, kpc_cm;
 };
 
+// The kpc and nH grids a block searches (in shared memory when they fit) and
+// the elapsed-time index, which is the same for every particle of a call.
+struct GridView {
+    const float *kpc, *nH;
+    int it;
+};
+
+constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per block
+
+// Stages the 1-D grids in the block's shared memory (when they fit) and finds
+// the elapsed-time point.  Every thread of the block calls it once, before
+// its particle loop.
+__device__ __forceinline__ GridView stage_grids(const CoolArgs &A, float *sg) {
+    const bool fit = A.nkpc + A.nnH + A.nt <= kGridSmem;
+    if (fit) {
+        for (int j = threadIdx.x; j < A.nkpc; j += blockDim.x) sg[j] = A.kpc[j];
+        for (int j = threadIdx.x; j < A.nnH; j += blockDim.x) sg[A.nkpc + j] = A.nH[j];
+        for (int j = threadIdx.x; j < A.nt; j += blockDim.x) sg[A.nkpc + A.nnH + j] = A.t[j];
+    }
+    __syncthreads();
+    GridView g;
+    g.kpc = fit ? sg : A.kpc;
+    g.nH = fit ? sg + A.nkpc : A.nH;
+    const float *tg = fit ? sg + A.nkpc + A.nnH : A.t;
+    g.it = nearest_point(tg, A.nt, __fmul_rn(A.dt, A.unit_time), A.mono_t);
+    return g;
+}
+
 // One particle's table lookups.  Returns the new u (code units) and the base
 // offset of its ion fractions in the species table (species k at base + k N_t).
-__device__ __forceinline__ float cool_one(const CoolArgs &A, float x, float y, float z, float rho, float u,
-                                          int64_t &ion_base, bool &negative) {
-    const float dt_sec = __fmul_rn(A.dt, A.unit_time);
+__device__ __forceinline__ float cool_one(const CoolArgs &A, const GridView &G, float x, float y, float z,
+                                          float rho, float u, int64_t &ion_base, bool &negative) {
     // distance from the origin in kpc
     float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
     r = __fdiv_rn(__fmul_rn(r, A.unit_length), A.kpc_cm);
-    const int ik = nearest_point(A.kpc, A.nkpc, r, A.mono_kpc);
+    const int ik = nearest_point(G.kpc, A.nkpc, r, A.mono_kpc);
     // hydrogen number density
     const float rho_cgs = __fmul_rn(rho, A.unit_density);
     const float nh = __fdiv_rn(__fmul_rn(rho_cgs, kXH), kMassH);
-    const int ih = nearest_point(A.nH, A.nnH, nh, A.mono_nH);
+    const int ih = nearest_point(G.nH, A.nnH, nh, A.mono_nH);
     const int iz = A.z_index;
-    const int it = nearest_point(A.t, A.nt, dt_sec, A.mono_t);
+    const int it = G.it;
     // T row from u: strides of uArr [kpc][T][nH][Z]
     const int64_t sT0 = (int64_t)A.nnH * A.nZ;
     const int64_t sK0 = (int64_t)A.nT * sT0;
@@ -138,10 +165,20 @@ __device__ __forceinline__ float cool_one(const CoolArgs &A, float x, float y, f
     return __fdiv_rn(uev, A.unit_u);
 }
 
-// One particle's N_M species fractions (species k at metalz[base + k N_t])
-// into its output row, thread by thread.
-__device__ __forceinline__ void ionfrac_row(const CoolArgs &A, float *dst, int64_t base) {
-    for (int k = 0; k < A.nM; ++k) dst[k] = A.metalz[base + (int64_t)k * A.nt];
+// One particle's N_M species fractions (species k at metalz[base + k N_t]),
+// handed to put(k, value): eight loads in flight before their stores, so a
+// particle waits on about N_M / 8 memory round trips rather than N_M.
+template <class Put>
+__device__ __forceinline__ void gather_species(const CoolArgs &A, int64_t base, Put put) {
+    for (int k0 = 0; k0 < A.nM; k0 += 8) {
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (k0 + j < A.nM) v[j] = A.metalz[base + (int64_t)(k0 + j) * A.nt];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (k0 + j < A.nM) put(k0 + j, v[j]);
+    }
 }
 
 constexpr int kCoolThreads = 256;
@@ -158,6 +195,8 @@ __global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n
                                                           const float *rho, const float *x, const float *y,
                                                           const float *z, float *ionfrac, unsigned *status) {
     __shared__ float stage[kCoolThreads / 32][32][kIonStage + 1];
+    __shared__ float grids[kGridSmem];
+    const GridView G = stage_grids(A, grids);
     const int lane = threadIdx.x & 31;
     float(*buf)[kIonStage + 1] = stage[threadIdx.x >> 5];
     const bool staged = A.nM <= kIonStage;
@@ -171,16 +210,16 @@ __global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n
         int64_t base = 0;
         bool neg = false;
         if (gas) {
-            u[i] = cool_one(A, x[i], y[i], z[i], rho[i], u[i], base, neg);
+            u[i] = cool_one(A, G, x[i], y[i], z[i], rho[i], u[i], base, neg);
             if (neg && status) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
         }
         if (!ionfrac) continue;
         if (!staged) {
-            if (gas) ionfrac_row(A, ionfrac + i * A.nM, base);
+            float *row = ionfrac + i * A.nM;
+            if (gas) gather_species(A, base, [&](int k, float v) { row[k] = v; });
             continue;
         }
-        if (gas)
-            for (int k = 0; k < A.nM; ++k) buf[lane][k] = A.metalz[base + (int64_t)k * A.nt];
+        if (gas) gather_species(A, base, [&](int k, float v) { buf[lane][k] = v; });
         const unsigned gm = __ballot_sync(0xffffffffu, gas);
         __syncwarp();
         const int rows = n - i0 < 32 ? (int)(n - i0) : 32;
@@ -210,15 +249,20 @@ __global__ void __launch_bounds__(kCoolThreads) k_hcooling_state(CoolArgs A, int
                                                                 const double *rho, double *u,
                                                                 const int64_t *orig, float *ionfrac,
                                                                 unsigned *status) {
+    __shared__ float grids[kGridSmem];
+    const GridView G = stage_grids(A, grids);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int64_t base = 0;
         bool neg = false;
-        const float un = cool_one(A, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
+        const float un = cool_one(A, G, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
                                   (float)u[i], base, neg);
         u[i] = (double)un;
         if (neg) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
-        if (ionfrac) ionfrac_row(A, ionfrac + orig[i] * A.nM, base);
+        if (ionfrac) {
+            float *row = ionfrac + orig[i] * A.nM;
+            gather_species(A, base, [&](int k, float v) { row[k] = v; });
+        }
     }
 }
 
