@@ -100,13 +100,24 @@ struct GridView {
     int it;
 };
 
-constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per block
+constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per block (at most)
+constexpr int kCoolThreads = 256;
+constexpr int kCoolMinBlocks = 6;  // 48 resident warps per SM: registers capped at 40
+constexpr int kIonStage = 32;      // species staged per particle (rows of N_M + 1 floats) up to this N_M
+
+// Dynamic shared memory of a cooling launch, in floats: the 1-D grids (when
+// they fit) and, for the raw arrays with N_M <= kIonStage, a padded row of
+// N_M + 1 floats per thread.
+__host__ __device__ __forceinline__ int grid_floats(int nkpc, int nnH, int nt) {
+    return nkpc + nnH + nt <= kGridSmem ? nkpc + nnH + nt : 0;
+}
+__host__ __device__ __forceinline__ int stage_floats(int nM) { return nM <= kIonStage ? kCoolThreads * (nM + 1) : 0; }
 
 // Stages the 1-D grids in the block's shared memory (when they fit) and finds
 // the elapsed-time point.  Every thread of the block calls it once, before
 // its particle loop.
 __device__ __forceinline__ GridView stage_grids(const CoolArgs &A, float *sg) {
-    const bool fit = A.nkpc + A.nnH + A.nt <= kGridSmem;
+    const bool fit = grid_floats(A.nkpc, A.nnH, A.nt) > 0;
     if (fit) {
         for (int j = threadIdx.x; j < A.nkpc; j += blockDim.x) sg[j] = A.kpc[j];
         for (int j = threadIdx.x; j < A.nnH; j += blockDim.x) sg[A.nkpc + j] = A.nH[j];
@@ -166,43 +177,39 @@ __device__ __forceinline__ float cool_one(const CoolArgs &A, const GridView &G, 
 }
 
 // One particle's N_M species fractions (species k at metalz[base + k N_t]),
-// handed to put(k, value): eight loads in flight before their stores, so a
-// particle waits on about N_M / 8 memory round trips rather than N_M.
+// handed to put(k, value): four loads in flight before their stores, so a
+// particle waits on about N_M / 4 memory round trips rather than N_M.
 template <class Put>
 __device__ __forceinline__ void gather_species(const CoolArgs &A, int64_t base, Put put) {
-    for (int k0 = 0; k0 < A.nM; k0 += 8) {
-        float v[8];
+    for (int k0 = 0; k0 < A.nM; k0 += 4) {
+        float v[4];
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
+        for (int j = 0; j < 4; ++j)
             if (k0 + j < A.nM) v[j] = A.metalz[base + (int64_t)(k0 + j) * A.nt];
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
+        for (int j = 0; j < 4; ++j)
             if (k0 + j < A.nM) put(k0 + j, v[j]);
     }
 }
 
-constexpr int kCoolThreads = 256;
-constexpr int kIonStage = 32;  // species staged per particle (rows of 32 floats, padded to 33)
-
 // Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).  A
 // warp's 32 particles own the contiguous rows [i0, i0 + 32) of ionfrac.  With
-// N_M <= 32 each lane gathers its species into a padded shared-memory row and
-// the warp then writes the whole block of 32 * N_M floats with consecutive
-// lanes on consecutive addresses (rows of non-gas particles are skipped, so
-// they keep their contents); with more species each thread writes its row.
-// Whole warps stay in the loop.
-__global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u,
-                                                          const float *rho, const float *x, const float *y,
-                                                          const float *z, float *ionfrac, unsigned *status) {
-    __shared__ float stage[kCoolThreads / 32][32][kIonStage + 1];
-    __shared__ float grids[kGridSmem];
-    const GridView G = stage_grids(A, grids);
+// N_M <= kIonStage each lane gathers its species into a padded shared-memory
+// row (N_M + 1 floats: an odd stride, so the lanes' rows fall in different
+// banks) and the warp then writes the whole block of 32 * N_M floats with
+// consecutive lanes on consecutive addresses (rows of non-gas particles are
+// skipped, so they keep their contents); with more species each thread
+// writes its own row.  Whole warps stay in the loop.  Dynamic shared memory:
+// grid_floats + stage_floats floats.
+__global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
+    k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u, const float *rho, const float *x, const float *y,
+               const float *z, float *ionfrac, unsigned *status) {
+    extern __shared__ float cool_smem[];
+    const GridView G = stage_grids(A, cool_smem);
     const int lane = threadIdx.x & 31;
-    float(*buf)[kIonStage + 1] = stage[threadIdx.x >> 5];
     const bool staged = A.nM <= kIonStage;
-    // position in the warp block of this lane's first element: row p, species k
-    const int p0 = staged ? lane / A.nM : 0, k0 = staged ? lane - p0 * A.nM : 0;
-    const int dp = staged ? 32 / A.nM : 0, dk = staged ? 32 - dp * A.nM : 0;  // per 32 elements
+    const int rs = A.nM + 1;  // staged row stride
+    float *buf = cool_smem + grid_floats(A.nkpc, A.nnH, A.nt) + (threadIdx.x & ~31) * rs;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
         const int64_t i = i0 + lane;
@@ -219,15 +226,18 @@ __global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n
             if (gas) gather_species(A, base, [&](int k, float v) { row[k] = v; });
             continue;
         }
-        if (gas) gather_species(A, base, [&](int k, float v) { buf[lane][k] = v; });
+        if (gas) gather_species(A, base, [&](int k, float v) { buf[lane * rs + k] = v; });
         const unsigned gm = __ballot_sync(0xffffffffu, gas);
         __syncwarp();
         const int rows = n - i0 < 32 ? (int)(n - i0) : 32;
         const int total = rows * A.nM;
         float *out = ionfrac + i0 * A.nM;
-        int p = p0, k = k0;
+        // this lane's first element of the warp block (row p, species k), and
+        // the row and species steps of 32 elements
+        int p = lane / A.nM, k = lane - p * A.nM;
+        const int dp = 32 / A.nM, dk = 32 - dp * A.nM;
         for (int e = lane; e < total; e += 32) {
-            if ((gm >> p) & 1u) out[e] = buf[p][k];
+            if ((gm >> p) & 1u) out[e] = buf[p * rs + k];
             p += dp;
             k += dk;
             if (k >= A.nM) {
@@ -245,12 +255,11 @@ __global__ void __launch_bounds__(kCoolThreads) k_hcooling(CoolArgs A, int64_t n
 // particle's row in the caller's order (orig: sorted -> caller index), so they
 // stay valid whatever the context's order later becomes; those rows are
 // scattered, so each thread writes its own.
-__global__ void __launch_bounds__(kCoolThreads) k_hcooling_state(CoolArgs A, int64_t n, const double *pos,
-                                                                const double *rho, double *u,
-                                                                const int64_t *orig, float *ionfrac,
-                                                                unsigned *status) {
-    __shared__ float grids[kGridSmem];
-    const GridView G = stage_grids(A, grids);
+__global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
+    k_hcooling_state(CoolArgs A, int64_t n, const double *pos, const double *rho, double *u, const int64_t *orig,
+                     float *ionfrac, unsigned *status) {
+    extern __shared__ float cool_smem[];
+    const GridView G = stage_grids(A, cool_smem);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int64_t base = 0;
@@ -326,7 +335,8 @@ int cool_table_species(const sph3_cool_table *T) { return T ? T->nM : 0; }
 void launch_cooling_state(const State &S, const sph3_cool_table *T, const sph3_cool_units *U, double dt,
                           float *ionfrac, cudaStream_t st) {
     if (S.n == 0) return;
-    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), kCoolThreads, 0, st>>>(
+    const size_t smem = sizeof(float) * grid_floats(T->nkpc, T->nnH, T->nt);
+    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), kCoolThreads, smem, st>>>(
         make_args(T, U, (float)dt), S.n, S.pos, S.rho, S.u, S.orig, ionfrac, S.status);
 }
 
@@ -419,7 +429,8 @@ int sph3_hcooling(const sph3_cool_table *T, const sph3_cool_units *U, float dt, 
     if (cudaGetDevice(&prev) != cudaSuccess) return SPH3_ERR_CUDA;
     if (prev != T->device && cudaSetDevice(T->device) != cudaSuccess) return SPH3_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    k_hcooling<<<cool_grid(n, T->device), kCoolThreads, 0, st>>>(make_args(T, U, dt), n, typ, u, rho, x, y, z, ionfrac,
+    const size_t smem = sizeof(float) * (grid_floats(T->nkpc, T->nnH, T->nt) + (ionfrac ? stage_floats(T->nM) : 0));
+    k_hcooling<<<cool_grid(n, T->device), kCoolThreads, smem, st>>>(make_args(T, U, dt), n, typ, u, rho, x, y, z, ionfrac,
                                                         status);
     const cudaError_t e = cudaGetLastError();
     if (prev != T->device) cudaSetDevice(prev);
