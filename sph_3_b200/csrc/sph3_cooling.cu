@@ -102,7 +102,7 @@ struct GridView {
 
 constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per block (at most)
 constexpr int kCoolThreads = 256;
-constexpr int kCoolMinBlocks = 6;  // 48 resident warps per SM: registers capped at 40
+constexpr int kCoolMinBlocks = 5;  // 40 resident warps per SM: registers capped at 48
 constexpr int kIonStage = 32;      // species staged per particle (rows of N_M + 1 floats) up to this N_M
 
 // Dynamic shared memory of a cooling launch, in floats: the 1-D grids (when
