@@ -102,16 +102,19 @@ struct GridView {
 
 constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per block (at most)
 constexpr int kCoolThreads = 256;
-constexpr int kCoolMinBlocks = 5;  // 40 resident warps per SM: registers capped at 48
+constexpr int kCoolMinBlocks = 5;  // context kernel: 40 resident warps per SM, registers capped at 48
+constexpr int kCoolRawMinBlocks = 4;  // raw kernel (two particles per thread): 32 warps, 64 registers
 constexpr int kIonStage = 32;      // species staged per particle (rows of N_M + 1 floats) up to this N_M
 
 // Dynamic shared memory of a cooling launch, in floats: the 1-D grids (when
 // they fit) and, for the raw arrays with N_M <= kIonStage, a padded row of
-// N_M + 1 floats per thread.
+// N_M + 1 floats per particle of a block pass (two per thread).
 __host__ __device__ __forceinline__ int grid_floats(int nkpc, int nnH, int nt) {
     return nkpc + nnH + nt <= kGridSmem ? nkpc + nnH + nt : 0;
 }
-__host__ __device__ __forceinline__ int stage_floats(int nM) { return nM <= kIonStage ? kCoolThreads * (nM + 1) : 0; }
+__host__ __device__ __forceinline__ int stage_floats(int nM) {
+    return nM <= kIonStage ? 2 * kCoolThreads * (nM + 1) : 0;  // two particles per thread
+}
 
 // Stages the 1-D grids in the block's shared memory (when they fit) and finds
 // the elapsed-time point.  Every thread of the block calls it once, before
@@ -132,48 +135,98 @@ __device__ __forceinline__ GridView stage_grids(const CoolArgs &A, float *sg) {
     return g;
 }
 
-// One particle's table lookups.  Returns the new u (code units) and the base
-// offset of its ion fractions in the species table (species k at base + k N_t).
-__device__ __forceinline__ float cool_one(const CoolArgs &A, const GridView &G, float x, float y, float z,
-                                          float rho, float u, int64_t &ion_base, bool &negative) {
-    // distance from the origin in kpc
-    float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
-    r = __fdiv_rn(__fmul_rn(r, A.unit_length), A.kpc_cm);
-    const int ik = nearest_point(G.kpc, A.nkpc, r, A.mono_kpc);
-    // hydrogen number density
-    const float rho_cgs = __fmul_rn(rho, A.unit_density);
-    const float nh = __fdiv_rn(__fmul_rn(rho_cgs, kXH), kMassH);
-    const int ih = nearest_point(G.nH, A.nnH, nh, A.mono_nH);
+// First j with x[q] <= col[q][j * stride] for K particles at once, -1 when
+// none (or NaN), over columns of n non-decreasing entries: a bisection with
+// a fixed number of steps (the largest power of two <= n, halved to 1), so
+// the K particles' loads of one step are issued together.  pos counts the
+// leading entries with the predicate false.
+template <int K>
+__device__ __forceinline__ void first_at_or_above_k(const float *const (&col)[K], int n, int64_t stride,
+                                                    const float (&x)[K], int (&out)[K]) {
+    int pos[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) pos[q] = 0;
+    int step = 1;
+    while (2 * step <= n) step *= 2;
+    for (; step > 0; step >>= 1) {
+        float g[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) g[q] = pos[q] + step <= n ? col[q][(int64_t)(pos[q] + step - 1) * stride] : 0.f;
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+            if (pos[q] + step <= n && !(x[q] <= g[q])) pos[q] += step;
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = pos[q] < n ? pos[q] : -1;
+}
+
+// K particles' table lookups, their dependent loads issued together.  u[q]
+// (code units) is replaced by the new u; base[q] is the offset of the
+// particle's ion fractions in the species table (species k at base + k N_t).
+template <int K>
+__device__ __forceinline__ void cool_k(const CoolArgs &A, const GridView &G, const float (&x)[K],
+                                       const float (&y)[K], const float (&z)[K], const float (&rho)[K],
+                                       float (&u)[K], int64_t (&base)[K], bool (&negative)[K]) {
     const int iz = A.z_index;
     const int it = G.it;
-    // T row from u: strides of uArr [kpc][T][nH][Z]
-    const int64_t sT0 = (int64_t)A.nnH * A.nZ;
+    const int64_t sT0 = (int64_t)A.nnH * A.nZ;  // strides of uArr [kpc][T][nH][Z]
     const int64_t sK0 = (int64_t)A.nT * sT0;
-    const float u_cgs = __fmul_rn(u, A.unit_u);
-    const float *col = A.uarr + ik * sK0 + (int64_t)ih * A.nZ + iz;
-    int iu = first_at_or_above(col, A.nT, sT0, u_cgs, A.mono_u);
-    if (iu < 0) iu = A.nT - 1;
+    int ik[K], ih[K], iu[K];
+    float ucgs[K];
+    const float *col[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        // distance from the origin in kpc
+        float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[q], x[q]), __fmul_rn(y[q], y[q])),
+                                       __fmul_rn(z[q], z[q])));
+        r = __fdiv_rn(__fmul_rn(r, A.unit_length), A.kpc_cm);
+        ik[q] = nearest_point(G.kpc, A.nkpc, r, A.mono_kpc);
+        // hydrogen number density
+        const float rho_cgs = __fmul_rn(rho[q], A.unit_density);
+        const float nh = __fdiv_rn(__fmul_rn(rho_cgs, kXH), kMassH);
+        ih[q] = nearest_point(G.nH, A.nnH, nh, A.mono_nH);
+        // T row from u
+        ucgs[q] = __fmul_rn(u[q], A.unit_u);
+        col[q] = A.uarr + ik[q] * sK0 + (int64_t)ih[q] * A.nZ + iz;
+    }
+    if (A.mono_u) {
+        first_at_or_above_k<K>(col, A.nT, sT0, ucgs, iu);
+    } else {
+#pragma unroll
+        for (int q = 0; q < K; ++q) iu[q] = first_at_or_above(col[q], A.nT, sT0, ucgs[q], 0);
+    }
     // evolved u: strides of uEvol [kpc][T][nH][Z][t]
     const int64_t sZ = A.nt, sH = (int64_t)A.nZ * sZ, sT = (int64_t)A.nnH * sH, sK = (int64_t)A.nT * sT;
-    const int64_t at = ik * sK + (int64_t)iu * sT + (int64_t)ih * sH + (int64_t)iz * sZ + it;
-    float uev;
-    if (iu > 0) {
-        const float e1 = A.uevol[at - sT], e2 = A.uevol[at];
-        const float lo = col[(int64_t)(iu - 1) * sT0], hi = col[(int64_t)iu * sT0];
-        const float fhi = __fdiv_rn(__fsub_rn(u_cgs, lo), __fsub_rn(hi, lo));
-        const float flo = __fsub_rn(1.0f, fhi);
-        // fused as fhi * e2 + (flo * e1): the form whose results equal the
-        // reference kernel's outputs bit for bit on the golden vectors
-        uev = __fmaf_rn(fhi, e2, __fmul_rn(flo, e1));
-    } else {
-        uev = A.uevol[at];
+    float e1[K], e2[K], lo[K], hi[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        if (iu[q] < 0) iu[q] = A.nT - 1;
+        const int64_t at = ik[q] * sK + (int64_t)iu[q] * sT + (int64_t)ih[q] * sH + (int64_t)iz * sZ + it;
+        const int below = iu[q] > 0 ? 1 : 0;
+        e2[q] = A.uevol[at];
+        e1[q] = A.uevol[at - below * sT];
+        hi[q] = col[q][(int64_t)iu[q] * sT0];
+        lo[q] = col[q][(int64_t)(iu[q] - below) * sT0];
     }
-    negative = uev < 0.0f;
     // species fractions: metalz [kpc][T][nH][Z][M][t]
     const int64_t mM = A.nt, mZ = (int64_t)A.nM * mM, mH = (int64_t)A.nZ * mZ, mT = (int64_t)A.nnH * mH,
                   mK = (int64_t)A.nT * mT;
-    ion_base = ik * mK + (int64_t)iu * mT + (int64_t)ih * mH + (int64_t)iz * mZ + it;
-    return __fdiv_rn(uev, A.unit_u);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        float uev;
+        if (iu[q] > 0) {
+            const float fhi = __fdiv_rn(__fsub_rn(ucgs[q], lo[q]), __fsub_rn(hi[q], lo[q]));
+            const float flo = __fsub_rn(1.0f, fhi);
+            // fused as fhi * e2 + (flo * e1): the form whose results equal the
+            // reference kernel's outputs bit for bit on the golden vectors
+            uev = __fmaf_rn(fhi, e2[q], __fmul_rn(flo, e1[q]));
+        } else {
+            uev = e2[q];
+        }
+        negative[q] = uev < 0.0f;
+        base[q] = ik[q] * mK + (int64_t)iu[q] * mT + (int64_t)ih[q] * mH + (int64_t)iz * mZ + it;
+        u[q] = __fdiv_rn(uev, A.unit_u);
+    }
 }
 
 // One particle's N_M species fractions (species k at metalz[base + k N_t]),
@@ -192,16 +245,18 @@ __device__ __forceinline__ void gather_species(const CoolArgs &A, int64_t base, 
     }
 }
 
-// Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).  A
-// warp's 32 particles own the contiguous rows [i0, i0 + 32) of ionfrac.  With
-// N_M <= kIonStage each lane gathers its species into a padded shared-memory
-// row (N_M + 1 floats: an odd stride, so the lanes' rows fall in different
-// banks) and the warp then writes the whole block of 32 * N_M floats with
-// consecutive lanes on consecutive addresses (rows of non-gas particles are
-// skipped, so they keep their contents); with more species each thread
-// writes its own row.  Whole warps stay in the loop.  Dynamic shared memory:
-// grid_floats + stage_floats floats.
-__global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
+// Raw arrays (the reference's float device arrays, Typ[i] == 0 is gas).
+// Each lane takes two particles, i0 + lane and i0 + 32 + lane, whose
+// dependent table reads are issued together (cool_k<2>), so a warp's 64
+// particles own the contiguous rows [i0, i0 + 64) of ionfrac.  With
+// N_M <= kIonStage each lane gathers its particles' species into padded
+// shared-memory rows (N_M + 1 floats: an odd stride, so the lanes' rows fall
+// in different banks) and the warp then writes the whole block of 64 * N_M
+// floats with consecutive lanes on consecutive addresses (rows of non-gas
+// particles are skipped, so they keep their contents); with more species
+// each thread writes its own rows.  Whole warps stay in the loop.  Dynamic
+// shared memory: grid_floats + stage_floats floats.
+__global__ void __launch_bounds__(kCoolThreads, kCoolRawMinBlocks)
     k_hcooling(CoolArgs A, int64_t n, const int *typ, float *u, const float *rho, const float *x, const float *y,
                const float *z, float *ionfrac, unsigned *status) {
     extern __shared__ float cool_smem[];
@@ -209,27 +264,50 @@ __global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
     const int lane = threadIdx.x & 31;
     const bool staged = A.nM <= kIonStage;
     const int rs = A.nM + 1;  // staged row stride
-    float *buf = cool_smem + grid_floats(A.nkpc, A.nnH, A.nt) + (threadIdx.x & ~31) * rs;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
-        const int64_t i = i0 + lane;
-        const bool gas = i < n && (typ == nullptr || typ[i] == 0);
-        int64_t base = 0;
-        bool neg = false;
-        if (gas) {
-            u[i] = cool_one(A, G, x[i], y[i], z[i], rho[i], u[i], base, neg);
-            if (neg && status) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
+    float *buf = cool_smem + grid_floats(A.nkpc, A.nnH, A.nt) + 2 * (threadIdx.x & ~31) * rs;
+    const int64_t stride = 2 * (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = 2 * ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)); i0 < n; i0 += stride) {
+        int64_t idx[2];
+        bool gas[2];
+        float xs[2], ys[2], zs[2], rs_[2], us[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            idx[q] = i0 + 32 * q + lane;
+            gas[q] = idx[q] < n && (typ == nullptr || typ[idx[q]] == 0);
+            // lanes without a gas particle run the lookups on harmless values
+            xs[q] = gas[q] ? x[idx[q]] : 0.f;
+            ys[q] = gas[q] ? y[idx[q]] : 0.f;
+            zs[q] = gas[q] ? z[idx[q]] : 0.f;
+            rs_[q] = gas[q] ? rho[idx[q]] : 1.f;
+            us[q] = gas[q] ? u[idx[q]] : 1.f;
+        }
+        int64_t base[2];
+        bool neg[2];
+        cool_k<2>(A, G, xs, ys, zs, rs_, us, base, neg);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (!gas[q]) continue;
+            u[idx[q]] = us[q];
+            if (neg[q] && status) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
         }
         if (!ionfrac) continue;
         if (!staged) {
-            float *row = ionfrac + i * A.nM;
-            if (gas) gather_species(A, base, [&](int k, float v) { row[k] = v; });
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float *row = ionfrac + idx[q] * A.nM;
+                if (gas[q]) gather_species(A, base[q], [&](int k, float v) { row[k] = v; });
+            }
             continue;
         }
-        if (gas) gather_species(A, base, [&](int k, float v) { buf[lane * rs + k] = v; });
-        const unsigned gm = __ballot_sync(0xffffffffu, gas);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            float *row = buf + (32 * q + lane) * rs;
+            if (gas[q]) gather_species(A, base[q], [&](int k, float v) { row[k] = v; });
+        }
+        const unsigned long long gm = (unsigned long long)__ballot_sync(0xffffffffu, gas[0]) |
+                                      ((unsigned long long)__ballot_sync(0xffffffffu, gas[1]) << 32);
         __syncwarp();
-        const int rows = n - i0 < 32 ? (int)(n - i0) : 32;
+        const int rows = n - i0 < 64 ? (int)(n - i0) : 64;
         const int total = rows * A.nM;
         float *out = ionfrac + i0 * A.nM;
         // this lane's first element of the warp block (row p, species k), and
@@ -237,7 +315,7 @@ __global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
         int p = lane / A.nM, k = lane - p * A.nM;
         const int dp = 32 / A.nM, dk = 32 - dp * A.nM;
         for (int e = lane; e < total; e += 32) {
-            if ((gm >> p) & 1u) out[e] = buf[p * rs + k];
+            if ((gm >> p) & 1ull) out[e] = buf[p * rs + k];
             p += dp;
             k += dk;
             if (k >= A.nM) {
@@ -262,15 +340,17 @@ __global__ void __launch_bounds__(kCoolThreads, kCoolMinBlocks)
     const GridView G = stage_grids(A, cool_smem);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        int64_t base = 0;
-        bool neg = false;
-        const float un = cool_one(A, G, (float)pos[i], (float)pos[n + i], (float)pos[2 * n + i], (float)rho[i],
-                                  (float)u[i], base, neg);
-        u[i] = (double)un;
-        if (neg) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
+        int64_t base[1];
+        bool neg[1];
+        const float xs[1] = {(float)pos[i]}, ys[1] = {(float)pos[n + i]}, zs[1] = {(float)pos[2 * n + i]};
+        const float rs_[1] = {(float)rho[i]};
+        float us[1] = {(float)u[i]};
+        cool_k<1>(A, G, xs, ys, zs, rs_, us, base, neg);
+        u[i] = (double)us[0];
+        if (neg[0]) atomicOr(status, SPH3_STATUS_COOL_NEGATIVE_U);
         if (ionfrac) {
             float *row = ionfrac + orig[i] * A.nM;
-            gather_species(A, base, [&](int k, float v) { row[k] = v; });
+            gather_species(A, base[0], [&](int k, float v) { row[k] = v; });
         }
     }
 }
@@ -303,10 +383,12 @@ CoolArgs make_args(const sph3_cool_table *T, const sph3_cool_units *U, float dt)
     return A;
 }
 
+// blocks of a raw-array launch: two particles per thread, at most 8 blocks per SM
 int cool_grid(int64_t n, int dev) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 2 * kCoolThreads - 1) / (2 * kCoolThreads),
+                                                       (int64_t)sms * 8));
 }
 
 bool nondecreasing(const float *g, int64_t n, int64_t stride) {
