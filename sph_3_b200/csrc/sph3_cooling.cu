@@ -104,7 +104,7 @@ constexpr int kGridSmem = 2048;  // floats of the kpc, nH and t grids staged per
 constexpr int kCoolThreads = 256;
 constexpr int kCoolMinBlocks = 5;  // context kernel: 40 resident warps per SM, registers capped at 48
 constexpr int kCoolRawMinBlocks = 4;  // raw kernel (two particles per thread): 32 warps, 64 registers
-constexpr int kIonStage = 32;      // species staged per particle (rows of N_M + 1 floats) up to this N_M
+constexpr int kIonStage = 16;      // species staged per particle (rows of N_M + 1 floats) up to this N_M
 
 // Dynamic shared memory of a cooling launch, in floats: the 1-D grids (when
 // they fit) and, for the raw arrays with N_M <= kIonStage, a padded row of
@@ -115,6 +115,10 @@ __host__ __device__ __forceinline__ int grid_floats(int nkpc, int nnH, int nt) {
 __host__ __device__ __forceinline__ int stage_floats(int nM) {
     return nM <= kIonStage ? 2 * kCoolThreads * (nM + 1) : 0;  // two particles per thread
 }
+// the largest dynamic shared memory of a launch stays within the 48 KB that
+// needs no opt-in
+static_assert(sizeof(float) * (kGridSmem + 2 * kCoolThreads * (kIonStage + 1)) <= 48 * 1024,
+              "cooling launch above 48 KB of dynamic shared memory");
 
 // Stages the 1-D grids in the block's shared memory (when they fit) and finds
 // the elapsed-time point.  Every thread of the block calls it once, before
