@@ -387,12 +387,13 @@ CoolArgs make_args(const sph3_cool_table *T, const sph3_cool_units *U, float dt)
     return A;
 }
 
-// blocks of a raw-array launch: two particles per thread, at most 8 blocks per SM
+// blocks of a raw-array launch: two particles per thread, at most one wave
+// of resident blocks (kCoolRawMinBlocks per SM), which then stride
 int cool_grid(int64_t n, int dev) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + 2 * kCoolThreads - 1) / (2 * kCoolThreads),
-                                                       (int64_t)sms * 8));
+                                                       (int64_t)sms * kCoolRawMinBlocks));
 }
 
 bool nondecreasing(const float *g, int64_t n, int64_t stride) {
@@ -422,7 +423,8 @@ void launch_cooling_state(const State &S, const sph3_cool_table *T, const sph3_c
                           float *ionfrac, cudaStream_t st) {
     if (S.n == 0) return;
     const size_t smem = sizeof(float) * grid_floats(T->nkpc, T->nnH, T->nt);
-    k_hcooling_state<<<std::min<int64_t>((S.n + 255) / 256, (int64_t)S.num_sms * 8), kCoolThreads, smem, st>>>(
+    k_hcooling_state<<<std::min<int64_t>((S.n + kCoolThreads - 1) / kCoolThreads, (int64_t)S.num_sms * kCoolMinBlocks),
+                       kCoolThreads, smem, st>>>(
         make_args(T, U, (float)dt), S.n, S.pos, S.rho, S.u, S.orig, ionfrac, S.status);
 }
 
