@@ -485,7 +485,9 @@ int sph3_set_cooling(sph3_ctx *ctx, const sph3_cool_table *table, const sph3_coo
 int sph3_cool_now(sph3_ctx *ctx, double dt, void *stream);
 
 /* Ion fractions of the last cooled step, (n, N_M) float in the caller's
- * particle order, into a host buffer.  SPH3_ERR_STATE when none exist. */
+ * particle order, into a host buffer (synchronises the device first).
+ * SPH3_ERR_STATE when none exist; SPH3_ERR_INVALID_ARG when n_species is not
+ * the table's N_M. */
 int sph3_get_ionfrac(sph3_ctx *ctx, float *out, int64_t n_species);
 
 #ifdef __cplusplus

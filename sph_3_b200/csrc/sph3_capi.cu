@@ -1883,7 +1883,9 @@ int sph3_set_cooling(sph3_ctx *c, const sph3_cool_table *table, const sph3_cool_
     drop_graphs(c);  // the step graphs change
     c->cool = table;
     if (table) c->cool_units = *units;
-    return ensure_ionfrac(c);
+    const int rc = ensure_ionfrac(c);
+    if (rc) c->cool = nullptr;  // no buffer for the ion fractions: cooling stays off
+    return rc;
 }
 
 int sph3_cool_now(sph3_ctx *c, double dt, void *stream) {
@@ -1906,7 +1908,7 @@ int sph3_get_ionfrac(sph3_ctx *c, float *out, int64_t n_species) {
     if (n_species != cool_table_species(c->cool)) return SPH3_ERR_INVALID_ARG;
     if (c->S.n == 0) return SPH3_OK;
     CK(cudaSetDevice(c->device));
-    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaDeviceSynchronize());  // the last step may have run on any stream of the caller's
     CK(cudaMemcpy(out, c->ionfrac, sizeof(float) * c->S.n * n_species, cudaMemcpyDeviceToHost));
     return SPH3_OK;
 }
