@@ -72,3 +72,11 @@ def test_c_abi_argument_checks_without_gpu():
                              None) == _lib.C["SPH3_ERR_INVALID_ARG"]
     assert lib.sph3_cool_table_destroy(None) == 0
     assert lib.sph3_set_cooling(None, None, None) == _lib.C["SPH3_ERR_INVALID_ARG"]
+
+
+def test_units_layout_matches_header():
+    # sph3_cool_units: five floats then an int32
+    assert ctypes.sizeof(_lib.CoolUnits) == 24
+    u = cooling.Units(1.5, 2.5, 3.5, 4.5, 5.5, 2).to_c()
+    assert (u.unit_density_cgs, u.unit_time_s, u.unit_u_cgs, u.unit_length_cm, u.kpc_cm, u.z_index) == \
+        (1.5, 2.5, 3.5, 4.5, 5.5, 2)
