@@ -198,12 +198,19 @@ void orc_h_smooth(int64_t n, const double *pos, const double *h_in, const int64_
                 double dz = min_image(pos[3 * j + 2] - pos[3 * i + 2], bz);
                 dist[j] = sqrt(dx * dx + dy * dy + dz * dz);
             }
-            /* sort only the K smallest distances: a count below t <= dist[K-1]
-             * is exact on that prefix; larger t falls back to a full scan. */
-            int64_t K = n < 2048 ? n : 2048;
-            if (K < n) select_kth(dist, n, K - 1);
-            qsort(dist, (size_t)K, sizeof(double), cmp_double);
-            int64_t nn = count_prefix(dist, n, K, 2.0 * hi);
+            /* the first count is one pass over the distances, as the
+             * reference's np.sum(dist < 2h); only a row that has to iterate
+             * sorts its K smallest distances, so that every further count
+             * below t <= dist[K-1] is exact on that prefix (larger t falls
+             * back to a full scan) */
+            int64_t nn = 0;
+            for (int64_t j = 0; j < n; ++j) nn += dist[j] < 2.0 * hi;
+            int64_t K = n;
+            if ((nn > up) || (nn < low)) {
+                K = n < 2048 ? n : 2048;
+                if (K < n) select_kth(dist, n, K - 1);
+                qsort(dist, (size_t)K, sizeof(double), cmp_double);
+            }
             int64_t it = 0;
             while ((nn > up) || (nn < low)) {
                 if (it >= max_iter) { it = -1; break; }
@@ -307,6 +314,60 @@ void orc_div_curl(int64_t n, const double *pos, const double *v, const double *r
  * visc = 2: signal form times the Balsara factor of getAcc_sph_shear /
  *           get_dU_shear (sph_code/shear.py:149-235, 332-406).
  * acc (3 per row) and/or dudt may be NULL. */
+/* One row of getAcc_sph / get_dU; want_acc and want_dudt are constants at
+ * every call site, so each specialisation computes only the terms of the
+ * outputs it keeps (as the reference's two separate functions do), with the
+ * same operations for those. */
+static inline __attribute__((always_inline)) void hydro_row(
+    int64_t n, const double *pos, const double *v, const double *rho, const double *P, const double *c,
+    const double *h, const double *m, const double *divV, const double *curlV, int visc, double alpha,
+    double beta, double eta, int64_t i, double bx, double by, double bz, int want_acc, int want_dudt,
+    double *acc_r, double *dudt_r) {
+    double axt = 0.0, ayt = 0.0, azt = 0.0, du_t = 0.0;
+    for (int64_t j = 0; j < n; ++j) {
+        double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
+        double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
+        double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
+        double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
+        double hij = 0.5 * (h[i] + h[j]);
+        double q = rr / hij;
+        double nW = m4_grad_factor(q, hij);
+        double gWx = 0.0, gWy = 0.0, gWz = 0.0;
+        if (q <= 2.0) { gWx = nW * dx; gWy = nW * dy; gWz = nW * dz; }
+        double vxij = v[3 * i + 0] - v[3 * j + 0];
+        double vyij = v[3 * i + 1] - v[3 * j + 1];
+        double vzij = v[3 * i + 2] - v[3 * j + 2];
+        double vij_gWij = vxij * gWx + vyij * gWy + vzij * gWz;
+        double vij_rij = vxij * dx + vyij * dy + vzij * dz;
+        double cij = 0.5 * (c[i] + c[j]);
+        double rhoij = 0.5 * (rho[i] + rho[j]);
+        double PIij = 0.0;
+        if (visc == 1) {
+            double muij = hij * vij_rij / (rr * rr + hij * hij * eta * eta);
+            if (vij_rij <= 0) PIij = (-alpha * cij * muij + beta * muij * muij) / rhoij;
+        } else {
+            double wij = vij_rij / (rr + 1e-5);
+            double vij_sig = c[i] + c[j] - 3.0 * wij;
+            if (vij_rij <= 0) PIij = -0.5 * alpha * vij_sig * wij / rhoij;
+            if (visc == 2) {
+                double fi = divV[i] / (divV[i] + curlV[i] + 0.0001 * c[i] / h[i]);
+                double fj = divV[j] / (divV[j] + curlV[j] + 0.0001 * c[j] / h[j]);
+                double fij = 0.5 * (fi + fj);
+                PIij = fij * PIij;
+            }
+        }
+        if (want_acc) {
+            double pterm = P[i] / ipow(rho[i], 2) + P[j] / ipow(rho[j], 2) + PIij;
+            axt -= m[j] * pterm * gWx;
+            ayt -= m[j] * pterm * gWy;
+            azt -= m[j] * pterm * gWz;
+        }
+        if (want_dudt) du_t += m[j] * (P[i] / ipow(rho[i], 2) + PIij / 2.) * vij_gWij;
+    }
+    if (want_acc) { acc_r[0] = axt; acc_r[1] = ayt; acc_r[2] = azt; }
+    if (want_dudt) *dudt_r = du_t;
+}
+
 void orc_hydro(int64_t n, const double *pos, const double *v, const double *rho,
                const double *P, const double *c, const double *h, const double *m,
                const double *divV, const double *curlV, int visc, double alpha, double beta,
@@ -315,48 +376,14 @@ void orc_hydro(int64_t n, const double *pos, const double *v, const double *rho,
     const double bx = box ? box[0] : 0.0, by = box ? box[1] : 0.0, bz = box ? box[2] : 0.0;
 #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t r = 0; r < nrows; ++r) {
-        int64_t i = rows[r];
-        double axt = 0.0, ayt = 0.0, azt = 0.0, du_t = 0.0;
-        for (int64_t j = 0; j < n; ++j) {
-            double dx = min_image(pos[3 * i + 0] - pos[3 * j + 0], bx);
-            double dy = min_image(pos[3 * i + 1] - pos[3 * j + 1], by);
-            double dz = min_image(pos[3 * i + 2] - pos[3 * j + 2], bz);
-            double rr = sqrt(ipow(dx, 2) + ipow(dy, 2) + ipow(dz, 2));
-            double hij = 0.5 * (h[i] + h[j]);
-            double q = rr / hij;
-            double nW = m4_grad_factor(q, hij);
-            double gWx = 0.0, gWy = 0.0, gWz = 0.0;
-            if (q <= 2.0) { gWx = nW * dx; gWy = nW * dy; gWz = nW * dz; }
-            double vxij = v[3 * i + 0] - v[3 * j + 0];
-            double vyij = v[3 * i + 1] - v[3 * j + 1];
-            double vzij = v[3 * i + 2] - v[3 * j + 2];
-            double vij_gWij = vxij * gWx + vyij * gWy + vzij * gWz;
-            double vij_rij = vxij * dx + vyij * dy + vzij * dz;
-            double cij = 0.5 * (c[i] + c[j]);
-            double rhoij = 0.5 * (rho[i] + rho[j]);
-            double PIij = 0.0;
-            if (visc == 1) {
-                double muij = hij * vij_rij / (rr * rr + hij * hij * eta * eta);
-                if (vij_rij <= 0) PIij = (-alpha * cij * muij + beta * muij * muij) / rhoij;
-            } else {
-                double wij = vij_rij / (rr + 1e-5);
-                double vij_sig = c[i] + c[j] - 3.0 * wij;
-                if (vij_rij <= 0) PIij = -0.5 * alpha * vij_sig * wij / rhoij;
-                if (visc == 2) {
-                    double fi = divV[i] / (divV[i] + curlV[i] + 0.0001 * c[i] / h[i]);
-                    double fj = divV[j] / (divV[j] + curlV[j] + 0.0001 * c[j] / h[j]);
-                    double fij = 0.5 * (fi + fj);
-                    PIij = fij * PIij;
-                }
-            }
-            double pterm = P[i] / ipow(rho[i], 2) + P[j] / ipow(rho[j], 2) + PIij;
-            axt -= m[j] * pterm * gWx;
-            ayt -= m[j] * pterm * gWy;
-            azt -= m[j] * pterm * gWz;
-            du_t += m[j] * (P[i] / ipow(rho[i], 2) + PIij / 2.) * vij_gWij;
-        }
-        if (acc) { acc[3 * r + 0] = axt; acc[3 * r + 1] = ayt; acc[3 * r + 2] = azt; }
-        if (dudt) dudt[r] = du_t;
+        const int64_t i = rows[r];
+        double *ar = acc ? acc + 3 * r : NULL, *dr = dudt ? dudt + r : NULL;
+        if (acc && dudt)
+            hydro_row(n, pos, v, rho, P, c, h, m, divV, curlV, visc, alpha, beta, eta, i, bx, by, bz, 1, 1, ar, dr);
+        else if (acc)
+            hydro_row(n, pos, v, rho, P, c, h, m, divV, curlV, visc, alpha, beta, eta, i, bx, by, bz, 1, 0, ar, dr);
+        else if (dudt)
+            hydro_row(n, pos, v, rho, P, c, h, m, divV, curlV, visc, alpha, beta, eta, i, bx, by, bz, 0, 1, ar, dr);
     }
 }
 
